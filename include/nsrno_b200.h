@@ -1,0 +1,171 @@
+/*
+ * nsrno_b200 -- C ABI of the B200 frequency-domain Helmholtz solve.
+ *
+ * Conventions (mirroring the reference's native ABI, nsrno/native_time.cu:117-155
+ * and nsrno/native_time.py:25-41):
+ *   - every entry point returns 0 on success, a cudaError_t value (< 1000) or an
+ *     NSR_ERR_* code (>= 1000); nsr_error_string() describes either;
+ *   - every buffer is a caller-owned DEVICE pointer unless stated otherwise;
+ *     complex values are interleaved (re, im) pairs: "c64" = 2 x float,
+ *     "c128" = 2 x double;
+ *   - work runs on the caller's stream (a cudaStream_t passed as void*);
+ *     only nsr_solve_batched synchronises (it polls a completion counter);
+ *   - no exceptions cross the ABI; nothing here allocates device memory
+ *     except where stated (nsr_solve_batched takes a caller workspace sized by
+ *     nsr_solve_workspace_size).
+ *
+ * Fields are [z, x] row-major (x contiguous), nz rows by nx columns, like the
+ * reference grid of nsrno/theranostic/wave.py:29-87.
+ */
+#ifndef NSRNO_B200_H
+#define NSRNO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes of one solved system.  They map one to one onto the reason
+ * strings of the reference Krylov drivers (nsrno/dense_wave.py:127-147,
+ * nsrno/wave_solver.py:17-37). */
+enum {
+  NSR_CONVERGED = 0,
+  NSR_ITERATION_BUDGET = 1,
+  NSR_BREAKDOWN = 2,
+  NSR_DIVERGED = 3,
+  NSR_NONFINITE = 4,
+  NSR_NOT_RUN = 5
+};
+
+/* Library error codes (cudaError_t values stay below 1000). */
+enum {
+  NSR_ERR_ARGUMENT = 1001,       /* null pointer, bad size or bad parameter   */
+  NSR_ERR_UNSUPPORTED_SIZE = 1002, /* nz or nx not 2^a 3^b in [8, 2048]       */
+  NSR_ERR_WORKSPACE = 1003,      /* workspace smaller than the query returned */
+  NSR_ERR_INTERNAL = 1004,       /* solver loop did not drain its queue       */
+  NSR_ERR_CAPACITY = 1005        /* request exceeds a fixed capacity          */
+};
+
+/* Grid, PML and acquisition geometry of one record.  Mirrors the reference
+ * Grid/Solver parameters (theranostic/wave.py:29-125) plus the plane-wave array
+ * row of nsrno/conditioned_wave.py:29-30. */
+typedef struct NsrGrid {
+  int32_t nz, nx;            /* rows (z) and columns (x)                       */
+  int32_t n_pml;             /* PML thickness in nodes on every side           */
+  int32_t face;              /* row of the source line and receivers           */
+  double h;                  /* node spacing [m]                               */
+  double c0;                 /* reference speed for k0 and the PML [m/s]       */
+  double rho0;               /* reference density [kg/m^3]                     */
+  double pml_strength;       /* sigma_max = strength * c0 / (n_pml h)          */
+  double alpha_power;        /* power-law exponent y of alpha [dB/cm/MHz^y]    */
+  double aperture_half_width;/* cosine taper half width of the source line [m] */
+} NsrGrid;
+
+/* Krylov parameters of nsr_solve_batched. */
+typedef struct NsrSolveParams {
+  double tolerance;          /* relative true residual ||b-Ax||/||b||          */
+  double shift;              /* shifted-Laplace preconditioner shift (0.15)    */
+  int32_t max_iterations;    /* BiCGSTAB iterations per system                 */
+  int32_t replace_every;     /* true-residual replacement period (40)          */
+  int32_t n_slots;           /* systems resident at once                       */
+  int32_t adjoint;           /* 0: A x = b; 1: A^H x = b                       */
+  int32_t graph_iterations;  /* iterations per captured CUDA graph (16)        */
+  int32_t profile_iterations;/* first iterations launched one by one with CUDA
+                                events between kernels (0: none); their average
+                                durations are reported in NsrSolveStats          */
+} NsrSolveParams;
+
+/* Optional host-side statistics of one nsr_solve_batched call. */
+typedef struct NsrSolveStats {
+  double loop_ms;            /* device time of the solve loop                   */
+  double kernel_ms[6];       /* mean duration per launch: fwd, cols, inv of the
+                                first half, then of the second half             */
+  int32_t kernel_timed[6];   /* launches averaged in kernel_ms                  */
+  int64_t launches;          /* kernels launched by the call                    */
+  int32_t graph_launches;    /* CUDA graph launches                             */
+  int32_t reserved;
+} NsrSolveStats;
+
+/* Version of this ABI (major * 100 + minor). */
+int nsr_version(void);
+
+/* Text for a return code (status, NSR_ERR_* or cudaError_t). */
+const char* nsr_error_string(int code);
+
+/* Material planes: c [m/s], rho [kg/m^3], alpha [dB/cm/MHz^y] (float, [nz,nx])
+ * -> coef = three float planes [3][nz][nx]: a = rho0/rho (1 + m_eta),
+ * b = rho0 c0^2/(rho c^2) (1 + m_kappa), t = attenuation slope with
+ * e(f) = t (f/1 MHz)^(y-1) = alpha_Np(f) c / omega.  Computed in double and
+ * rounded once.  Replaces the material part of Solver.matrix
+ * (theranostic/wave.py:158-180) and of WaveResidualOperator.setup
+ * (nsrno/wave_operator.py:48-67). */
+int nsr_setup_material(const NsrGrid* grid, const float* c, const float* rho,
+                       const float* alpha_db, float* coef, void* stream);
+
+/* y = A x (adjoint = 0) or A^H x (adjoint = 1) for S systems of frequencies
+ * freq_hz[S] (device, double), fields [S][nz][nx].  A is the h^2-scaled
+ * 5-point operator (the reference matrix of theranostic/wave.py:174-188 times
+ * h^2, with the attenuation mass term).  precision 0: c64 in/out, float math;
+ * precision 1: c128 in/out, double math.  Replaces Solver.matrix @ x and
+ * WaveResidualOperator.apply_operator (nsrno/wave_operator.py:105-109). */
+int nsr_apply(const NsrGrid* grid, const float* coef, const double* freq_hz,
+              int32_t n_systems, int32_t adjoint, int32_t precision,
+              const void* x, void* y, void* stream);
+
+/* y = M^-1 x: the fixed shifted-Laplace preconditioner
+ * M^-1 = IFFT[ 1 / (h^2 L(q) + (k0 h)^2 (1 + i shift)) FFT ], periodic 5-point
+ * Laplacian symbol, c64 fields [S][nz][nx].  Replaces the fixed preconditioner
+ * of nsrno/dense_wave.py:194-196 and conditioned_wave.py:90-92.  Requires
+ * workspace of nsr_precondition_workspace_size bytes. */
+size_t nsr_precondition_workspace_size(const NsrGrid* grid, int32_t n_systems);
+int nsr_precondition(const NsrGrid* grid, const double* freq_hz, int32_t n_systems,
+                     double shift, int32_t adjoint, const float* x, float* y,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Plane-wave right-hand side in SI units, b = -line(x)/h^2 on row `face`,
+ * line = taper(x) exp(-i k0 x sin(theta)) (nsrno/wave_operator.py:111-115 and
+ * theranostic/wave.py:260).  b: c128 [S][nz][nx]. */
+int nsr_plane_wave_rhs(const NsrGrid* grid, const double* freq_hz, const double* angle_rad,
+                       int32_t n_systems, void* b, void* stream);
+
+/* Batched right-preconditioned BiCGSTAB over a queue of S systems held in
+ * params->n_slots resident slots; converged systems retire and their slots
+ * refill.  Replaces solve_system/bicgstab (nsrno/dense_wave.py:118-148,
+ * 167-225) and the GMRES loop of solve_frequency (nsrno/wave_solver.py:38-67)
+ * for whole records.
+ *   coef          material planes from nsr_setup_material
+ *   freq_hz[S]    device double
+ *   angle_rad[S]  device double (plane-wave source; ignored when rhs != NULL)
+ *   rhs           NULL or c64 [S][nz][nx] explicit right-hand sides (SI units)
+ *   x0            NULL or c64 [S][nz][nx] initial fields (warm start)
+ *   rx_index[n_rx] device int32 flat node indices of the receivers
+ * Outputs (device): iq c128 [S][n_rx], residual f64 [S] (true relative
+ * residual, FP64), iterations i32 [S], status i32 [S] (NSR_CONVERGED ...),
+ * fields NULL or c64 [S][nz][nx]; stats NULL or a host NsrSolveStats.
+ * The call synchronises its stream while it polls for completion. */
+size_t nsr_solve_workspace_size(const NsrGrid* grid, int32_t n_slots);
+int nsr_solve_batched(const NsrGrid* grid, const float* coef,
+                      const double* freq_hz, const double* angle_rad, int32_t n_systems,
+                      const float* rhs, const float* x0,
+                      const int32_t* rx_index, int32_t n_rx,
+                      const NsrSolveParams* params,
+                      void* workspace, size_t workspace_bytes,
+                      double* iq, double* residual, int32_t* iterations, int32_t* status,
+                      float* fields, NsrSolveStats* stats, void* stream);
+
+/* g_logc, g_logrho (double [nz][nx]) += -Re(lambda^H dA/dm u) summed over S
+ * systems, u and lambda c64 [S][nz][nx] (SI fields), m = log c and log rho.
+ * The exact derivative of the 5-point discretisation that
+ * theranostic/wave.py:331-389 (born_jacobian) forms column by column and
+ * nsrno/dense_wave.py:250-255 obtains by autograd. */
+int nsr_grad_accum(const NsrGrid* grid, const float* coef, const double* freq_hz,
+                   int32_t n_systems, const float* u, const float* lam,
+                   double* g_logc, double* g_logrho, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NSRNO_B200_H */

@@ -1,0 +1,87 @@
+"""ctypes binding of ``libnsrno_b200.so`` (the C ABI declared in include/nsrno_b200.h).
+
+The reference binds its native kernels the same way (nsrno/native_time.py:25-41:
+``ctypes.CDLL``, integer status codes raised as ``RuntimeError``).  There is no
+fallback: if the library is missing or a call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIBRARY = Path(__file__).resolve().parent / "libnsrno_b200.so"
+
+CONVERGED, ITERATION_BUDGET, BREAKDOWN, DIVERGED, NONFINITE, NOT_RUN = range(6)
+REASONS = {CONVERGED: "converged", ITERATION_BUDGET: "iteration_budget", BREAKDOWN: "breakdown",
+           DIVERGED: "diverged", NONFINITE: "nonfinite", NOT_RUN: "not_run"}
+
+EXPORTS = ("nsr_version", "nsr_error_string", "nsr_setup_material", "nsr_apply",
+           "nsr_precondition_workspace_size", "nsr_precondition", "nsr_plane_wave_rhs",
+           "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_grad_accum")
+
+
+class NsrGrid(ctypes.Structure):
+    _fields_ = [("nz", ctypes.c_int32), ("nx", ctypes.c_int32), ("n_pml", ctypes.c_int32),
+                ("face", ctypes.c_int32), ("h", ctypes.c_double), ("c0", ctypes.c_double),
+                ("rho0", ctypes.c_double), ("pml_strength", ctypes.c_double),
+                ("alpha_power", ctypes.c_double), ("aperture_half_width", ctypes.c_double)]
+
+
+class NsrSolveParams(ctypes.Structure):
+    _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double),
+                ("max_iterations", ctypes.c_int32), ("replace_every", ctypes.c_int32),
+                ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
+                ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32)]
+
+
+class NsrSolveStats(ctypes.Structure):
+    _fields_ = [("loop_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double * 6),
+                ("kernel_timed", ctypes.c_int32 * 6), ("launches", ctypes.c_int64),
+                ("graph_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    KERNELS = ("fwd_h0", "cols_h0", "inv_h0", "fwd_h1", "cols_h1", "inv_h1")
+
+    def as_dict(self):
+        return dict(loop_ms=self.loop_ms, launches=int(self.launches), graph_launches=int(self.graph_launches),
+                    kernel_ms={k: self.kernel_ms[i] for i, k in enumerate(self.KERNELS)},
+                    kernel_timed={k: int(self.kernel_timed[i]) for i, k in enumerate(self.KERNELS)})
+
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIBRARY.exists():
+        raise RuntimeError(f"{LIBRARY} is missing: run `python -m nsrno_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(str(LIBRARY))
+    P, I, D, S = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_size_t
+    G = ctypes.POINTER(NsrGrid)
+    lib.nsr_version.restype = ctypes.c_int
+    lib.nsr_error_string.restype = ctypes.c_char_p
+    lib.nsr_error_string.argtypes = [ctypes.c_int]
+    lib.nsr_setup_material.argtypes = [G, P, P, P, P, P]
+    lib.nsr_apply.argtypes = [G, P, P, I, I, I, P, P, P]
+    lib.nsr_precondition_workspace_size.restype = S
+    lib.nsr_precondition_workspace_size.argtypes = [G, I]
+    lib.nsr_precondition.argtypes = [G, P, I, D, I, P, P, P, S, P]
+    lib.nsr_plane_wave_rhs.argtypes = [G, P, P, I, P, P]
+    lib.nsr_solve_workspace_size.restype = S
+    lib.nsr_solve_workspace_size.argtypes = [G, I]
+    lib.nsr_solve_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrSolveParams),
+                                      P, S, P, P, P, P, P, ctypes.POINTER(NsrSolveStats), P]
+    lib.nsr_grad_accum.argtypes = [G, P, P, I, P, P, P, P, P]
+    for name in EXPORTS:
+        getattr(lib, name)
+    _lib = lib
+    return lib
+
+
+def check(code):
+    """Raise ``RuntimeError(nsr_error_string(code))`` for a non-zero return code."""
+    if code:
+        raise RuntimeError(load().nsr_error_string(int(code)).decode())
+    return code

@@ -1,0 +1,237 @@
+"""Reference-facing entry points: drop-ins for the frequency-domain solve of NSRNO.
+
+* :func:`solve_frequency` mirrors ``nsrno.wave_solver.solve_frequency``
+  (nsrno/wave_solver.py:38-67): one medium, one frequency, one angle ->
+  ``(receiver spectrum, status)``; raises ``ValueError`` on ``requires_grad`` or
+  when ``max_iterations`` is not a positive multiple of ``restart``.
+* :func:`solve_system` mirrors ``nsrno.dense_wave.solve_system``
+  (nsrno/dense_wave.py:167-225): ``(x, info)`` with ``reason``, ``steps``,
+  ``residual``, ``max_angle_residual``, ``seconds``, ``dtype``, ``method``.
+* :class:`ImplicitChannels` / :func:`implicit_channels` mirror
+  nsrno/dense_wave.py:227-259: a converged forward solve, receiver channels
+  times the receive response, and an implicit adjoint gradient w.r.t. the
+  medium ``[2, h, w] = (c, rho)``.
+* :class:`HelmholtzSurrogate` mirrors ``DenseSurrogate``
+  (nsrno/dense_surrogate.py:9-36): ``forward`` (differentiable) and ``truncated``.
+
+All solves run on the GPU through ``libnsrno_b200.so``.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .solver import (DEFAULT_REPLACE, DEFAULT_SHIFT, Geometry, Medium, apply, grad_accum, plane_wave_rhs,
+                     receiver_response, solve_batched)
+
+V5_CLOCK_HZ = 40e6
+V5_SAMPLES = 2401
+
+
+def bin_frequency(frequency_bin):
+    """Frequency of a V5 record bin: ``bin * 40 MHz / 2401`` (nsrno/dense_wave.py:49)."""
+    return frequency_bin * V5_CLOCK_HZ / V5_SAMPLES
+
+
+class PlaneWaveModel:
+    """Acquisition model for :func:`solve_frequency`: a geometry, its angles and a known alpha map.
+
+    Stands in for the ``model`` argument of the reference (a
+    ``WaveResidualOperator``), which carries the grid, the receiver columns and
+    the angle table (nsrno/wave_operator.py:14-45).
+    """
+
+    def __init__(self, geometry: Geometry, angles_deg, alpha=None, warm_start=None):
+        self.geometry = geometry
+        self.angles = np.deg2rad(np.asarray(angles_deg, dtype=np.float64))
+        self.alpha = alpha
+        self.warm_start = warm_start
+        self.iterations = 0 if warm_start is None else getattr(warm_start, "iterations", 1)
+
+    def eval(self):
+        return self
+
+
+@torch.no_grad()
+def solve_frequency(model: PlaneWaveModel, medium, frequency_hz, angle_index, tolerance=1e-4,
+                    max_iterations=2560, restart=32):
+    """Receiver spectrum and measured convergence status of one (frequency, angle) solve.
+
+    ``medium`` is ``[1, 2, nz, nx]`` (c, rho).  ``restart`` keeps the reference
+    signature; here it is the true-residual replacement period of BiCGSTAB.
+    """
+    if isinstance(medium, torch.Tensor) and medium.requires_grad:
+        raise ValueError("This reference has no implicit-adjoint backward; use the neural forward for input gradients.")
+    if max_iterations < restart or max_iterations % restart:
+        raise ValueError("max_iterations must be a positive multiple of restart")
+    started = time.perf_counter()
+    g = model.geometry
+    medium = torch.as_tensor(medium)
+    if medium.dim() != 4 or medium.shape[0] != 1 or medium.shape[1] != 2:
+        raise ValueError("One native medium per frequency solve: expected [1, 2, nz, nx]")
+    dev = medium.device if medium.is_cuda else torch.device("cuda")
+    alpha = model.alpha if model.alpha is not None else torch.zeros((g.nz, g.nx))
+    med = Medium(g, medium[0, 0], medium[0, 1], alpha, device=dev)
+    x0 = None
+    if model.warm_start is not None:
+        x0 = model.warm_start(med, [frequency_hz], [model.angles[angle_index]])
+    res = solve_batched(med, [frequency_hz], [model.angles[angle_index]], x0=x0, tolerance=tolerance,
+                        max_iterations=max_iterations, replace_every=restart, n_slots=1)
+    status = int(res.status[0])
+    reason = "converged" if status == _lib.CONVERGED else "iteration_budget"
+    iters = int(res.iterations[0])
+    rel = float(res.residual[0])
+    prediction = res.iq[0].to(torch.complex64)
+    return prediction, dict(reason=reason, initial_neural_iterations=model.iterations,
+                            solver_iterations=iters, relative_residual=rel,
+                            seconds=time.perf_counter() - started,
+                            trace=[dict(iterations=iters, relative_residual=rel)],
+                            status=_lib.REASONS[status])
+
+
+class HelmholtzSystem:
+    """One medium at one frequency: the ``system`` argument of :func:`solve_system`."""
+
+    def __init__(self, medium: Medium, frequency_hz: float):
+        self.medium = medium
+        self.frequency = float(frequency_hz)
+
+    @property
+    def geometry(self):
+        return self.medium.geometry
+
+
+@torch.no_grad()
+def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=False, tolerance=1e-5,
+                 max_cycles=100, warm_steps=8, mixed=False, method="bicgstab", initial=None,
+                 max_iterations=None):
+    """Solve ``A x = rhs`` (or ``A^H x = rhs``) for a batch of angles sharing one operator.
+
+    ``rhs`` is ``[A, nz, nx]`` complex (SI units).  The angle batch shares one
+    frequency like the reference; every angle is its own Krylov system here and
+    ``max_angle_residual`` is the largest of them.  ``residual`` is the
+    combined ``||R|| / ||B||`` over all angles, as the reference measures it
+    (nsrno/dense_wave.py:221-225).
+    """
+    started = time.perf_counter()
+    med = system.medium
+    g = med.geometry
+    rhs = torch.as_tensor(rhs)
+    squeeze = rhs.dim() == 2
+    if squeeze:
+        rhs = rhs[None]
+    if rhs.dim() != 3 or tuple(rhs.shape[1:]) != (g.nz, g.nx):
+        raise ValueError("rhs must be [A, nz, nx]")
+    A = rhs.shape[0]
+    b = rhs.to(med.device, torch.complex64).contiguous()
+    x0 = None if initial is None else torch.as_tensor(initial).to(med.device, torch.complex64).reshape(b.shape).contiguous()
+    if max_iterations is None:
+        max_iterations = max_cycles * 24
+    res = solve_batched(med, [system.frequency] * A, rhs=b, x0=x0, tolerance=tolerance,
+                        max_iterations=max_iterations, adjoint=adjoint, return_fields=True, n_slots=A)
+    bn = torch.linalg.vector_norm(rhs.reshape(A, -1).to(torch.complex128), dim=1).to(res.residual.device)
+    combined = float(torch.sqrt((res.residual.square() * bn.square()).sum() / bn.square().sum().clamp_min(1e-300)))
+    statuses = [int(s) for s in res.status.cpu()]
+    reason = "converged" if all(s == _lib.CONVERGED for s in statuses) else _lib.REASONS[max(statuses)]
+    x = res.fields.to(torch.complex128)
+    if squeeze:
+        x = x[0]
+    return x, {"reason": reason, "steps": int(res.iterations.sum()) * 2, "residual": combined,
+               "max_angle_residual": float(res.residual.max()), "seconds": time.perf_counter() - started,
+               "dtype": "complex64 Krylov / FP64 residual", "method": "BiCGSTAB",
+               "iterations": [int(i) for i in res.iterations.cpu()]}
+
+
+class AcquisitionData:
+    """The ``data`` argument of :func:`implicit_channels`: geometry, angle table, response."""
+
+    def __init__(self, geometry: Geometry, angles_deg, response=True):
+        self.geometry = geometry
+        self.angles = np.deg2rad(np.asarray(angles_deg, dtype=np.float64))
+        self.response = response
+
+    def channel_response(self, frequency_hz):
+        return receiver_response(float(frequency_hz)) if self.response else 1.0
+
+
+class ImplicitChannels(torch.autograd.Function):
+    """Converged channels with an implicit adjoint (nsrno/dense_wave.py:227-256)."""
+
+    @staticmethod
+    def forward(ctx, medium, alpha, data, frequency_hz, angles, tolerance, max_iterations):
+        g = data.geometry
+        med = Medium(g, medium[0].detach(), medium[1].detach(), alpha.detach(), device=medium.device)
+        th = [data.angles[a] for a in angles]
+        res = solve_batched(med, [frequency_hz] * len(th), th, tolerance=tolerance, max_iterations=max_iterations,
+                            return_fields=True, n_slots=len(th))
+        bad = [i for i, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
+        if bad:
+            raise RuntimeError("Forward failed to converge: " + str({"reasons": res.reasons(),
+                                                                      "residual": res.residual.tolist()}))
+        resp = data.channel_response(frequency_hz)
+        ctx.data, ctx.frequency, ctx.angles, ctx.tolerance, ctx.max_iterations = data, frequency_hz, th, tolerance, max_iterations
+        ctx.med = med
+        ctx.resp = resp
+        ctx.save_for_backward(medium, res.fields)
+        out = res.iq * resp
+        return out.to(torch.complex128)
+
+    @staticmethod
+    def backward(ctx, gradient):
+        medium, u = ctx.saved_tensors
+        data, med = ctx.data, ctx.med
+        g = data.geometry
+        A = len(ctx.angles)
+        with torch.no_grad():
+            rhs = torch.zeros((A, g.nz, g.nx), dtype=torch.complex64, device=medium.device)
+            rx = torch.as_tensor(np.asarray(g.rx_cols), device=medium.device)
+            rhs[:, g.face, rx] = (gradient * ctx.resp).to(torch.complex64)
+            res = solve_batched(med, [ctx.frequency] * A, rhs=rhs, tolerance=ctx.tolerance,
+                                max_iterations=ctx.max_iterations, adjoint=True, return_fields=True, n_slots=A)
+            bad = [i for i, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
+            if bad:
+                raise RuntimeError("Adjoint failed to converge: " + str({"reasons": res.reasons(),
+                                                                          "residual": res.residual.tolist()}))
+            g_logc, g_logrho = grad_accum(med, [ctx.frequency] * A, u, res.fields)
+            grad = torch.stack((g_logc / med.c.double(), g_logrho / med.rho.double())).to(medium.dtype)
+        return grad, None, None, None, None, None, None
+
+
+def implicit_channels(medium, alpha, data, frequency_hz, angles, tolerance=1e-5, max_iterations=4000):
+    """Differentiable converged receiver channels ``[A, n_rx]`` (complex128)."""
+    return ImplicitChannels.apply(medium, alpha, data, frequency_hz, list(angles), tolerance, max_iterations)
+
+
+class HelmholtzSurrogate(torch.nn.Module):
+    """Drop-in for ``DenseSurrogate`` (nsrno/dense_surrogate.py:9-36) on a synthetic record."""
+
+    def __init__(self, geometry: Geometry, angles_deg, bins=None, response=True, device="cuda"):
+        super().__init__()
+        self.data = AcquisitionData(geometry, angles_deg, response=response)
+        self.bins = list(range(241, 535)) if bins is None else list(bins)
+        self.device = torch.device(device)
+
+    def forward(self, medium, alpha, frequency_bin, angles=None, tolerance=1e-5):
+        if frequency_bin not in self.bins:
+            raise ValueError("Frequency outside cached dense band")
+        angles = list(range(len(self.data.angles))) if angles is None else list(angles)
+        return implicit_channels(medium, alpha, self.data, bin_frequency(frequency_bin), angles, tolerance)
+
+    @torch.no_grad()
+    def truncated(self, medium, alpha, frequency_bin, angles=None, iterations=32):
+        """Channels after a fixed number of iterations and their actual residual."""
+        if frequency_bin not in self.bins:
+            raise ValueError("Frequency outside cached dense band")
+        angles = list(range(len(self.data.angles))) if angles is None else list(angles)
+        g = self.data.geometry
+        med = Medium(g, medium[0], medium[1], alpha, device=medium.device)
+        f = bin_frequency(frequency_bin)
+        th = [self.data.angles[a] for a in angles]
+        res = solve_batched(med, [f] * len(th), th, tolerance=1e-30, max_iterations=iterations, n_slots=len(th))
+        resp = self.data.channel_response(f)
+        rel = float(res.residual.max())
+        return (res.iq * resp).to(torch.complex128), rel

@@ -1,0 +1,295 @@
+// Shared device code of the nsrno_b200 library: complex arithmetic, the PML
+// geometry, the h^2-scaled 5-point viscoacoustic Helmholtz stencil and a
+// shared-memory mixed-radix FFT used by the shifted-Laplace preconditioner.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "nsrno_b200.h"
+
+#define NSR_MAX_RADIX_STAGES 12
+#define NSR_MAX_LINE 2048
+#define NSR_PI 3.14159265358979323846
+
+// ---------------------------------------------------------------------------
+// Complex helpers on float2 / double2.
+// ---------------------------------------------------------------------------
+template <typename T> struct CxT;
+template <> struct CxT<float> { typedef float2 type; };
+template <> struct CxT<double> { typedef double2 type; };
+
+template <typename C> __host__ __device__ __forceinline__ C cx(decltype(C::x) re, decltype(C::x) im) {
+  C z; z.x = re; z.y = im; return z;
+}
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 operator*(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 operator*(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__host__ __device__ __forceinline__ float2 conjc(float2 a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ double2 conjc(double2 a) { return make_double2(a.x, -a.y); }
+__host__ __device__ __forceinline__ float2 divc(float2 a, float2 b) {
+  float d = 1.0f / (b.x * b.x + b.y * b.y);
+  return make_float2((a.x * b.x + a.y * b.y) * d, (a.y * b.x - a.x * b.y) * d);
+}
+__host__ __device__ __forceinline__ double2 divc(double2 a, double2 b) {
+  double d = 1.0 / (b.x * b.x + b.y * b.y);
+  return make_double2((a.x * b.x + a.y * b.y) * d, (a.y * b.x - a.x * b.y) * d);
+}
+__host__ __device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+__host__ __device__ __forceinline__ float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
+// conj(a) * b accumulated in double
+__device__ __forceinline__ void dot_acc(double& re, double& im, float2 a, float2 b) {
+  re += (double)a.x * b.x + (double)a.y * b.y;
+  im += (double)a.x * b.y - (double)a.y * b.x;
+}
+
+// ---------------------------------------------------------------------------
+// Geometry.  Index-space form of Solver._stretch (theranostic/wave.py:127-135):
+// the fraction max((lower + w - x)/w, (x - upper + w)/w) with x = x0 + pos*h
+// and w = n_pml*h becomes max(n_pml - pos, pos - (n-1-n_pml)) / n_pml.
+// ---------------------------------------------------------------------------
+struct Geo {
+  int nz, nx, n_pml, face;
+  double h, c0, rho0, strength, alpha_power, ap_half;
+};
+
+__host__ __device__ __forceinline__ Geo make_geo(const NsrGrid& g) {
+  Geo o;
+  o.nz = g.nz; o.nx = g.nx; o.n_pml = g.n_pml; o.face = g.face;
+  o.h = g.h; o.c0 = g.c0; o.rho0 = g.rho0; o.strength = g.pml_strength;
+  o.alpha_power = g.alpha_power; o.ap_half = g.aperture_half_width;
+  return o;
+}
+
+template <typename T>
+__device__ __forceinline__ T pml_profile(T pos, int n, int n_pml) {
+  if (n_pml <= 0) return T(0);
+  T f = fmax(T(n_pml) - pos, pos - T(n - 1 - n_pml)) / T(n_pml);
+  f = fmin(fmax(f, T(0)), T(1));
+  return f * f;
+}
+
+// Per-system scalars of one frequency.
+struct SysScalars {
+  double kh2;    // (k0 h)^2
+  double sig;    // sigma_max / omega (stretch = 1 + i sig * profile)
+  double fpow;   // (f / 1 MHz)^(y - 1)
+  double k0;     // omega / c0
+};
+
+__host__ __device__ __forceinline__ SysScalars sys_scalars(const Geo& g, double f) {
+  SysScalars s;
+  double omega = 2.0 * NSR_PI * f;
+  s.k0 = omega / g.c0;
+  s.kh2 = (s.k0 * g.h) * (s.k0 * g.h);
+  s.sig = g.n_pml > 0 ? g.strength * g.c0 / (g.n_pml * g.h) / omega : 0.0;
+  s.fpow = pow(f / 1e6, g.alpha_power - 1.0);
+  return s;
+}
+
+// h^2-scaled stencil at node (i, j).  `P` fetches the field at (i2, j2) and
+// returns zero outside the grid (the reference's zero ghost,
+// theranostic/wave.py:109-115); `A` fetches the inverse-density ratio a and
+// returns 1 outside (zero ghost contrast).  Fluxes follow
+// theranostic/wave.py:150-155,179: stretch * (a_i + a_j) / 2; the mass term is
+// theranostic/wave.py:180 times the attenuation factor (1 + i e)^2.
+template <typename T, bool ADJ, typename FP, typename FA>
+__device__ __forceinline__ typename CxT<T>::type stencil(const Geo& g, const SysScalars& s, int i, int j,
+                                                         T b_c, T t_c, FP P, FA A) {
+  typedef typename CxT<T>::type C;
+  const T sig = (T)s.sig;
+  const T a_c = A(i, j);
+  const C pc = P(i, j);
+  // stretches at nodes and half nodes
+  const C sx = cx<C>(T(1), sig * pml_profile<T>(T(j), g.nx, g.n_pml));
+  const C sz = cx<C>(T(1), sig * pml_profile<T>(T(i), g.nz, g.n_pml));
+  const C sxe = cx<C>(T(1), sig * pml_profile<T>(T(j) + T(0.5), g.nx, g.n_pml));
+  const C sxw = cx<C>(T(1), sig * pml_profile<T>(T(j) - T(0.5), g.nx, g.n_pml));
+  const C szs = cx<C>(T(1), sig * pml_profile<T>(T(i) + T(0.5), g.nz, g.n_pml));
+  const C szn = cx<C>(T(1), sig * pml_profile<T>(T(i) - T(0.5), g.nz, g.n_pml));
+  C fe = T(0.5) * (a_c + A(i, j + 1)) * divc(sz, sxe);
+  C fw = T(0.5) * (a_c + A(i, j - 1)) * divc(sz, sxw);
+  C fs = T(0.5) * (a_c + A(i + 1, j)) * divc(sx, szs);
+  C fn = T(0.5) * (a_c + A(i - 1, j)) * divc(sx, szn);
+  const T e = t_c * (T)s.fpow;
+  C loss = cx<C>(T(1) - e * e, T(2) * e);
+  C mass = ((T)s.kh2 * b_c) * ((sx * sz) * loss);
+  if (ADJ) { fe = conjc(fe); fw = conjc(fw); fs = conjc(fs); fn = conjc(fn); mass = conjc(mass); }
+  C y = mass * pc;
+  y = y + fe * (P(i, j + 1) - pc);
+  y = y + fw * (P(i, j - 1) - pc);
+  y = y + fs * (P(i + 1, j) - pc);
+  y = y + fn * (P(i - 1, j) - pc);
+  return y;
+}
+
+// Plane-wave source line value at column j (SI line amplitude, no 1/h^2):
+// taper(x) exp(-i k0 x sin(theta)), nsrno/wave_operator.py:114-115.
+__device__ __forceinline__ double2 source_line(const Geo& g, double k0, double sin_theta, int j) {
+  double x = (j - 0.5 * (g.nx - 1)) * g.h;
+  if (fabs(x) > g.ap_half || g.ap_half <= 0.0) return make_double2(0.0, 0.0);
+  double taper = 0.5 * (1.0 + cos(NSR_PI * x / g.ap_half));
+  double sn, cs;
+  sincos(-k0 * x * sin_theta, &sn, &cs);
+  return make_double2(taper * cs, taper * sn);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-radix FFT along lines held in shared memory.
+//
+// Forward transforms are decimation-in-frequency (natural order in,
+// digit-reversed order out); inverse transforms are the exact stage-by-stage
+// inverse (digit-reversed in, natural out, unnormalised).  The preconditioner
+// multiplies in the digit-reversed domain, so no reordering pass is needed.
+// ---------------------------------------------------------------------------
+struct FftPlan {
+  int n;
+  int nst;
+  int radix[NSR_MAX_RADIX_STAGES];
+  const float2* tw;   // tw[k] = exp(-2 pi i k / n), k < n
+};
+
+template <int R, bool INV>
+__device__ __forceinline__ void small_dft(float2* x) {
+  if (R == 2) {
+    float2 a = x[0], b = x[1];
+    x[0] = a + b; x[1] = a - b;
+  } else if (R == 3) {
+    const float h3 = 0.86602540378443864676f;
+    float2 t1 = x[1] + x[2];
+    float2 t2 = x[0] - 0.5f * t1;
+    float2 d = x[1] - x[2];
+    // forward: t3 = -i (sqrt3/2) d ; inverse: +i (sqrt3/2) d
+    float2 t3 = INV ? make_float2(-h3 * d.y, h3 * d.x) : make_float2(h3 * d.y, -h3 * d.x);
+    x[0] = x[0] + t1; x[1] = t2 + t3; x[2] = t2 - t3;
+  } else if (R == 4) {
+    float2 a = x[0] + x[2], b = x[0] - x[2], c = x[1] + x[3], e = x[1] - x[3];
+    float2 d = INV ? make_float2(-e.y, e.x) : make_float2(e.y, -e.x);
+    x[0] = a + c; x[2] = a - c; x[1] = b + d; x[3] = b - d;
+  } else if (R == 8) {
+    float2 ev[4] = {x[0], x[2], x[4], x[6]};
+    float2 od[4] = {x[1], x[3], x[5], x[7]};
+    small_dft<4, INV>(ev);
+    small_dft<4, INV>(od);
+    const float r2 = 0.70710678118654752440f;
+    // W8^k = exp(-+ i pi k / 4)
+    float2 w1 = INV ? make_float2(r2, r2) : make_float2(r2, -r2);
+    float2 w2 = INV ? make_float2(0.f, 1.f) : make_float2(0.f, -1.f);
+    float2 w3 = INV ? make_float2(-r2, r2) : make_float2(-r2, -r2);
+    float2 o1 = w1 * od[1], o2 = w2 * od[2], o3 = w3 * od[3];
+    x[0] = ev[0] + od[0]; x[4] = ev[0] - od[0];
+    x[1] = ev[1] + o1;    x[5] = ev[1] - o1;
+    x[2] = ev[2] + o2;    x[6] = ev[2] - o2;
+    x[3] = ev[3] + o3;    x[7] = ev[3] - o3;
+  }
+}
+
+// One DIF stage (forward) or its inverse over `nl` lines.
+// Element k of line l lives at s[l*lstride + k*estride].  When `line_fast`
+// the thread index runs over lines first (columns held side by side in
+// shared memory), otherwise over butterflies of one line first (rows).
+template <int R, bool INV>
+__device__ __forceinline__ void fft_stage(float2* s, int nl, int lstride, int estride, bool line_fast,
+                                          const FftPlan& P, int L) {
+  const int m = L / R;
+  const int per_line = P.n / R;
+  const int nb = nl * per_line;
+  const int tstep = P.n / L;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    int l, bb;
+    if (line_fast) { l = b % nl; bb = b / nl; } else { l = b / per_line; bb = b % per_line; }
+    const int o = bb / m, j = bb - o * m;
+    float2* base = s + l * lstride + (o * L + j) * estride;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = base[q * m * estride];
+    if (!INV) {
+      small_dft<R, false>(v);
+#pragma unroll
+      for (int k = 1; k < R; ++k) v[k] = v[k] * __ldg(&P.tw[j * k * tstep]);
+    } else {
+#pragma unroll
+      for (int k = 1; k < R; ++k) v[k] = v[k] * conjc(__ldg(&P.tw[j * k * tstep]));
+      small_dft<R, true>(v);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) base[q * m * estride] = v[q];
+  }
+}
+
+template <bool INV>
+__device__ void fft_lines(float2* s, int nl, int lstride, int estride, bool line_fast, const FftPlan& P) {
+  if (!INV) {
+    int L = P.n;
+    for (int st = 0; st < P.nst; ++st) {
+      const int R = P.radix[st];
+      switch (R) {
+        case 2: fft_stage<2, false>(s, nl, lstride, estride, line_fast, P, L); break;
+        case 3: fft_stage<3, false>(s, nl, lstride, estride, line_fast, P, L); break;
+        case 4: fft_stage<4, false>(s, nl, lstride, estride, line_fast, P, L); break;
+        default: fft_stage<8, false>(s, nl, lstride, estride, line_fast, P, L); break;
+      }
+      __syncthreads();
+      L /= R;
+    }
+  } else {
+    // Lengths of the forward stages, replayed backwards.
+    int Ls[NSR_MAX_RADIX_STAGES];
+    int L = P.n;
+    for (int st = 0; st < P.nst; ++st) { Ls[st] = L; L /= P.radix[st]; }
+    for (int st = P.nst - 1; st >= 0; --st) {
+      const int R = P.radix[st];
+      switch (R) {
+        case 2: fft_stage<2, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+        case 3: fft_stage<3, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+        case 4: fft_stage<4, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+        default: fft_stage<8, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Host-side radix plan: n = 2^a 3^b, 8 <= n <= 2048.  Powers of two are split
+// into 8s with 4s and 2s so that stages stay balanced (1024 = 8*8*4*4).
+__host__ __device__ inline bool nsr_make_radices(int n, int* radix, int* nst) {
+  if (n < 8 || n > NSR_MAX_LINE) return false;
+  int a = 0, b = 0, m = n;
+  while (m % 2 == 0) { m /= 2; ++a; }
+  while (m % 3 == 0) { m /= 3; ++b; }
+  if (m != 1) return false;
+  int k = 0;
+  for (int i = 0; i < b; ++i) radix[k++] = 3;
+  int eights = a / 3, rem = a % 3;
+  if (rem == 1 && eights > 0) { eights -= 1; radix[k++] = 4; radix[k++] = 4; rem = 0; }
+  for (int i = 0; i < eights; ++i) radix[k++] = 8;
+  if (rem == 2) radix[k++] = 4;
+  if (rem == 1) radix[k++] = 2;
+  if (k > NSR_MAX_RADIX_STAGES) return false;
+  *nst = k;
+  return true;
+}
+
+// Frequency index held at DIF output position p (mixed-radix digit reversal).
+__host__ __device__ inline int nsr_digit_reverse(int p, int n, const int* radix, int nst) {
+  int freq = 0, scale = 1, L = n;
+  for (int st = 0; st < nst; ++st) {
+    int m = L / radix[st];
+    int k = p / m;
+    p -= k * m;
+    freq += k * scale;
+    scale *= radix[st];
+    L = m;
+  }
+  return freq;
+}

@@ -1,0 +1,384 @@
+// Stand-alone operators of the nsrno_b200 C ABI: material planes, the 5-point
+// operator apply, the FFT shifted-Laplace preconditioner, plane-wave
+// right-hand sides and the adjoint-state material gradient.
+#include "nsr_common.cuh"
+#include "nsr_internal.cuh"
+
+#include <string.h>
+
+// ---------------------------------------------------------------------------
+// Error strings and argument checks.
+// ---------------------------------------------------------------------------
+extern "C" int nsr_version(void) { return 100; }
+
+extern "C" const char* nsr_error_string(int code) {
+  switch (code) {
+    case 0: return "ok";
+    case NSR_ERR_ARGUMENT: return "nsrno_b200: invalid argument";
+    case NSR_ERR_UNSUPPORTED_SIZE: return "nsrno_b200: nz and nx must be 2^a 3^b between 8 and 2048";
+    case NSR_ERR_WORKSPACE: return "nsrno_b200: workspace too small";
+    case NSR_ERR_INTERNAL: return "nsrno_b200: solver queue did not drain";
+    case NSR_ERR_CAPACITY: return "nsrno_b200: request exceeds the fixed capacity";
+    default: break;
+  }
+  if (code > 0 && code < 1000) return cudaGetErrorString((cudaError_t)code);
+  return "nsrno_b200: unknown error";
+}
+
+int nsr_check_grid(const NsrGrid* g, bool need_fft) {
+  if (!g) return NSR_ERR_ARGUMENT;
+  if (g->nz < 3 || g->nx < 3 || g->n_pml < 0 || 2 * g->n_pml >= g->nz || 2 * g->n_pml >= g->nx) return NSR_ERR_ARGUMENT;
+  if (!(g->h > 0) || !(g->c0 > 0) || !(g->rho0 > 0) || !(g->pml_strength >= 0)) return NSR_ERR_ARGUMENT;
+  if (g->face < 0 || g->face >= g->nz) return NSR_ERR_ARGUMENT;
+  if ((long long)g->nz * g->nx > (1LL << 30)) return NSR_ERR_ARGUMENT;
+  if (need_fft) {
+    int r[NSR_MAX_RADIX_STAGES], k;
+    if (!nsr_make_radices(g->nz, r, &k) || !nsr_make_radices(g->nx, r, &k)) return NSR_ERR_UNSUPPORTED_SIZE;
+  }
+  return 0;
+}
+
+static inline int last_error() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
+// ---------------------------------------------------------------------------
+// Material planes.
+// ---------------------------------------------------------------------------
+__global__ void k_setup_material(Geo g, const float* __restrict__ c, const float* __restrict__ rho,
+                                 const float* __restrict__ alpha, float* __restrict__ coef, long long n) {
+  const double neper = 100.0 * 2.302585092994045684 / 20.0;  // dB/cm -> Np/m
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    double cc = c[k], rr = rho[k], al = alpha[k];
+    coef[k] = (float)(g.rho0 / rr);
+    coef[n + k] = (float)(g.rho0 * g.c0 * g.c0 / (rr * cc * cc));
+    coef[2 * n + k] = (float)(al * neper * cc / (2.0 * NSR_PI * 1e6));
+  }
+}
+
+extern "C" int nsr_setup_material(const NsrGrid* grid, const float* c, const float* rho,
+                                  const float* alpha_db, float* coef, void* stream) {
+  int err = nsr_check_grid(grid, false);
+  if (err) return err;
+  if (!c || !rho || !alpha_db || !coef) return NSR_ERR_ARGUMENT;
+  long long n = (long long)grid->nz * grid->nx;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_setup_material<<<blocks, 256, 0, (cudaStream_t)stream>>>(make_geo(*grid), c, rho, alpha_db, coef, n);
+  return last_error();
+}
+
+// ---------------------------------------------------------------------------
+// Operator apply (one thread per node; used for checks and true residuals).
+// ---------------------------------------------------------------------------
+template <typename T, bool ADJ>
+__global__ void k_apply(Geo g, const float* __restrict__ coef, const double* __restrict__ freq,
+                        const typename CxT<T>::type* __restrict__ x, typename CxT<T>::type* __restrict__ y) {
+  typedef typename CxT<T>::type C;
+  const long long n = (long long)g.nz * g.nx;
+  const int sysi = blockIdx.y;
+  const SysScalars s = sys_scalars(g, freq[sysi]);
+  const C* xs = x + sysi * n;
+  const float* ca = coef;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.nx), j = (int)(k - (long long)i * g.nx);
+    auto P = [&](int i2, int j2) -> C {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return cx<C>(T(0), T(0));
+      return xs[(long long)i2 * g.nx + j2];
+    };
+    auto A = [&](int i2, int j2) -> T {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return T(1);
+      return (T)ca[(long long)i2 * g.nx + j2];
+    };
+    y[sysi * n + k] = stencil<T, ADJ>(g, s, i, j, (T)coef[n + k], (T)coef[2 * n + k], P, A);
+  }
+}
+
+extern "C" int nsr_apply(const NsrGrid* grid, const float* coef, const double* freq_hz,
+                         int32_t n_systems, int32_t adjoint, int32_t precision,
+                         const void* x, void* y, void* stream) {
+  int err = nsr_check_grid(grid, false);
+  if (err) return err;
+  if (!coef || !freq_hz || !x || !y || n_systems < 0 || n_systems > 65535) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;
+  long long n = (long long)grid->nz * grid->nx;
+  int bx = (int)((n + 255) / 256);
+  if (bx > 4096) bx = 4096;
+  dim3 gridd(bx, n_systems);
+  cudaStream_t st = (cudaStream_t)stream;
+  Geo g = make_geo(*grid);
+  if (precision == 0) {
+    if (adjoint) k_apply<float, true><<<gridd, 256, 0, st>>>(g, coef, freq_hz, (const float2*)x, (float2*)y);
+    else k_apply<float, false><<<gridd, 256, 0, st>>>(g, coef, freq_hz, (const float2*)x, (float2*)y);
+  } else if (precision == 1) {
+    if (adjoint) k_apply<double, true><<<gridd, 256, 0, st>>>(g, coef, freq_hz, (const double2*)x, (double2*)y);
+    else k_apply<double, false><<<gridd, 256, 0, st>>>(g, coef, freq_hz, (const double2*)x, (double2*)y);
+  } else {
+    return NSR_ERR_ARGUMENT;
+  }
+  return last_error();
+}
+
+// ---------------------------------------------------------------------------
+// Preconditioner tables and passes (shared with the solver).
+// ---------------------------------------------------------------------------
+__global__ void k_fft_tables(int n, FftPlan plan, float2* tw, float* s2) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincospi(-2.0 * k / n, &sn, &cs);
+    tw[k] = make_float2((float)cs, (float)sn);
+    int f = nsr_digit_reverse(k, n, plan.radix, plan.nst);
+    double sp = sinpi((double)f / n);
+    s2[k] = (float)(sp * sp);
+  }
+}
+
+int nsr_prec_setup(const NsrGrid* g, PrecTables* t, void* table_mem, cudaStream_t st) {
+  char* p = (char*)table_mem;
+  t->px.n = g->nx;
+  t->pz.n = g->nz;
+  if (!nsr_make_radices(g->nx, t->px.radix, &t->px.nst)) return NSR_ERR_UNSUPPORTED_SIZE;
+  if (!nsr_make_radices(g->nz, t->pz.radix, &t->pz.nst)) return NSR_ERR_UNSUPPORTED_SIZE;
+  float2* twx = (float2*)p; p += nsr_align(sizeof(float2) * g->nx);
+  float2* twz = (float2*)p; p += nsr_align(sizeof(float2) * g->nz);
+  float* s2x = (float*)p; p += nsr_align(sizeof(float) * g->nx);
+  float* s2z = (float*)p; p += nsr_align(sizeof(float) * g->nz);
+  t->px.tw = twx; t->pz.tw = twz; t->s2x = s2x; t->s2z = s2z;
+  k_fft_tables<<<(g->nx + 255) / 256, 256, 0, st>>>(g->nx, t->px, twx, s2x);
+  k_fft_tables<<<(g->nz + 255) / 256, 256, 0, st>>>(g->nz, t->pz, twz, s2z);
+  return last_error();
+}
+
+size_t nsr_prec_table_bytes(const NsrGrid* g) {
+  return nsr_align(sizeof(float2) * g->nx) + nsr_align(sizeof(float2) * g->nz) +
+         nsr_align(sizeof(float) * g->nx) + nsr_align(sizeof(float) * g->nz);
+}
+
+// Column pass: forward DIF along z, multiply by the shifted-Laplace symbol in
+// the digit-reversed domain, inverse along z.  In place on w.
+__global__ void __launch_bounds__(256) k_prec_cols(Geo g, PrecTables t, const double* __restrict__ freq,
+                                                   const int* __restrict__ sys_of_slot, float2* __restrict__ w,
+                                                   double shift, int adjoint, int tc) {
+  extern __shared__ float2 sm[];
+  const int slot = blockIdx.y;
+  int sysi = slot;
+  if (sys_of_slot) {
+    sysi = sys_of_slot[slot];
+    if (sysi < 0) return;
+  }
+  const long long n = (long long)g.nz * g.nx;
+  float2* ws = w + slot * n;
+  const int c0 = blockIdx.x * tc;
+  const int ncol = min(tc, g.nx - c0);
+  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
+    int z = k / tc, c = k - z * tc;
+    if (c < ncol) sm[k] = ws[(long long)z * g.nx + c0 + c];
+  }
+  __syncthreads();
+  fft_lines<false>(sm, tc, 1, tc, true, t.pz);
+  const SysScalars s = sys_scalars(g, freq[sysi]);
+  const float kh2 = (float)s.kh2;
+  const float inv_n = 1.0f / (float)n;
+  const float2 shiftc = make_float2(kh2, (float)(kh2 * shift));
+  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
+    int z = k / tc, c = k - z * tc;
+    if (c < ncol) {
+      float sym = -4.0f * (t.s2z[z] + t.s2x[c0 + c]);
+      float2 den = make_float2(sym + shiftc.x, shiftc.y);
+      float2 mul = divc(make_float2(inv_n, 0.f), den);
+      if (adjoint) mul = conjc(mul);
+      sm[k] = sm[k] * mul;
+    }
+  }
+  __syncthreads();
+  fft_lines<true>(sm, tc, 1, tc, true, t.pz);
+  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
+    int z = k / tc, c = k - z * tc;
+    if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];
+  }
+}
+
+int nsr_cols_tc(const NsrGrid* g) { return g->nz <= 1024 ? 16 : 8; }
+size_t nsr_cols_smem(const NsrGrid* g) { return sizeof(float2) * (size_t)g->nz * nsr_cols_tc(g); }
+
+// Stand-alone row passes of nsr_precondition.
+__global__ void __launch_bounds__(256) k_prec_rows_fwd(Geo g, PrecTables t, const float2* __restrict__ x,
+                                                       float2* __restrict__ w, int rows) {
+  extern __shared__ float2 sm[];
+  const long long n = (long long)g.nz * g.nx;
+  const int z0 = blockIdx.x * rows;
+  const int nr = min(rows, g.nz - z0);
+  const float2* xs = x + blockIdx.y * n + (long long)z0 * g.nx;
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) sm[k] = xs[k];
+  __syncthreads();
+  fft_lines<false>(sm, nr, g.nx, 1, false, t.px);
+  float2* ws = w + blockIdx.y * n + (long long)z0 * g.nx;
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) ws[k] = sm[k];
+}
+
+__global__ void __launch_bounds__(256) k_prec_rows_inv(Geo g, PrecTables t, const float2* __restrict__ w,
+                                                       float2* __restrict__ y, int rows) {
+  extern __shared__ float2 sm[];
+  const long long n = (long long)g.nz * g.nx;
+  const int z0 = blockIdx.x * rows;
+  const int nr = min(rows, g.nz - z0);
+  const float2* ws = w + blockIdx.y * n + (long long)z0 * g.nx;
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) sm[k] = ws[k];
+  __syncthreads();
+  fft_lines<true>(sm, nr, g.nx, 1, false, t.px);
+  float2* ys = y + blockIdx.y * n + (long long)z0 * g.nx;
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) ys[k] = sm[k];
+}
+
+extern "C" size_t nsr_precondition_workspace_size(const NsrGrid* grid, int32_t n_systems) {
+  if (nsr_check_grid(grid, true) || n_systems < 0) return 0;
+  return nsr_prec_table_bytes(grid) + nsr_align(sizeof(float2) * (size_t)grid->nz * grid->nx * n_systems);
+}
+
+extern "C" int nsr_precondition(const NsrGrid* grid, const double* freq_hz, int32_t n_systems,
+                                double shift, int32_t adjoint, const float* x, float* y,
+                                void* workspace, size_t workspace_bytes, void* stream) {
+  int err = nsr_check_grid(grid, true);
+  if (err) return err;
+  if (!freq_hz || !x || !y || !workspace || n_systems < 0 || n_systems > 65535) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;
+  if (workspace_bytes < nsr_precondition_workspace_size(grid, n_systems)) return NSR_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  PrecTables t;
+  err = nsr_prec_setup(grid, &t, workspace, st);
+  if (err) return err;
+  float2* w = (float2*)((char*)workspace + nsr_prec_table_bytes(grid));
+  Geo g = make_geo(*grid);
+  const int rows = nsr_rows_per_cta(grid);
+  const size_t row_smem = sizeof(float2) * (size_t)rows * grid->nx;
+  dim3 gr((grid->nz + rows - 1) / rows, n_systems);
+  k_prec_rows_fwd<<<gr, 256, row_smem, st>>>(g, t, (const float2*)x, w, rows);
+  const int tc = nsr_cols_tc(grid);
+  dim3 gc((grid->nx + tc - 1) / tc, n_systems);
+  size_t csm = nsr_cols_smem(grid);
+  cudaFuncSetAttribute(k_prec_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+  k_prec_cols<<<gc, 256, csm, st>>>(g, t, freq_hz, nullptr, w, shift, adjoint, tc);
+  k_prec_rows_inv<<<gr, 256, row_smem, st>>>(g, t, w, (float2*)y, rows);
+  return last_error();
+}
+
+int nsr_rows_per_cta(const NsrGrid* g) {
+  // Keep row tiles near 32 KB of shared memory.
+  int rows = (int)(4096 / g->nx);
+  if (rows < 1) rows = 1;
+  if (rows > 8) rows = 8;
+  return rows;
+}
+
+// ---------------------------------------------------------------------------
+// Plane-wave right-hand side (SI units, c128).
+// ---------------------------------------------------------------------------
+__global__ void k_plane_wave_rhs(Geo g, const double* __restrict__ freq, const double* __restrict__ angle,
+                                 double2* __restrict__ b) {
+  const long long n = (long long)g.nz * g.nx;
+  const int sysi = blockIdx.y;
+  const SysScalars s = sys_scalars(g, freq[sysi]);
+  const double st = sin(angle[sysi]);
+  const double inv_h2 = 1.0 / (g.h * g.h);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.nx), j = (int)(k - (long long)i * g.nx);
+    double2 v = make_double2(0.0, 0.0);
+    if (i == g.face) {
+      double2 l = source_line(g, s.k0, st, j);
+      v = make_double2(-l.x * inv_h2, -l.y * inv_h2);
+    }
+    b[sysi * n + k] = v;
+  }
+}
+
+extern "C" int nsr_plane_wave_rhs(const NsrGrid* grid, const double* freq_hz, const double* angle_rad,
+                                  int32_t n_systems, void* b, void* stream) {
+  int err = nsr_check_grid(grid, false);
+  if (err) return err;
+  if (!freq_hz || !angle_rad || !b || n_systems < 0 || n_systems > 65535) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;
+  long long n = (long long)grid->nz * grid->nx;
+  int bx = (int)((n + 255) / 256);
+  if (bx > 4096) bx = 4096;
+  k_plane_wave_rhs<<<dim3(bx, n_systems), 256, 0, (cudaStream_t)stream>>>(make_geo(*grid), freq_hz, angle_rad,
+                                                                           (double2*)b);
+  return last_error();
+}
+
+// ---------------------------------------------------------------------------
+// Material gradient: -Re(lambda^H dA/dm u) for m = log c, log rho.
+// d mass / d log c  = -2 k0^2 sx sz b (1 + i e)
+// d mass / d log rho = -mass
+// each edge e=(i,j): d(lam^H A u)/d log rho_i = a_i w_e conj(lam_j - lam_i)(u_j - u_i),
+// w_e = stretch_e / (2 h^2).
+// ---------------------------------------------------------------------------
+__global__ void k_grad(Geo g, const float* __restrict__ coef, const double* __restrict__ freq, int ns,
+                       const float2* __restrict__ u, const float2* __restrict__ lam,
+                       double* __restrict__ gc, double* __restrict__ gr) {
+  const long long n = (long long)g.nz * g.nx;
+  const double inv_h2 = 1.0 / (g.h * g.h);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.nx), j = (int)(k - (long long)i * g.nx);
+    const double a_c = coef[k], b_c = coef[n + k], t_c = coef[2 * n + k];
+    double acc_c = 0.0, acc_r = 0.0;
+    for (int sidx = 0; sidx < ns; ++sidx) {
+      const SysScalars s = sys_scalars(g, freq[sidx]);
+      const float2* us = u + sidx * n;
+      const float2* ls = lam + sidx * n;
+      auto U = [&](int i2, int j2) -> double2 {
+        if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return make_double2(0.0, 0.0);
+        return to_d(us[(long long)i2 * g.nx + j2]);
+      };
+      auto L = [&](int i2, int j2) -> double2 {
+        if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return make_double2(0.0, 0.0);
+        return to_d(ls[(long long)i2 * g.nx + j2]);
+      };
+      const double2 uc = U(i, j), lc = L(i, j);
+      const double2 lu = conjc(lc) * uc;
+      const double sig = s.sig;
+      const double2 sx = make_double2(1.0, sig * pml_profile<double>((double)j, g.nx, g.n_pml));
+      const double2 sz = make_double2(1.0, sig * pml_profile<double>((double)i, g.nz, g.n_pml));
+      const double e = t_c * s.fpow;
+      const double2 onepie = make_double2(1.0, e);
+      const double2 cell = (s.kh2 * b_c) * (sx * sz);          // h^2 k0^2 sx sz b
+      const double2 dm_c = (-2.0) * (cell * onepie);
+      const double2 dm_r = (-1.0) * (cell * (onepie * onepie));
+      double2 edge = make_double2(0.0, 0.0);
+      const int di[4] = {0, 0, 1, -1}, dj[4] = {1, -1, 0, 0};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double2 st;
+        if (q < 2) {
+          double2 sh = make_double2(1.0, sig * pml_profile<double>(j + 0.5 * dj[q], g.nx, g.n_pml));
+          st = divc(sz, sh);
+        } else {
+          double2 sh = make_double2(1.0, sig * pml_profile<double>(i + 0.5 * di[q], g.nz, g.n_pml));
+          st = divc(sx, sh);
+        }
+        const double2 du = U(i + di[q], j + dj[q]) - uc;
+        const double2 dl = conjc(L(i + di[q], j + dj[q]) - lc);
+        edge = edge + (0.5 * st) * (dl * du);
+      }
+      acc_c += -(lu * dm_c).x;
+      acc_r += -(lu * dm_r).x - a_c * edge.x;
+    }
+    gc[k] += acc_c * inv_h2;
+    gr[k] += acc_r * inv_h2;
+  }
+}
+
+extern "C" int nsr_grad_accum(const NsrGrid* grid, const float* coef, const double* freq_hz,
+                              int32_t n_systems, const float* u, const float* lam,
+                              double* g_logc, double* g_logrho, void* stream) {
+  int err = nsr_check_grid(grid, false);
+  if (err) return err;
+  if (!coef || !freq_hz || !u || !lam || !g_logc || !g_logrho || n_systems < 0) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;
+  long long n = (long long)grid->nz * grid->nx;
+  int bx = (int)((n + 255) / 256);
+  if (bx > 148 * 16) bx = 148 * 16;
+  k_grad<<<bx, 256, 0, (cudaStream_t)stream>>>(make_geo(*grid), coef, freq_hz, n_systems, (const float2*)u,
+                                              (const float2*)lam, g_logc, g_logrho);
+  return last_error();
+}

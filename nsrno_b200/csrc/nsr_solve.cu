@@ -1,0 +1,795 @@
+// Batched right-preconditioned BiCGSTAB for the 5-point Helmholtz systems of a
+// record.  Design:
+//   * n_slots systems are resident; a device-side queue refills a slot when
+//     its system finishes (converged, budget, breakdown, divergence).
+//   * One BiCGSTAB iteration = two halves; each half is three launches:
+//       fwd  : elementwise Krylov update fused with the forward row FFT,
+//       cols : column FFT, shifted-Laplace multiply, inverse column FFT,
+//       inv  : inverse row FFT fused with the 5-point stencil and the
+//              FP64 inner products of that half.
+//     The last CTA of a slot (arrival counter, no waiting) sums the per-CTA
+//     partials in a fixed order and advances that slot's scalar recurrence,
+//     so no host synchronisation happens inside the loop.
+//   * The update of x is deferred: y accumulates alpha p + omega s and
+//     x += M^-1 y is applied at every true-residual replacement, where
+//     r = b - A x is recomputed in FP64 from an FP64 x.
+//   * The host captures `graph_iterations` iterations in a CUDA graph and
+//     relaunches it, polling a completion counter.
+// Algorithmic reference: bicgstab, nsrno/dense_wave.py:118-148 (right
+// preconditioned, shared-angle inner products, true residual every 40
+// iterations, breakdown/divergence reasons) and the fixed preconditioner of
+// nsrno/dense_wave.py:194-196.
+#include "nsr_internal.cuh"
+
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES = 4, MODE_EMIT = 5 };
+#define NSR_NPART 8
+
+struct __align__(16) SlotState {
+  int sys, mode, iters, final_reason;
+  int xpar, zero_rhs, pad0, pad1;
+  double bnorm2, rnorm2, resid;
+  double freq, angle;
+  double2 rho, alpha, omega, beta;
+  // s = r + c_sv v ; r_new = s + c_rt t ; y += c_yp p + c_ys s ; p_new = r_new + c_pp p + c_pv v
+  double2 c_sv, c_rt, c_yp, c_ys, c_pp, c_pv;
+};
+
+struct SolveBufs {
+  SlotState* slots;
+  int* arrive;        // [n_slots]
+  int* queue;         // next system to start
+  int* done;          // systems finished
+  double* partials;   // [n_slots][nb_inv][NSR_NPART]
+  float2 *r, *rh, *p, *v, *t, *y, *w;   // [n_slots][n]
+  double2* x;         // [n_slots][2][n]
+};
+
+struct SolveArgs {
+  Geo g;
+  PrecTables tab;
+  SolveBufs B;
+  const float* coef;
+  const double* freq;
+  const double* angle;
+  const float2* rhs;
+  const float2* x0;
+  const int* rx;
+  int n_rx;
+  int n_systems;
+  int rows;      // rows per fwd CTA
+  int tc;        // columns per cols CTA
+  int tz;        // band rows per inv CTA
+  int nb_inv;    // inv CTAs per slot
+  double tol2;
+  double shift;
+  int max_it;
+  int replace_every;
+  int adjoint;
+  double2* iq;
+  double* residual;
+  int* iterations;
+  int* status;
+  float2* fields;
+};
+
+__device__ __forceinline__ bool active_in(int mode, int half) {
+  return (half == 0 && mode == MODE_ITER_A) || (half == 1 && mode == MODE_ITER_B) || mode == MODE_RES ||
+         mode == MODE_INIT || mode == MODE_EMIT;
+}
+
+__device__ __forceinline__ float2 f2(double2 a) { return make_float2((float)a.x, (float)a.y); }
+__device__ __forceinline__ bool finite2(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+__device__ __forceinline__ double abs2(double2 a) { return a.x * a.x + a.y * a.y; }
+
+// ---------------------------------------------------------------------------
+// fwd: elementwise update + forward row FFT into w.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
+  extern __shared__ float2 sm[];
+  const int slot = blockIdx.y;
+  const SlotState& S = A.B.slots[slot];
+  const int mode = S.mode;
+  if (!active_in(mode, half)) return;
+  const Geo& g = A.g;
+  const long long n = (long long)g.nz * g.nx;
+  const int z0 = blockIdx.x * A.rows;
+  const int nr = min(A.rows, g.nz - z0);
+  const long long off = slot * n + (long long)z0 * g.nx;
+  const int cnt = nr * g.nx;
+  float2 *r = A.B.r + off, *p = A.B.p + off, *v = A.B.v + off, *t = A.B.t + off, *y = A.B.y + off;
+  if (mode == MODE_INIT) {
+    const float2 z = make_float2(0.f, 0.f);
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) { p[k] = z; v[k] = z; t[k] = z; y[k] = z; }
+    return;
+  }
+  if (mode == MODE_EMIT) {
+    if (A.fields && S.sys >= 0) {
+      const double2* x = A.B.x + (2LL * slot + S.xpar) * n + (long long)z0 * g.nx;
+      float2* f = A.fields + (long long)S.sys * n + (long long)z0 * g.nx;
+      for (int k = threadIdx.x; k < cnt; k += blockDim.x) f[k] = S.zero_rhs ? make_float2(0.f, 0.f) : f2(x[k]);
+    }
+    return;
+  }
+  const float2 sv = f2(S.c_sv), rt = f2(S.c_rt), yp = f2(S.c_yp), ys = f2(S.c_ys), pp = f2(S.c_pp), pv = f2(S.c_pv);
+  if (mode == MODE_ITER_A) {
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 rk = r[k], vk = v[k], tk = t[k], pk = p[k], yk = y[k];
+      const float2 s = rk + sv * vk;
+      const float2 rn = s + rt * tk;
+      const float2 yn = yk + yp * pk + ys * s;
+      const float2 pn = rn + pp * pk + pv * vk;
+      r[k] = rn; p[k] = pn; y[k] = yn;
+      sm[k] = pn;
+    }
+  } else if (mode == MODE_ITER_B) {
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) sm[k] = r[k] + sv * v[k];
+  } else {  // MODE_RES: apply the pending update to y, transform y, clear it
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 s = r[k] + sv * v[k];
+      sm[k] = y[k] + yp * p[k] + ys * s;
+      y[k] = make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+  fft_lines<false>(sm, nr, g.nx, 1, false, A.tab.px);
+  float2* w = A.B.w + off;
+  for (int k = threadIdx.x; k < cnt; k += blockDim.x) w[k] = sm[k];
+}
+
+// ---------------------------------------------------------------------------
+// cols: column FFT, preconditioner multiply, inverse column FFT (in place).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_cols(SolveArgs A, int half) {
+  extern __shared__ float2 sm[];
+  const int slot = blockIdx.y;
+  const int mode = A.B.slots[slot].mode;
+  if (!((half == 0 && mode == MODE_ITER_A) || (half == 1 && mode == MODE_ITER_B) || mode == MODE_RES)) return;
+  const Geo& g = A.g;
+  const long long n = (long long)g.nz * g.nx;
+  float2* ws = A.B.w + slot * n;
+  const int tc = A.tc;
+  const int c0 = blockIdx.x * tc;
+  const int ncol = min(tc, g.nx - c0);
+  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
+    int z = k / tc, c = k - z * tc;
+    sm[k] = c < ncol ? ws[(long long)z * g.nx + c0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_lines<false>(sm, tc, 1, tc, true, A.tab.pz);
+  const SysScalars s = sys_scalars(g, A.B.slots[slot].freq);
+  const float kh2 = (float)s.kh2;
+  const float inv_n = 1.0f / (float)n;
+  const float2 shiftc = make_float2(kh2, (float)(s.kh2 * A.shift));
+  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
+    int z = k / tc, c = k - z * tc;
+    if (c < ncol) {
+      float sym = -4.0f * (A.tab.s2z[z] + A.tab.s2x[c0 + c]);
+      float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
+      if (A.adjoint) mul = conjc(mul);
+      sm[k] = sm[k] * mul;
+    }
+  }
+  __syncthreads();
+  fft_lines<true>(sm, tc, 1, tc, true, A.tab.pz);
+  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
+    int z = k / tc, c = k - z * tc;
+    if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reduction helpers.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-reduce NV doubles into red[0..NV) (valid in thread 0 afterwards).
+template <int NV>
+__device__ __forceinline__ void block_sum(double* vals, double* red) {
+  __shared__ double wsum[32][NSR_NPART];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = warp_sum(vals[q]);
+    if (lane == 0) wsum[wid][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += wsum[w][q];
+      red[q] = s;
+    }
+  }
+}
+
+__device__ void pop_next(const SolveArgs& A, SlotState& S) {
+  const int nxt = atomicAdd(A.B.queue, 1);
+  if (nxt < A.n_systems) {
+    S.sys = nxt;
+    S.mode = MODE_INIT;
+    S.freq = A.freq[nxt];
+    S.angle = A.angle ? A.angle[nxt] : 0.0;
+  } else {
+    S.sys = -1;
+    S.mode = MODE_EMPTY;
+  }
+}
+
+__device__ void finish_system(const SolveArgs& A, SlotState& S, int reason, double rel) {
+  const long long n = (long long)A.g.nz * A.g.nx;
+  const int slot = (int)(&S - A.B.slots);
+  const double2* x = A.B.x + (2LL * slot + S.xpar) * n;
+  for (int k = 0; k < A.n_rx; ++k) {
+    const int idx = A.rx[k];
+    const bool ok = idx >= 0 && (long long)idx < n;   // out-of-range receivers read as NaN
+    A.iq[(long long)S.sys * A.n_rx + k] = !ok ? make_double2(NAN, NAN)
+                                         : (S.zero_rhs ? make_double2(0.0, 0.0) : __ldcg(&x[idx]));
+  }
+  A.residual[S.sys] = rel;
+  A.iterations[S.sys] = S.iters;
+  A.status[S.sys] = reason;
+  __threadfence();
+  atomicAdd(A.B.done, 1);
+  if (A.fields) S.mode = MODE_EMIT;
+  else pop_next(A, S);
+}
+
+// Scalar recurrence of one slot, run by thread 0 of the slot's last CTA.
+__device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const double* sum) {
+  const double tol2 = A.tol2;
+  if (mode == MODE_EMIT) { pop_next(A, S); return; }
+  if (mode == MODE_INIT) {
+    S.bnorm2 = sum[0];
+    S.rnorm2 = sum[1];
+    S.xpar ^= 1;
+    S.iters = 0;
+    S.final_reason = -1;
+    S.zero_rhs = 0;
+    if (!(S.bnorm2 > 0.0)) {
+      S.zero_rhs = isfinite(S.bnorm2) ? 1 : 0;
+      finish_system(A, S, isfinite(S.bnorm2) ? NSR_CONVERGED : NSR_NONFINITE, 0.0);
+      return;
+    }
+    const double rel2 = S.rnorm2 / S.bnorm2;
+    if (!isfinite(rel2)) { finish_system(A, S, NSR_NONFINITE, rel2); return; }
+    if (rel2 < tol2) { finish_system(A, S, NSR_CONVERGED, sqrt(rel2)); return; }
+    S.rho = make_double2(S.rnorm2, 0.0);
+    S.alpha = S.omega = S.beta = make_double2(0.0, 0.0);
+    const double2 z = make_double2(0.0, 0.0);
+    S.c_sv = S.c_rt = S.c_yp = S.c_ys = S.c_pp = S.c_pv = z;
+    S.mode = MODE_ITER_A;
+    return;
+  }
+  if (mode == MODE_ITER_A) {
+    const double2 sigma = make_double2(sum[0], sum[1]);
+    const double z2 = abs2(sigma);
+    if (!finite2(sigma) || !(z2 > 1e-60 * S.bnorm2 * S.bnorm2)) {
+      S.final_reason = NSR_BREAKDOWN;
+      S.c_sv = S.c_yp = S.c_ys = make_double2(0.0, 0.0);
+      S.mode = MODE_RES;
+      return;
+    }
+    S.alpha = divc(S.rho, sigma);
+    S.c_sv = make_double2(-S.alpha.x, -S.alpha.y);
+    S.mode = MODE_ITER_B;
+    return;
+  }
+  if (mode == MODE_ITER_B) {
+    const double2 ts = make_double2(sum[0], sum[1]);
+    const double tt = sum[2], ss = sum[3];
+    const double2 rt = make_double2(sum[4], sum[5]);
+    const double2 rs = make_double2(sum[6], sum[7]);
+    S.iters += 1;
+    const double2 z = make_double2(0.0, 0.0);
+    if (ss < tol2 * S.bnorm2) {   // early exit on s (nsrno/dense_wave.py:138-139)
+      S.omega = z;
+      S.c_yp = S.alpha; S.c_ys = z; S.c_sv = make_double2(-S.alpha.x, -S.alpha.y); S.c_rt = z;
+      S.mode = MODE_RES;
+      return;
+    }
+    if (!(tt > 0.0) || !isfinite(tt) || !finite2(ts)) {
+      S.final_reason = isfinite(tt) ? NSR_BREAKDOWN : NSR_NONFINITE;
+      S.omega = z;
+      S.c_yp = S.alpha; S.c_ys = z; S.c_sv = make_double2(-S.alpha.x, -S.alpha.y);
+      S.mode = MODE_RES;
+      return;
+    }
+    const double2 omega = make_double2(ts.x / tt, ts.y / tt);
+    const double2 rho_new = rs - omega * rt;
+    double rn2 = ss - abs2(ts) / tt;
+    S.rnorm2 = rn2 > 0.0 ? rn2 : 0.0;
+    S.omega = omega;
+    S.c_sv = make_double2(-S.alpha.x, -S.alpha.y);
+    S.c_rt = make_double2(-omega.x, -omega.y);
+    S.c_yp = S.alpha;
+    S.c_ys = omega;
+    const bool omega_ok = abs2(omega) > 1e-60;
+    const bool rho_ok = finite2(rho_new) && abs2(rho_new) > 1e-60 * S.bnorm2 * S.bnorm2;
+    if (omega_ok && rho_ok) {
+      S.beta = divc(rho_new, S.rho) * divc(S.alpha, omega);
+      S.rho = rho_new;
+      S.c_pp = S.beta;
+      S.c_pv = make_double2(0.0, 0.0) - S.beta * omega;
+    } else {
+      S.final_reason = NSR_BREAKDOWN;
+    }
+    if (S.final_reason >= 0 || S.rnorm2 < tol2 * S.bnorm2 || S.iters >= A.max_it ||
+        (A.replace_every > 0 && S.iters % A.replace_every == 0)) {
+      if (S.iters >= A.max_it && S.final_reason < 0) S.final_reason = NSR_ITERATION_BUDGET;
+      S.mode = MODE_RES;
+    } else {
+      S.mode = MODE_ITER_A;
+    }
+    return;
+  }
+  if (mode == MODE_RES) {
+    const double rr = sum[0];
+    const double2 rhr = make_double2(sum[1], sum[2]);
+    S.xpar ^= 1;
+    const double rel2 = rr / S.bnorm2;
+    const double rel = sqrt(rel2);
+    S.resid = rel;
+    if (!isfinite(rel2)) { finish_system(A, S, NSR_NONFINITE, rel); return; }
+    if (rel2 < tol2) { finish_system(A, S, NSR_CONVERGED, rel); return; }
+    if (S.final_reason >= 0) { finish_system(A, S, S.final_reason, rel); return; }
+    if (rel > 1e5) { finish_system(A, S, NSR_DIVERGED, rel); return; }
+    if (S.iters >= A.max_it) { finish_system(A, S, NSR_ITERATION_BUDGET, rel); return; }
+    const double2 z = make_double2(0.0, 0.0);
+    S.c_sv = S.c_rt = S.c_yp = S.c_ys = z;
+    if (abs2(S.omega) > 1e-60 && abs2(S.rho) > 0.0) {
+      // Replace the recursive residual by the true one and rescale beta.
+      S.beta = S.beta * divc(rhr, S.rho);
+      S.c_pp = S.beta;
+      S.c_pv = z - S.beta * S.omega;
+    } else {
+      // The s-based exit was premature: restart the recurrence from r.
+      S.c_pp = S.c_pv = z;
+    }
+    S.rho = rhr;
+    S.rnorm2 = rr;
+    S.mode = MODE_ITER_A;
+    return;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// inv: inverse row FFT + stencil + inner products; INIT/RES do the FP64
+// true residual instead.
+// ---------------------------------------------------------------------------
+template <bool ADJ>
+__global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
+  extern __shared__ float2 sm[];
+  __shared__ double red[NSR_NPART];
+  __shared__ int am_last;
+  const int slot = blockIdx.y;
+  SlotState& S = A.B.slots[slot];
+  const int mode = S.mode;
+  if (!active_in(mode, half)) return;
+  const Geo& g = A.g;
+  const long long n = (long long)g.nz * g.nx;
+  const int tz = A.tz;
+  const int z0 = blockIdx.x * tz;
+  const int nb = min(tz, g.nz - z0);
+  const int nx = g.nx;
+  const SysScalars sc = sys_scalars(g, S.freq);
+  const float* ca = A.coef;
+  const float* cb = A.coef + n;
+  const float* ct = A.coef + 2 * n;
+  auto Aa32 = [&](int i2, int j2) -> float {
+    if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return 1.0f;
+    return __ldg(&ca[(long long)i2 * nx + j2]);
+  };
+  auto Aa64 = [&](int i2, int j2) -> double {
+    if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return 1.0;
+    return (double)__ldg(&ca[(long long)i2 * nx + j2]);
+  };
+  double acc[NSR_NPART];
+#pragma unroll
+  for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
+  const long long soff = slot * n;
+  const bool need_fft = (mode == MODE_ITER_A || mode == MODE_ITER_B || mode == MODE_RES);
+  if (need_fft) {
+    // rows z0-1 .. z0+nb of w into shared memory (zero outside the grid)
+    const float2* w = A.B.w + soff;
+    const int nl = nb + 2;
+    for (int k = threadIdx.x; k < nl * nx; k += blockDim.x) {
+      const int zr = k / nx, j = k - zr * nx;
+      const int z = z0 - 1 + zr;
+      sm[k] = (z >= 0 && z < g.nz) ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_lines<true>(sm, nl, nx, 1, false, A.tab.px);
+  }
+  if (mode == MODE_ITER_A || mode == MODE_ITER_B) {
+    auto P = [&](int i2, int j2) -> float2 {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return make_float2(0.f, 0.f);
+      return sm[(i2 - z0 + 1) * nx + j2];
+    };
+    const float2* rh = A.B.rh + soff;
+    if (mode == MODE_ITER_A) {
+      float2* v = A.B.v + soff;
+      for (int k = threadIdx.x; k < nb * nx; k += blockDim.x) {
+        const int i = z0 + k / nx, j = k % nx;
+        const long long idx = (long long)i * nx + j;
+        const float2 av = stencil<float, ADJ>(g, sc, i, j, __ldg(&cb[idx]), __ldg(&ct[idx]), P, Aa32);
+        v[idx] = av;
+        dot_acc(acc[0], acc[1], rh[idx], av);
+      }
+    } else {
+      float2* t = A.B.t + soff;
+      const float2* r = A.B.r + soff;
+      const float2* v = A.B.v + soff;
+      const float2 sv = f2(S.c_sv);
+      for (int k = threadIdx.x; k < nb * nx; k += blockDim.x) {
+        const int i = z0 + k / nx, j = k % nx;
+        const long long idx = (long long)i * nx + j;
+        const float2 at = stencil<float, ADJ>(g, sc, i, j, __ldg(&cb[idx]), __ldg(&ct[idx]), P, Aa32);
+        t[idx] = at;
+        const float2 s = r[idx] + sv * v[idx];
+        const float2 rk = rh[idx];
+        dot_acc(acc[0], acc[1], at, s);        // <t, s>
+        acc[2] += (double)at.x * at.x + (double)at.y * at.y;
+        acc[3] += (double)s.x * s.x + (double)s.y * s.y;
+        dot_acc(acc[4], acc[5], rk, at);       // <rhat, t>
+        dot_acc(acc[6], acc[7], rk, s);        // <rhat, s>
+      }
+    }
+  } else if (mode == MODE_RES || mode == MODE_INIT) {
+    const double2* xo = A.B.x + (2LL * slot + S.xpar) * n;
+    double2* xn = A.B.x + (2LL * slot + (S.xpar ^ 1)) * n;
+    const float2* x0 = (A.x0 && S.sys >= 0) ? A.x0 + (long long)S.sys * n : nullptr;
+    auto P = [&](int i2, int j2) -> double2 {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return make_double2(0.0, 0.0);
+      const long long id = (long long)i2 * nx + j2;
+      if (mode == MODE_INIT) return x0 ? to_d(x0[id]) : make_double2(0.0, 0.0);
+      return xo[id] + to_d(sm[(i2 - z0 + 1) * nx + j2]);
+    };
+    const double h2 = g.h * g.h;
+    const float2* rhs = A.rhs ? A.rhs + (long long)S.sys * n : nullptr;
+    const double st = sin(S.angle);
+    float2* r = A.B.r + soff;
+    float2* rh = A.B.rh + soff;
+    for (int k = threadIdx.x; k < nb * nx; k += blockDim.x) {
+      const int i = z0 + k / nx, j = k % nx;
+      const long long idx = (long long)i * nx + j;
+      double2 b;
+      if (rhs) {
+        b = h2 * to_d(rhs[idx]);
+      } else if (i == g.face) {
+        double2 l = source_line(g, sc.k0, st, j);
+        b = make_double2(-l.x, -l.y);
+      } else {
+        b = make_double2(0.0, 0.0);
+      }
+      const double2 ax = stencil<double, ADJ>(g, sc, i, j, (double)__ldg(&cb[idx]), (double)__ldg(&ct[idx]), P, Aa64);
+      const double2 res = b - ax;
+      xn[idx] = P(i, j);
+      const float2 rf = to_f(res);
+      r[idx] = rf;
+      if (mode == MODE_INIT) {
+        rh[idx] = rf;
+        acc[0] += b.x * b.x + b.y * b.y;
+        acc[1] += (double)rf.x * rf.x + (double)rf.y * rf.y;
+      } else {
+        acc[0] += (double)rf.x * rf.x + (double)rf.y * rf.y;
+        dot_acc(acc[1], acc[2], rh[idx], rf);
+      }
+    }
+  }
+  // ---- per-CTA partials, arrival, last-CTA finalize -------------------------
+  block_sum<NSR_NPART>(acc, red);
+  double* part = A.B.partials + (long long)slot * A.nb_inv * NSR_NPART;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < NSR_NPART; ++q) part[blockIdx.x * NSR_NPART + q] = red[q];
+    __threadfence();
+    const int prev = atomicAdd(&A.B.arrive[slot], 1);
+    am_last = (prev == (int)gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  // Deterministic sum over CTAs: thread q sums column q in CTA order.
+  __shared__ double tot[NSR_NPART];
+  if (threadIdx.x < NSR_NPART) {
+    double s = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(&part[b * NSR_NPART + threadIdx.x]);
+    tot[threadIdx.x] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    A.B.arrive[slot] = 0;
+    finalize(A, S, mode, tot);
+    __threadfence();
+  }
+}
+
+__global__ void k_solve_init(SolveArgs A, int n_slots) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int s = tid; s < A.n_systems; s += gridDim.x * blockDim.x) {
+    A.status[s] = NSR_NOT_RUN;
+    A.iterations[s] = 0;
+    A.residual[s] = NAN;
+  }
+  for (int s = tid; s < n_slots; s += gridDim.x * blockDim.x) {
+    SlotState st;
+    memset(&st, 0, sizeof(st));
+    st.final_reason = -1;
+    if (s < A.n_systems) {
+      st.sys = s;
+      st.mode = MODE_INIT;
+      st.freq = A.freq[s];
+      st.angle = A.angle ? A.angle[s] : 0.0;
+    } else {
+      st.sys = -1;
+      st.mode = MODE_EMPTY;
+    }
+    A.B.slots[s] = st;
+    A.B.arrive[s] = 0;
+  }
+  if (tid == 0) {
+    *A.B.queue = min(A.n_systems, n_slots);
+    *A.B.done = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+static int band_rows(const NsrGrid* g) {
+  int budget = g->nx <= 1024 ? 8192 : 16384;
+  int tz = budget / g->nx - 2;
+  if (tz < 1) tz = 1;
+  if (tz > g->nz) tz = g->nz;
+  return tz;
+}
+
+struct Layout {
+  size_t tables, slots, arrive, queue, partials, vec, x, total;
+  int nb_inv;
+};
+
+static Layout layout(const NsrGrid* g, int n_slots) {
+  Layout L;
+  const size_t n = (size_t)g->nz * g->nx;
+  const int tz = band_rows(g);
+  L.nb_inv = (g->nz + tz - 1) / tz;
+  size_t off = 0;
+  L.tables = off; off += nsr_align(nsr_prec_table_bytes(g));
+  L.slots = off; off += nsr_align(sizeof(SlotState) * n_slots);
+  L.arrive = off; off += nsr_align(sizeof(int) * n_slots);
+  L.queue = off; off += nsr_align(sizeof(int) * 2);
+  L.partials = off; off += nsr_align(sizeof(double) * NSR_NPART * (size_t)L.nb_inv * n_slots);
+  L.vec = off; off += 7 * nsr_align(sizeof(float2) * n * n_slots);
+  L.x = off; off += nsr_align(sizeof(double2) * n * 2 * n_slots);
+  L.total = off;
+  return L;
+}
+
+extern "C" size_t nsr_solve_workspace_size(const NsrGrid* grid, int32_t n_slots) {
+  if (nsr_check_grid(grid, true) || n_slots <= 0 || n_slots > 65535) return 0;
+  return layout(grid, n_slots).total;
+}
+
+static int* pinned_counter() {
+  static int* p = nullptr;
+  if (!p) {
+    if (cudaHostAlloc((void**)&p, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) p = nullptr;
+  }
+  return p;
+}
+
+extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
+                                 const double* freq_hz, const double* angle_rad, int32_t n_systems,
+                                 const float* rhs, const float* x0,
+                                 const int32_t* rx_index, int32_t n_rx,
+                                 const NsrSolveParams* params,
+                                 void* workspace, size_t workspace_bytes,
+                                 double* iq, double* residual, int32_t* iterations, int32_t* status,
+                                 float* fields, NsrSolveStats* stats, void* stream) {
+  int err = nsr_check_grid(grid, true);
+  if (err) return err;
+  if (!params || !coef || !freq_hz || n_systems < 0 || n_rx < 0 || (n_rx > 0 && !rx_index)) return NSR_ERR_ARGUMENT;
+  if (!rhs && !angle_rad) return NSR_ERR_ARGUMENT;
+  if (!iq && n_rx > 0) return NSR_ERR_ARGUMENT;
+  if (!residual || !iterations || !status || !workspace) return NSR_ERR_ARGUMENT;
+  const int n_slots = params->n_slots;
+  if (n_slots <= 0 || n_slots > 65535 || params->max_iterations <= 0 || !(params->tolerance > 0) ||
+      !(params->shift >= 0) || params->replace_every < 0) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;
+  const Layout L = layout(grid, n_slots);
+  if (workspace_bytes < L.total) return NSR_ERR_WORKSPACE;
+  const size_t n = (size_t)grid->nz * grid->nx;
+  cudaStream_t caller = (cudaStream_t)stream;
+
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_poll[2] = {nullptr, nullptr};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev_loop[2] = {nullptr, nullptr};
+  cudaEvent_t* ev_prof = nullptr;
+  int n_prof_events = 0;
+  long long launches = 0;
+  int graph_launches = 0;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  int* host = pinned_counter();
+  if (!host) return (int)cudaErrorMemoryAllocation;
+  cudaError_t ce;
+#define NSR_TRY(x) do { ce = (x); if (ce != cudaSuccess) { err = (int)ce; goto cleanup; } } while (0)
+  {
+    NSR_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    NSR_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+    NSR_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+    NSR_TRY(cudaEventCreateWithFlags(&ev_poll[0], cudaEventDisableTiming));
+    NSR_TRY(cudaEventCreateWithFlags(&ev_poll[1], cudaEventDisableTiming));
+    NSR_TRY(cudaEventRecord(ev_in, caller));
+    NSR_TRY(cudaStreamWaitEvent(st, ev_in, 0));
+
+    char* ws = (char*)workspace;
+    SolveArgs A;
+    memset(&A, 0, sizeof(A));
+    A.g = make_geo(*grid);
+    err = nsr_prec_setup(grid, &A.tab, ws + L.tables, st);
+    if (err) goto cleanup;
+    A.B.slots = (SlotState*)(ws + L.slots);
+    A.B.arrive = (int*)(ws + L.arrive);
+    A.B.queue = (int*)(ws + L.queue);
+    A.B.done = A.B.queue + 1;
+    A.B.partials = (double*)(ws + L.partials);
+    const size_t vb = nsr_align(sizeof(float2) * n * n_slots);
+    float2** vecs[7] = {&A.B.r, &A.B.rh, &A.B.p, &A.B.v, &A.B.t, &A.B.y, &A.B.w};
+    for (int q = 0; q < 7; ++q) *vecs[q] = (float2*)(ws + L.vec + q * vb);
+    A.B.x = (double2*)(ws + L.x);
+    A.coef = coef;
+    A.freq = freq_hz;
+    A.angle = rhs ? nullptr : angle_rad;
+    A.rhs = (const float2*)rhs;
+    A.x0 = (const float2*)x0;
+    A.rx = rx_index;
+    A.n_rx = n_rx;
+    A.n_systems = n_systems;
+    A.rows = nsr_rows_per_cta(grid);
+    A.tc = nsr_cols_tc(grid);
+    A.tz = band_rows(grid);
+    A.nb_inv = L.nb_inv;
+    A.tol2 = params->tolerance * params->tolerance;
+    A.shift = params->shift;
+    A.max_it = params->max_iterations;
+    A.replace_every = params->replace_every;
+    A.adjoint = params->adjoint;
+    A.iq = (double2*)iq;
+    A.residual = residual;
+    A.iterations = iterations;
+    A.status = status;
+    A.fields = (float2*)fields;
+
+    const size_t fwd_smem = sizeof(float2) * A.rows * grid->nx;
+    const size_t col_smem = nsr_cols_smem(grid);
+    const size_t inv_smem = sizeof(float2) * (A.tz + 2) * grid->nx;
+    NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_inv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_inv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+
+    k_solve_init<<<64, 256, 0, st>>>(A, n_slots);
+    NSR_TRY(cudaGetLastError());
+    launches = 3;  // two table kernels and the slot initialisation
+
+    const dim3 g_fwd((grid->nz + A.rows - 1) / A.rows, n_slots);
+    const dim3 g_col((grid->nx + A.tc - 1) / A.tc, n_slots);
+    const dim3 g_inv(L.nb_inv, n_slots);
+    const int K = params->graph_iterations > 0 ? params->graph_iterations : 16;
+    auto launch_half = [&](int half, int which) {
+      if (which == 0) k_fwd<<<g_fwd, 256, fwd_smem, st>>>(A, half);
+      else if (which == 1) k_cols<<<g_col, 256, col_smem, st>>>(A, half);
+      else if (A.adjoint) k_inv<true><<<g_inv, 256, inv_smem, st>>>(A, half);
+      else k_inv<false><<<g_inv, 256, inv_smem, st>>>(A, half);
+    };
+
+    NSR_TRY(cudaEventCreate(&ev_loop[0]));
+    NSR_TRY(cudaEventCreate(&ev_loop[1]));
+    NSR_TRY(cudaEventRecord(ev_loop[0], st));
+    // Profiled iterations: launched one by one with an event between kernels.
+    int P = params->profile_iterations;
+    if (P < 0) P = 0;
+    if (P > 256) P = 256;
+    if (P > 0) {
+      n_prof_events = 6 * P + 1;
+      ev_prof = (cudaEvent_t*)calloc(n_prof_events, sizeof(cudaEvent_t));
+      if (!ev_prof) { err = (int)cudaErrorMemoryAllocation; goto cleanup; }
+      for (int e = 0; e < n_prof_events; ++e) NSR_TRY(cudaEventCreate(&ev_prof[e]));
+      NSR_TRY(cudaEventRecord(ev_prof[0], st));
+      for (int it = 0; it < P; ++it)
+        for (int half = 0; half < 2; ++half)
+          for (int which = 0; which < 3; ++which) {
+            launch_half(half, which);
+            NSR_TRY(cudaGetLastError());
+            NSR_TRY(cudaEventRecord(ev_prof[1 + it * 6 + half * 3 + which], st));
+          }
+      launches += 6LL * P;
+    }
+
+    NSR_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < K; ++it)
+      for (int half = 0; half < 2; ++half)
+        for (int which = 0; which < 3; ++which) launch_half(half, which);
+    ce = cudaStreamEndCapture(st, &graph);
+    if (ce != cudaSuccess) { err = (int)ce; goto cleanup; }
+    NSR_TRY(cudaGraphInstantiate(&exec, graph, 0));
+
+    // Each system needs at most max_it iterations plus its replacement,
+    // init and emit half-iterations; bound the number of graph launches.
+    const long long per_sys = (long long)params->max_iterations * 2 + 16;
+    const long long waves = (n_systems + n_slots - 1) / n_slots + 1;
+    const long long max_launch = waves * ((per_sys + K - 1) / K) + 4;
+    long long launched = 0;
+    bool drained = false;
+    int pending = -1;
+    while (launched < max_launch) {
+      NSR_TRY(cudaGraphLaunch(exec, st));
+      ++graph_launches;
+      launches += 6LL * K;
+      const int slot_i = (int)(launched & 1);
+      NSR_TRY(cudaMemcpyAsync(&host[slot_i], A.B.done, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NSR_TRY(cudaEventRecord(ev_poll[slot_i], st));
+      ++launched;
+      if (pending >= 0) {
+        NSR_TRY(cudaEventSynchronize(ev_poll[pending]));
+        if (host[pending] >= n_systems) { drained = true; break; }
+      }
+      pending = slot_i;
+    }
+    if (!drained && pending >= 0) {
+      NSR_TRY(cudaEventSynchronize(ev_poll[pending]));
+      drained = host[pending] >= n_systems;
+    }
+    NSR_TRY(cudaEventRecord(ev_loop[1], st));
+    NSR_TRY(cudaStreamSynchronize(st));
+    if (!drained) err = NSR_ERR_INTERNAL;
+    if (stats) {
+      float ms = 0.f;
+      NSR_TRY(cudaEventElapsedTime(&ms, ev_loop[0], ev_loop[1]));
+      stats->loop_ms = ms;
+      stats->launches = launches;
+      stats->graph_launches = graph_launches;
+      // Skip the first two profiled iterations (slot initialisation).
+      for (int it = (P > 2 ? 2 : 0); it < P; ++it)
+        for (int k = 0; k < 6; ++k) {
+          float d = 0.f;
+          NSR_TRY(cudaEventElapsedTime(&d, ev_prof[it * 6 + k], ev_prof[it * 6 + k + 1]));
+          stats->kernel_ms[k] += d;
+          stats->kernel_timed[k] += 1;
+        }
+      for (int k = 0; k < 6; ++k)
+        if (stats->kernel_timed[k]) stats->kernel_ms[k] /= stats->kernel_timed[k];
+    }
+    NSR_TRY(cudaEventRecord(ev_out, st));
+    NSR_TRY(cudaStreamWaitEvent(caller, ev_out, 0));
+  }
+cleanup:
+  if (st) cudaStreamSynchronize(st);
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (ev_in) cudaEventDestroy(ev_in);
+  if (ev_out) cudaEventDestroy(ev_out);
+  if (ev_poll[0]) cudaEventDestroy(ev_poll[0]);
+  if (ev_poll[1]) cudaEventDestroy(ev_poll[1]);
+  if (ev_loop[0]) cudaEventDestroy(ev_loop[0]);
+  if (ev_loop[1]) cudaEventDestroy(ev_loop[1]);
+  if (ev_prof) {
+    for (int e = 0; e < n_prof_events; ++e)
+      if (ev_prof[e]) cudaEventDestroy(ev_prof[e]);
+    free(ev_prof);
+  }
+  if (st) cudaStreamDestroy(st);
+#undef NSR_TRY
+  return err;
+}

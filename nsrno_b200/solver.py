@@ -1,0 +1,275 @@
+"""Record-level host API over the CUDA library.
+
+Everything here runs on a CUDA device and goes through ``libnsrno_b200.so``;
+there is no CPU path.  Tensors are PyTorch tensors on the current device and
+kernels run on ``torch.cuda.current_stream()``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from functools import lru_cache
+
+import numpy as np
+import torch
+
+from . import _lib
+
+DEFAULT_SHIFT = 0.15          # shifted-Laplace shift of nsrno/dense_wave.py:194
+DEFAULT_REPLACE = 40          # true-residual period of nsrno/dense_wave.py:143
+
+
+def _require_cuda(t: torch.Tensor, name: str):
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (nsrno_b200 has no CPU path)")
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+@dataclass
+class Geometry:
+    """Grid, PML and array geometry of one record (lengths in metres)."""
+
+    nz: int
+    nx: int
+    h: float
+    n_pml: int
+    face: int
+    rx_cols: np.ndarray
+    aperture_half_width: float
+    c0: float = 1500.0
+    rho0: float = 1000.0
+    pml_strength: float = 12.0
+    alpha_power: float = 1.1
+
+    @classmethod
+    def from_record(cls, rec):
+        return cls(nz=rec.nz, nx=rec.nx, h=rec.h, n_pml=rec.n_pml, face=rec.face,
+                   rx_cols=np.asarray(rec.rx_cols), aperture_half_width=rec.aperture_half_width,
+                   c0=rec.c0, rho0=rec.rho0, pml_strength=rec.pml_strength, alpha_power=rec.alpha_power)
+
+    @property
+    def n(self):
+        return self.nz * self.nx
+
+    def struct(self):
+        return _lib.NsrGrid(self.nz, self.nx, self.n_pml, self.face, self.h, self.c0, self.rho0,
+                            self.pml_strength, self.alpha_power, self.aperture_half_width)
+
+    def rx_index(self, device):
+        flat = self.face * self.nx + np.asarray(self.rx_cols, dtype=np.int64)
+        return torch.as_tensor(flat.astype(np.int32), device=device)
+
+
+class Medium:
+    """Material planes (a, b, t) of one record resident in device memory."""
+
+    def __init__(self, geometry: Geometry, c, rho, alpha, device=None):
+        device = torch.device(device or "cuda")
+        self.geometry = geometry
+        shape = (geometry.nz, geometry.nx)
+        planes = []
+        for name, v in (("c", c), ("rho", rho), ("alpha", alpha)):
+            t = torch.as_tensor(v, dtype=torch.float32).to(device)
+            if tuple(t.shape) != shape:
+                raise ValueError(f"{name} must have shape {shape}")
+            planes.append(t.contiguous())
+        self.c, self.rho, self.alpha = planes
+        if not bool(torch.isfinite(self.c).all() and (self.c > 0).all() and
+                    torch.isfinite(self.rho).all() and (self.rho > 0).all() and torch.isfinite(self.alpha).all()):
+            raise ValueError("c and rho must be finite and positive; alpha must be finite")
+        _require_cuda(self.c, "medium")
+        self.coef = torch.empty((3,) + shape, dtype=torch.float32, device=device)
+        self._grid = geometry.struct()
+        _lib.check(_lib.load().nsr_setup_material(ctypes.byref(self._grid), _ptr(self.c), _ptr(self.rho),
+                                                  _ptr(self.alpha), _ptr(self.coef), _stream()))
+
+    @property
+    def device(self):
+        return self.coef.device
+
+
+@dataclass
+class BatchResult:
+    iq: torch.Tensor            # complex128 [S, n_rx]
+    residual: torch.Tensor      # float64 [S] true relative residual
+    iterations: torch.Tensor    # int32 [S]
+    status: torch.Tensor        # int32 [S]
+    fields: torch.Tensor | None = None   # complex64 [S, nz, nx]
+    seconds: float = 0.0
+    extra: dict = field(default_factory=dict)
+
+    def reasons(self):
+        return [_lib.REASONS[int(s)] for s in self.status.cpu()]
+
+
+class Workspace:
+    """Reusable device workspace for ``solve_batched`` (grows on demand)."""
+
+    def __init__(self):
+        self.buf = None
+
+    def get(self, nbytes, device):
+        if self.buf is None or self.buf.numel() < nbytes or self.buf.device != device:
+            self.buf = torch.empty(int(nbytes), dtype=torch.uint8, device=device)
+        return self.buf
+
+
+_default_ws = Workspace()
+
+
+def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tolerance=1e-6,
+                  max_iterations=2000, shift=DEFAULT_SHIFT, replace_every=DEFAULT_REPLACE, n_slots=16,
+                  adjoint=False, return_fields=False, rx_index=None, graph_iterations=16,
+                  profile_iterations=0, workspace: Workspace | None = None,
+                  out: BatchResult | None = None) -> BatchResult:
+    """Solve every (frequency, angle) system of a record with batched BiCGSTAB.
+
+    ``freqs``/``angles`` are 1-D (one entry per system).  ``rhs`` (complex64
+    [S, nz, nx], SI units) replaces the plane-wave source when given.
+    ``x0`` (complex64 [S, nz, nx]) is a warm start.
+    """
+    lib = _lib.load()
+    g = medium.geometry
+    dev = medium.device
+    freqs = torch.as_tensor(freqs, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+    S = int(freqs.numel())
+    if angles is None and rhs is None:
+        raise ValueError("either angles (plane-wave sources) or rhs must be given")
+    if angles is not None:
+        angles = torch.as_tensor(angles, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+        if angles.numel() != S:
+            raise ValueError("freqs and angles must have the same length")
+    def field_arg(t, name):
+        if t is None:
+            return None
+        t = torch.as_tensor(t)
+        if tuple(t.shape) != (S, g.nz, g.nx) or not t.is_complex():
+            raise ValueError(f"{name} must be a complex tensor of shape {(S, g.nz, g.nx)}")
+        return t.to(dev, torch.complex64).contiguous()
+
+    rhs = field_arg(rhs, "rhs")
+    x0 = field_arg(x0, "x0")
+    if rx_index is None:
+        rx_index = g.rx_index(dev)
+    n_rx = int(rx_index.numel())
+    n_slots = max(1, min(int(n_slots), S)) if S else 1
+    grid = medium._grid
+    ws_bytes = lib.nsr_solve_workspace_size(ctypes.byref(grid), n_slots)
+    if ws_bytes == 0:
+        raise ValueError("unsupported grid for the batched solver (nz, nx must be 2^a 3^b in [8, 2048])")
+    ws = (workspace or _default_ws).get(ws_bytes, dev)
+    if out is None:
+        out = BatchResult(iq=torch.empty((S, n_rx), dtype=torch.complex128, device=dev),
+                          residual=torch.empty(S, dtype=torch.float64, device=dev),
+                          iterations=torch.empty(S, dtype=torch.int32, device=dev),
+                          status=torch.empty(S, dtype=torch.int32, device=dev),
+                          fields=torch.empty((S, g.nz, g.nx), dtype=torch.complex64, device=dev)
+                          if return_fields else None)
+    params = _lib.NsrSolveParams(float(tolerance), float(shift), int(max_iterations), int(replace_every),
+                                 int(n_slots), int(bool(adjoint)), int(graph_iterations), int(profile_iterations))
+    stats = _lib.NsrSolveStats()
+    _lib.check(lib.nsr_solve_batched(
+        ctypes.byref(grid), _ptr(medium.coef), _ptr(freqs), _ptr(angles), S,
+        _ptr(rhs), _ptr(x0), _ptr(rx_index), n_rx, ctypes.byref(params),
+        _ptr(ws), ws.numel(), _ptr(out.iq), _ptr(out.residual), _ptr(out.iterations), _ptr(out.status),
+        _ptr(out.fields), ctypes.byref(stats), _stream()))
+    out.extra["stats"] = stats.as_dict()
+    out.extra["n_slots"] = n_slots
+    return out
+
+
+def apply(medium: Medium, x: torch.Tensor, freqs, adjoint=False):
+    """``A x`` (or ``A^H x``) of the h^2-scaled operator for fields x [S, nz, nx]."""
+    g = medium.geometry
+    _require_cuda(x, "x")
+    if x.dtype not in (torch.complex64, torch.complex128) or x.dim() != 3 or tuple(x.shape[1:]) != (g.nz, g.nx):
+        raise ValueError("x must be complex64/complex128 [S, nz, nx]")
+    x = x.contiguous()
+    freqs = torch.as_tensor(freqs, dtype=torch.float64, device=x.device).reshape(-1).contiguous()
+    if freqs.numel() != x.shape[0]:
+        raise ValueError("one frequency per field")
+    y = torch.empty_like(x)
+    _lib.check(_lib.load().nsr_apply(ctypes.byref(medium._grid), _ptr(medium.coef), _ptr(freqs), x.shape[0],
+                                     int(bool(adjoint)), 0 if x.dtype == torch.complex64 else 1,
+                                     _ptr(x), _ptr(y), _stream()))
+    return y
+
+
+def precondition(medium: Medium, x: torch.Tensor, freqs, shift=DEFAULT_SHIFT, adjoint=False):
+    """``M^-1 x`` of the FFT shifted-Laplace preconditioner, x complex64 [S, nz, nx]."""
+    g = medium.geometry
+    _require_cuda(x, "x")
+    if x.dtype != torch.complex64 or x.dim() != 3 or tuple(x.shape[1:]) != (g.nz, g.nx):
+        raise ValueError("x must be complex64 [S, nz, nx]")
+    x = x.contiguous()
+    S = x.shape[0]
+    freqs = torch.as_tensor(freqs, dtype=torch.float64, device=x.device).reshape(-1).contiguous()
+    lib = _lib.load()
+    nbytes = lib.nsr_precondition_workspace_size(ctypes.byref(medium._grid), S)
+    if nbytes == 0:
+        raise ValueError("unsupported grid for the preconditioner")
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=x.device)
+    y = torch.empty_like(x)
+    _lib.check(lib.nsr_precondition(ctypes.byref(medium._grid), _ptr(freqs), S, float(shift), int(bool(adjoint)),
+                                    _ptr(x), _ptr(y), _ptr(ws), nbytes, _stream()))
+    return y
+
+
+def plane_wave_rhs(medium: Medium, freqs, angles):
+    """SI right-hand sides ``-line/h^2`` on the array row, complex128 [S, nz, nx]."""
+    g = medium.geometry
+    dev = medium.device
+    freqs = torch.as_tensor(freqs, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+    angles = torch.as_tensor(angles, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+    b = torch.empty((freqs.numel(), g.nz, g.nx), dtype=torch.complex128, device=dev)
+    _lib.check(_lib.load().nsr_plane_wave_rhs(ctypes.byref(medium._grid), _ptr(freqs), _ptr(angles),
+                                              freqs.numel(), _ptr(b), _stream()))
+    return b
+
+
+def grad_accum(medium: Medium, freqs, u: torch.Tensor, lam: torch.Tensor, g_logc=None, g_logrho=None):
+    """Accumulate ``-Re(lam^H dA/dm u)`` over systems for m = log c, log rho (float64 planes)."""
+    g = medium.geometry
+    dev = medium.device
+    for name, t in (("u", u), ("lam", lam)):
+        _require_cuda(t, name)
+        if t.dtype != torch.complex64 or t.dim() != 3 or tuple(t.shape[1:]) != (g.nz, g.nx):
+            raise ValueError(f"{name} must be complex64 [S, nz, nx]")
+    u = u.contiguous()
+    lam = lam.contiguous()
+    freqs = torch.as_tensor(freqs, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+    if g_logc is None:
+        g_logc = torch.zeros((g.nz, g.nx), dtype=torch.float64, device=dev)
+    if g_logrho is None:
+        g_logrho = torch.zeros((g.nz, g.nx), dtype=torch.float64, device=dev)
+    _lib.check(_lib.load().nsr_grad_accum(ctypes.byref(medium._grid), _ptr(medium.coef), _ptr(freqs), u.shape[0],
+                                          _ptr(u), _ptr(lam), _ptr(g_logc), _ptr(g_logrho), _stream()))
+    return g_logc, g_logrho
+
+
+@lru_cache(maxsize=512)
+def receiver_response(frequency, dt=2.5e-9):
+    """Known receive-chain transfer at one frequency (nsrno/conditioned_data.py:10-24).
+
+    4th-order Butterworth band-pass 4-7.5 MHz applied forward and backward
+    (|H|^2) times the real part of the linear-phase-corrected Kaiser FIR of the
+    10x polyphase decimation.  A real scalar.
+    """
+    from scipy.signal import butter, firwin, freqz, sosfreqz
+
+    sos = butter(4, [4e6, 7.5e6], fs=1 / dt, btype="bandpass", output="sos")
+    _, h = sosfreqz(sos, worN=[frequency], fs=1 / dt)
+    down = 10
+    half_len = 10 * down
+    taps = firwin(2 * half_len + 1, 1 / down, window=("kaiser", 5.0))
+    omega = 2 * np.pi * frequency * dt
+    _, fir = freqz(taps, worN=[omega])
+    return float(abs(h[0]) ** 2 * (fir[0] * np.exp(1j * omega * half_len)).real)

@@ -1,0 +1,77 @@
+"""CPU checks of the C ABI: the library loads, exports every declared entry
+point, and rejects bad arguments before touching a device."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from nsrno_b200 import _lib, build
+    build.build()
+    return _lib.load()
+
+
+def declared_symbols():
+    names = set()
+    for header in (ROOT / "include").glob("*.h"):
+        text = header.read_text()
+        names.update(re.findall(r"^\s*(?:[\w\*\s]+?)\b(nsr_\w+)\s*\(", text, flags=re.M))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_symbols()
+    assert "nsr_solve_batched" in names and len(names) >= 10
+    for name in names:
+        assert hasattr(lib, name), name
+
+
+def test_binding_lists_every_declared_symbol():
+    from nsrno_b200 import _lib
+    assert set(declared_symbols()) <= set(_lib.EXPORTS)
+
+
+def test_version_and_error_strings(lib):
+    from nsrno_b200 import _lib
+    assert lib.nsr_version() >= 100
+    assert b"invalid argument" in lib.nsr_error_string(1001)
+    assert b"2^a 3^b" in lib.nsr_error_string(1002)
+    with pytest.raises(RuntimeError, match="workspace"):
+        _lib.check(1003)
+    assert _lib.check(0) == 0
+
+
+def grid(nz=768, nx=1024, **kw):
+    from nsrno_b200 import _lib
+    g = dict(nz=nz, nx=nx, n_pml=24, face=28, h=5e-5, c0=1500.0, rho0=1000.0, pml_strength=12.0,
+             alpha_power=1.1, aperture_half_width=0.0192)
+    g.update(kw)
+    return _lib.NsrGrid(**g)
+
+
+def test_argument_errors_need_no_device(lib):
+    null = ctypes.c_void_p(0)
+    bad = grid(nz=2)
+    assert lib.nsr_setup_material(ctypes.byref(bad), null, null, null, null, null) == 1001
+    good = grid()
+    assert lib.nsr_setup_material(ctypes.byref(good), null, null, null, null, null) == 1001
+    assert lib.nsr_apply(ctypes.byref(good), null, null, 1, 0, 0, null, null, null) == 1001
+    assert lib.nsr_grad_accum(ctypes.byref(good), null, null, 1, null, null, null, null, null) == 1001
+
+
+def test_workspace_queries(lib):
+    g = grid()
+    n = 768 * 1024
+    ws = lib.nsr_solve_workspace_size(ctypes.byref(g), 16)
+    # seven complex64 vectors and two complex128 iterates per slot, plus tables
+    assert ws >= 16 * n * (7 * 8 + 2 * 16)
+    assert ws < 16 * n * (7 * 8 + 2 * 16) + (1 << 22)
+    assert lib.nsr_solve_workspace_size(ctypes.byref(grid(nz=7 * 16)), 4) == 0   # 112 = 2^4 * 7
+    assert lib.nsr_solve_workspace_size(ctypes.byref(g), 0) == 0
+    assert lib.nsr_precondition_workspace_size(ctypes.byref(g), 2) >= 2 * n * 8
+    assert lib.nsr_precondition_workspace_size(ctypes.byref(grid(nx=4096)), 1) == 0

@@ -1,0 +1,159 @@
+"""GPU parity of the batched BiCGSTAB solve against the SuperLU oracle and the
+reference's own golden vectors."""
+import math
+
+import numpy as np
+import pytest
+import torch
+from scipy import sparse
+from scipy.special import hankel1
+
+from conftest import rel, spec_of
+from oracle import helmholtz_ref as H
+
+pytestmark = pytest.mark.gpu
+
+
+def blob_case(dev):
+    from nsrno_b200 import Geometry, Medium
+    from nsrno_b200.media import blob_record
+    rec = blob_record()
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=dev)
+    return rec, med
+
+
+def test_blob_record_matches_lu(cuda):
+    """256x256 record, 3 angles x 2 frequencies: fields and receiver IQ vs SuperLU."""
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    spec = spec_of(rec)
+    a, b, t = med.coef.double().cpu().numpy()
+    f, th = rec.systems()
+    res = solve_batched(med, f, th, tolerance=1e-7, max_iterations=2000, return_fields=True, n_slots=4)
+    assert res.reasons() == ["converged"] * len(f)
+    assert float(res.residual.max()) < 1e-7
+    fields = res.fields.cpu().numpy()
+    iq = res.iq.cpu().numpy()
+    for s in range(len(f)):
+        A = H.operator_planes(spec, a, b, t, f[s])
+        rhs = H.plane_wave_rhs(spec, f[s], th[s])
+        ref = H.solve_lu(A, rhs)
+        assert rel(fields[s].ravel(), ref) < 1e-5
+        assert rel(iq[s], H.receivers(spec, ref)) < 1e-5
+
+
+def test_slot_refill_is_bitwise_identical(cuda):
+    """Results do not depend on how many slots are resident (queue refill)."""
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    r1 = solve_batched(med, f, th, tolerance=1e-6, n_slots=1)
+    r6 = solve_batched(med, f, th, tolerance=1e-6, n_slots=6)
+    assert torch.equal(r1.iq, r6.iq)
+    assert torch.equal(r1.iterations, r6.iterations)
+
+
+def fixture_case(golden, dev):
+    from nsrno_b200 import Geometry, Medium
+    axis = golden["fixture_axis_mm"]
+    h = float(axis[1] - axis[0]) * 1e-3
+    n = axis.size
+    n_pml = int(round(float(golden["fixture_pml_mm"]) * 1e-3 / h))
+    geo = Geometry(nz=n, nx=n, h=h, n_pml=n_pml, face=n // 2, rx_cols=np.arange(4), aperture_half_width=0.0,
+                   c0=float(golden["fixture_c0"]))
+    ones = np.ones((n, n), np.float32)
+    med = Medium(geo, ones * geo.c0, ones * geo.rho0, ones * 0.0, device=dev)
+    W = sparse.csc_matrix((golden["weights_val"], (golden["weights_row"], golden["weights_col"])),
+                          shape=(n * n, 4))
+    return geo, med, W
+
+
+def test_reference_fixture_fields_and_response(cuda, golden):
+    """The reference unit-test fixture (81x81, four finite elements) against its own solve."""
+    from nsrno_b200 import solve_batched
+    geo, med, W = fixture_case(golden, cuda)
+    f = float(golden["fixture_freq_mhz"]) * 1e6
+    rhs = (-(W.toarray().T) / geo.h ** 2).reshape(4, geo.nz, geo.nx).astype(np.complex64)
+    res = solve_batched(med, [f] * 4, rhs=torch.as_tensor(rhs, device=cuda), tolerance=1e-9,
+                        max_iterations=3000, return_fields=True)
+    assert res.reasons() == ["converged"] * 4
+    u = res.fields.cpu().numpy().reshape(4, -1).T.astype(np.complex128)
+    assert rel(u, golden["fields"]) < 1e-5
+    response = (W.T @ u).T
+    assert rel(response, golden["response"]) < 1e-5
+    # reciprocity of the response matrix (complex symmetric, not Hermitian)
+    assert rel(response, response.T) < 1e-5
+
+
+def test_green_function_known_answer(cuda):
+    """div grad p + k^2 p = -delta against 0.25 i H0(k r) (tests/test_theranostic.py:141-158)."""
+    from nsrno_b200 import Geometry, Medium, solve_batched
+    axis = np.linspace(-16.0, 16.0, 81)
+    h = (axis[1] - axis[0]) * 1e-3
+    n = axis.size
+    geo = Geometry(nz=n, nx=n, h=h, n_pml=int(round(6.0 / (h * 1e3))), face=0, rx_cols=np.arange(1),
+                   aperture_half_width=0.0, c0=1540.0)
+    ones = np.ones((n, n), np.float32)
+    med = Medium(geo, ones * 1540.0, ones * 1000.0, ones * 0.0, device=cuda)
+    positions = np.array([[-3.2, 0.0], [3.2, 0.0], [0.0, 4.8]])
+    idx = [int(round((p[1] + 16.0) / (h * 1e3))) * n + int(round((p[0] + 16.0) / (h * 1e3))) for p in positions]
+    rhs = np.zeros((3, n * n), np.complex64)
+    for s, k in enumerate(idx):
+        rhs[s, k] = -1.0 / h ** 2
+    rx = torch.as_tensor(np.array(idx, np.int32), device=cuda)
+    f = 0.15e6
+    res = solve_batched(med, [f] * 3, rhs=torch.as_tensor(rhs.reshape(3, n, n), device=cuda), tolerance=1e-9,
+                        max_iterations=3000, rx_index=rx)
+    measured = res.iq.cpu().numpy()
+    off = ~np.eye(3, dtype=bool)
+    d = np.linalg.norm(positions[:, None] - positions[None, :], axis=2) * 1e-3
+    exact = 0.25j * hankel1(0, 2 * np.pi * f / 1540.0 * d[off])
+    assert rel(measured[off], exact) < 0.02
+
+
+def test_adjoint_solve_matches_lu(cuda):
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    spec = spec_of(rec)
+    a, b, t = med.coef.double().cpu().numpy()
+    rng = np.random.default_rng(9)
+    g = np.zeros((1, rec.nz, rec.nx), np.complex64)
+    g[0, rec.face, rec.rx_cols] = (rng.standard_normal(len(rec.rx_cols)) + 1j * rng.standard_normal(len(rec.rx_cols)))
+    f = 1.5e6
+    res = solve_batched(med, [f], rhs=torch.as_tensor(g, device=cuda), adjoint=True, tolerance=1e-8,
+                        return_fields=True)
+    A = H.operator_planes(spec, a, b, t, f)
+    ref = H.solve_lu(A.conj().T.tocsc(), g[0].ravel().astype(np.complex128))
+    assert res.reasons() == ["converged"]
+    assert rel(res.fields[0].cpu().numpy().ravel(), ref) < 1e-5
+
+
+def test_status_paths(cuda):
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    # iteration budget
+    r = solve_batched(med, f[:2], th[:2], tolerance=1e-12, max_iterations=3)
+    assert r.reasons() == ["iteration_budget"] * 2
+    assert (r.iterations.cpu() == 3).all()
+    assert (r.residual.cpu() > 1e-12).all()
+    # zero right-hand side converges to the zero field
+    z = torch.zeros((1, rec.nz, rec.nx), dtype=torch.complex64, device=cuda)
+    r = solve_batched(med, [1e6], rhs=z, return_fields=True)
+    assert r.reasons() == ["converged"]
+    assert float(r.fields.abs().max()) == 0.0
+    # non-finite right-hand side is reported, not trapped
+    bad = torch.zeros((1, rec.nz, rec.nx), dtype=torch.complex64, device=cuda)
+    bad[0, 5, 5] = float("nan")
+    r = solve_batched(med, [1e6], rhs=bad)
+    assert r.reasons() == ["nonfinite"]
+
+
+def test_warm_start_from_solution_needs_no_iterations(cuda):
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    r = solve_batched(med, f[:3], th[:3], tolerance=1e-7, return_fields=True)
+    w = solve_batched(med, f[:3], th[:3], tolerance=1e-5, x0=r.fields.contiguous())
+    assert w.reasons() == ["converged"] * 3
+    assert (w.iterations.cpu() == 0).all()
