@@ -67,6 +67,9 @@ typedef struct NsrGrid {
 typedef struct NsrSolveParams {
   double tolerance;          /* relative true residual ||b-Ax||/||b||          */
   double shift;              /* shifted-Laplace preconditioner shift (0.15)    */
+  double restart_factor;     /* restart (fresh shadow vector) once the true
+                                residual fell by this factor since the last
+                                restart (1e-2; 0 disables)                     */
   int32_t max_iterations;    /* BiCGSTAB iterations per system                 */
   int32_t replace_every;     /* true-residual replacement period (40)          */
   int32_t n_slots;           /* systems resident at once                       */
@@ -80,9 +83,10 @@ typedef struct NsrSolveParams {
 /* Optional host-side statistics of one nsr_solve_batched call. */
 typedef struct NsrSolveStats {
   double loop_ms;            /* device time of the solve loop                   */
-  double kernel_ms[6];       /* mean duration per launch: fwd, cols, inv of the
-                                first half, then of the second half             */
-  int32_t kernel_timed[6];   /* launches averaged in kernel_ms                  */
+  double kernel_ms[8];       /* mean duration per launch, in launch order: fwd,
+                                cols, inv of the first half; fwd, cols, res, inv
+                                of the second half; [7] unused                  */
+  int32_t kernel_timed[8];   /* launches averaged in kernel_ms                  */
   int64_t launches;          /* kernels launched by the call                    */
   int32_t graph_launches;    /* CUDA graph launches                             */
   int32_t reserved;

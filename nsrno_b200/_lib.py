@@ -28,18 +28,18 @@ class NsrGrid(ctypes.Structure):
 
 
 class NsrSolveParams(ctypes.Structure):
-    _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double),
+    _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double), ("restart_factor", ctypes.c_double),
                 ("max_iterations", ctypes.c_int32), ("replace_every", ctypes.c_int32),
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
                 ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32)]
 
 
 class NsrSolveStats(ctypes.Structure):
-    _fields_ = [("loop_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double * 6),
-                ("kernel_timed", ctypes.c_int32 * 6), ("launches", ctypes.c_int64),
+    _fields_ = [("loop_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double * 8),
+                ("kernel_timed", ctypes.c_int32 * 8), ("launches", ctypes.c_int64),
                 ("graph_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
-    KERNELS = ("fwd_h0", "cols_h0", "inv_h0", "fwd_h1", "cols_h1", "inv_h1")
+    KERNELS = ("fwd_h0", "cols_h0", "inv_h0", "fwd_h1", "cols_h1", "res_h1", "inv_h1")
 
     def as_dict(self):
         return dict(loop_ms=self.loop_ms, launches=int(self.launches), graph_launches=int(self.graph_launches),

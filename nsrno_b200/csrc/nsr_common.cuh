@@ -260,6 +260,143 @@ __device__ void fft_lines(float2* s, int nl, int lstride, int estride, bool line
   }
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time specialised line FFTs for the common sizes.  Same stage
+// sequence (and therefore the same digit-reversed order) as the runtime plan.
+// ---------------------------------------------------------------------------
+struct RadixList {
+  int nst;
+  int r[NSR_MAX_RADIX_STAGES];
+};
+
+__host__ __device__ constexpr RadixList nsr_radix_list(int n) {
+  RadixList L{0, {0}};
+  int a = 0, b = 0, m = n;
+  while (m % 2 == 0) { m /= 2; ++a; }
+  while (m % 3 == 0) { m /= 3; ++b; }
+  int k = 0;
+  for (int i = 0; i < b; ++i) L.r[k++] = 3;
+  int eights = a / 3, rem = a % 3;
+  if (rem == 1 && eights > 0) { eights -= 1; L.r[k++] = 4; L.r[k++] = 4; rem = 0; }
+  for (int i = 0; i < eights; ++i) L.r[k++] = 8;
+  if (rem == 2) L.r[k++] = 4;
+  if (rem == 1) L.r[k++] = 2;
+  L.nst = k;
+  return L;
+}
+
+__host__ __device__ constexpr int nsr_stage_len(int n, int stage) {
+  RadixList L = nsr_radix_list(n);
+  int len = n;
+  for (int s = 0; s < stage; ++s) len /= L.r[s];
+  return len;
+}
+
+// One stage, everything but the number of lines known at compile time.
+// Elements: s[l*LS + k*ES].  LF: thread index runs over lines first.
+template <int N, int R, int L, bool INV, bool LF, int LS, int ES>
+__device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __restrict__ tw) {
+  constexpr int m = L / R, per_line = N / R, tstep = N / L;
+  const int nb = nl * per_line;
+  for (int b0 = threadIdx.x; b0 < nb; b0 += 2 * blockDim.x) {
+    float2 v[2][R];
+    float2* base[2];
+    int jj[2];
+    const int b1 = b0 + blockDim.x;
+    const bool two = b1 < nb;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int b = u ? (two ? b1 : b0) : b0;
+      int l, bb;
+      if (LF) { l = b % nl; bb = b / nl; } else { l = b / per_line; bb = b - l * per_line; }
+      const int o = bb / m, j = bb - o * m;
+      jj[u] = j;
+      base[u] = s + l * LS + (o * L + j) * ES;
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[u][q] = base[u][q * m * ES];
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (!INV) {
+        small_dft<R, false>(v[u]);
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * __ldg(&tw[jj[u] * k * tstep]);
+      } else {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * conjc(__ldg(&tw[jj[u] * k * tstep]));
+        small_dft<R, true>(v[u]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) base[0][q * m * ES] = v[0][q];
+    if (two) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) base[1][q * m * ES] = v[1][q];
+    }
+  }
+}
+
+template <int N, int S, bool LF, int LS, int ES>
+__device__ __forceinline__ void ct_forward(float2* s, int nl, const float2* __restrict__ tw) {
+  constexpr RadixList RL = nsr_radix_list(N);
+  if constexpr (S < RL.nst) {
+    constexpr int R = RL.r[S];
+    constexpr int L = nsr_stage_len(N, S);
+    ct_stage<N, R, L, false, LF, LS, ES>(s, nl, tw);
+    __syncthreads();
+    ct_forward<N, S + 1, LF, LS, ES>(s, nl, tw);
+  }
+}
+
+template <int N, int S, bool LF, int LS, int ES>
+__device__ __forceinline__ void ct_inverse(float2* s, int nl, const float2* __restrict__ tw) {
+  constexpr RadixList RL = nsr_radix_list(N);
+  if constexpr (S >= 0) {
+    constexpr int R = RL.r[S];
+    constexpr int L = nsr_stage_len(N, S);
+    ct_stage<N, R, L, true, LF, LS, ES>(s, nl, tw);
+    __syncthreads();
+    ct_inverse<N, S - 1, LF, LS, ES>(s, nl, tw);
+  }
+}
+
+template <int N, bool INV, bool LF, int LS, int ES>
+__device__ __forceinline__ void ct_fft(float2* s, int nl, const float2* __restrict__ tw) {
+  constexpr RadixList RL = nsr_radix_list(N);
+  if (!INV) ct_forward<N, 0, LF, LS, ES>(s, nl, tw);
+  else ct_inverse<N, RL.nst - 1, LF, LS, ES>(s, nl, tw);
+}
+
+// Rows: nl lines of length n stored back to back (lstride n, estride 1).
+template <bool INV>
+__device__ void fft_rows(float2* s, int nl, const FftPlan& P) {
+  switch (P.n) {
+    case 256: ct_fft<256, INV, false, 256, 1>(s, nl, P.tw); return;
+    case 384: ct_fft<384, INV, false, 384, 1>(s, nl, P.tw); return;
+    case 512: ct_fft<512, INV, false, 512, 1>(s, nl, P.tw); return;
+    case 768: ct_fft<768, INV, false, 768, 1>(s, nl, P.tw); return;
+    case 1024: ct_fft<1024, INV, false, 1024, 1>(s, nl, P.tw); return;
+    case 1536: ct_fft<1536, INV, false, 1536, 1>(s, nl, P.tw); return;
+    case 2048: ct_fft<2048, INV, false, 2048, 1>(s, nl, P.tw); return;
+    default: fft_lines<INV>(s, nl, P.n, 1, false, P); return;
+  }
+}
+
+// Columns: TC lines side by side (lstride 1, estride TC).
+template <bool INV, int TC>
+__device__ void fft_cols(float2* s, const FftPlan& P) {
+  switch (P.n) {
+    case 256: ct_fft<256, INV, true, 1, TC>(s, TC, P.tw); return;
+    case 384: ct_fft<384, INV, true, 1, TC>(s, TC, P.tw); return;
+    case 512: ct_fft<512, INV, true, 1, TC>(s, TC, P.tw); return;
+    case 768: ct_fft<768, INV, true, 1, TC>(s, TC, P.tw); return;
+    case 1024: ct_fft<1024, INV, true, 1, TC>(s, TC, P.tw); return;
+    case 1536: ct_fft<1536, INV, true, 1, TC>(s, TC, P.tw); return;
+    case 2048: ct_fft<2048, INV, true, 1, TC>(s, TC, P.tw); return;
+    default: fft_lines<INV>(s, TC, 1, TC, true, P); return;
+  }
+}
+
 // Host-side radix plan: n = 2^a 3^b, 8 <= n <= 2048.  Powers of two are split
 // into 8s with 4s and 2s so that stages stay balanced (1024 = 8*8*4*4).
 __host__ __device__ inline bool nsr_make_radices(int n, int* radix, int* nst) {

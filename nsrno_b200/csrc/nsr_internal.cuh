@@ -19,6 +19,3 @@ int nsr_cols_tc(const NsrGrid* g);
 size_t nsr_cols_smem(const NsrGrid* g);
 int nsr_rows_per_cta(const NsrGrid* g);
 
-__global__ void k_prec_cols(Geo g, PrecTables t, const double* __restrict__ freq,
-                            const int* __restrict__ sys_of_slot, float2* __restrict__ w,
-                            double shift, int adjoint, int tc);

@@ -157,49 +157,44 @@ size_t nsr_prec_table_bytes(const NsrGrid* g) {
 
 // Column pass: forward DIF along z, multiply by the shifted-Laplace symbol in
 // the digit-reversed domain, inverse along z.  In place on w.
-__global__ void __launch_bounds__(256) k_prec_cols(Geo g, PrecTables t, const double* __restrict__ freq,
-                                                   const int* __restrict__ sys_of_slot, float2* __restrict__ w,
-                                                   double shift, int adjoint, int tc) {
+template <int TC>
+__global__ void __launch_bounds__(512) k_prec_cols(Geo g, PrecTables t, const double* __restrict__ freq,
+                                                   float2* __restrict__ w, double shift, int adjoint) {
   extern __shared__ float2 sm[];
-  const int slot = blockIdx.y;
-  int sysi = slot;
-  if (sys_of_slot) {
-    sysi = sys_of_slot[slot];
-    if (sysi < 0) return;
-  }
+  const int sysi = blockIdx.y;
   const long long n = (long long)g.nz * g.nx;
-  float2* ws = w + slot * n;
-  const int c0 = blockIdx.x * tc;
-  const int ncol = min(tc, g.nx - c0);
-  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
-    int z = k / tc, c = k - z * tc;
-    if (c < ncol) sm[k] = ws[(long long)z * g.nx + c0 + c];
+  float2* ws = w + sysi * n;
+  const int c0 = blockIdx.x * TC;
+  const int ncol = min(TC, g.nx - c0);
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
+    sm[k] = c < ncol ? ws[(long long)z * g.nx + c0 + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_lines<false>(sm, tc, 1, tc, true, t.pz);
+  fft_cols<false, TC>(sm, t.pz);
   const SysScalars s = sys_scalars(g, freq[sysi]);
   const float kh2 = (float)s.kh2;
   const float inv_n = 1.0f / (float)n;
-  const float2 shiftc = make_float2(kh2, (float)(kh2 * shift));
-  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
-    int z = k / tc, c = k - z * tc;
+  const float2 shiftc = make_float2(kh2, (float)(s.kh2 * shift));
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
     if (c < ncol) {
-      float sym = -4.0f * (t.s2z[z] + t.s2x[c0 + c]);
-      float2 den = make_float2(sym + shiftc.x, shiftc.y);
-      float2 mul = divc(make_float2(inv_n, 0.f), den);
+      const float sym = -4.0f * (t.s2z[z] + t.s2x[c0 + c]);
+      float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
       if (adjoint) mul = conjc(mul);
       sm[k] = sm[k] * mul;
     }
   }
   __syncthreads();
-  fft_lines<true>(sm, tc, 1, tc, true, t.pz);
-  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
-    int z = k / tc, c = k - z * tc;
+  fft_cols<true, TC>(sm, t.pz);
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
     if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];
   }
 }
 
 int nsr_cols_tc(const NsrGrid* g) { return g->nz <= 1024 ? 16 : 8; }
+int nsr_cols_threads() { return 512; }
 size_t nsr_cols_smem(const NsrGrid* g) { return sizeof(float2) * (size_t)g->nz * nsr_cols_tc(g); }
 
 // Stand-alone row passes of nsr_precondition.
@@ -212,7 +207,7 @@ __global__ void __launch_bounds__(256) k_prec_rows_fwd(Geo g, PrecTables t, cons
   const float2* xs = x + blockIdx.y * n + (long long)z0 * g.nx;
   for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) sm[k] = xs[k];
   __syncthreads();
-  fft_lines<false>(sm, nr, g.nx, 1, false, t.px);
+  fft_rows<false>(sm, nr, t.px);
   float2* ws = w + blockIdx.y * n + (long long)z0 * g.nx;
   for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) ws[k] = sm[k];
 }
@@ -226,7 +221,7 @@ __global__ void __launch_bounds__(256) k_prec_rows_inv(Geo g, PrecTables t, cons
   const float2* ws = w + blockIdx.y * n + (long long)z0 * g.nx;
   for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) sm[k] = ws[k];
   __syncthreads();
-  fft_lines<true>(sm, nr, g.nx, 1, false, t.px);
+  fft_rows<true>(sm, nr, t.px);
   float2* ys = y + blockIdx.y * n + (long long)z0 * g.nx;
   for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) ys[k] = sm[k];
 }
@@ -257,8 +252,13 @@ extern "C" int nsr_precondition(const NsrGrid* grid, const double* freq_hz, int3
   const int tc = nsr_cols_tc(grid);
   dim3 gc((grid->nx + tc - 1) / tc, n_systems);
   size_t csm = nsr_cols_smem(grid);
-  cudaFuncSetAttribute(k_prec_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
-  k_prec_cols<<<gc, 256, csm, st>>>(g, t, freq_hz, nullptr, w, shift, adjoint, tc);
+  if (tc == 16) {
+    cudaFuncSetAttribute(k_prec_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+    k_prec_cols<16><<<gc, 512, csm, st>>>(g, t, freq_hz, w, shift, adjoint);
+  } else {
+    cudaFuncSetAttribute(k_prec_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+    k_prec_cols<8><<<gc, 512, csm, st>>>(g, t, freq_hz, w, shift, adjoint);
+  }
   k_prec_rows_inv<<<gr, 256, row_smem, st>>>(g, t, w, (float2*)y, rows);
   return last_error();
 }

@@ -27,11 +27,13 @@
 
 enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES = 4, MODE_EMIT = 5 };
 #define NSR_NPART 8
+#define NSR_LAUNCHES_PER_IT 7
 
 struct __align__(16) SlotState {
   int sys, mode, iters, final_reason;
-  int xpar, zero_rhs, pad0, pad1;
-  double bnorm2, rnorm2, resid;
+  int xpar, zero_rhs, restart, force_restart;
+  int breakdowns, pad_b0, pad_b1, pad_b2;   // consecutive restarts forced by a breakdown
+  double bnorm2, rnorm2, resid, r0norm2;
   double freq, angle;
   double2 rho, alpha, omega, beta;
   // s = r + c_sv v ; r_new = s + c_rt t ; y += c_yp p + c_ys s ; p_new = r_new + c_pp p + c_pv v
@@ -66,6 +68,7 @@ struct SolveArgs {
   int nb_inv;    // inv CTAs per slot
   double tol2;
   double shift;
+  double restart2;   // squared restart factor
   int max_it;
   int replace_every;
   int adjoint;
@@ -76,9 +79,16 @@ struct SolveArgs {
   float2* fields;
 };
 
-__device__ __forceinline__ bool active_in(int mode, int half) {
-  return (half == 0 && mode == MODE_ITER_A) || (half == 1 && mode == MODE_ITER_B) || mode == MODE_RES ||
-         mode == MODE_INIT || mode == MODE_EMIT;
+// Which slots a launch serves.  The first half of an iteration runs only the
+// ITER_A work; the second half runs ITER_B and every FP64 residual, start and
+// emit pass.  A mode written by a finalize therefore never becomes active in
+// the half that wrote it.
+__device__ __forceinline__ bool fwd_active(int mode, int half) {
+  return half == 0 ? mode == MODE_ITER_A
+                   : (mode == MODE_ITER_B || mode == MODE_RES || mode == MODE_INIT || mode == MODE_EMIT);
+}
+__device__ __forceinline__ bool cols_active(int mode, int half) {
+  return half == 0 ? mode == MODE_ITER_A : (mode == MODE_ITER_B || mode == MODE_RES);
 }
 
 __device__ __forceinline__ float2 f2(double2 a) { return make_float2((float)a.x, (float)a.y); }
@@ -93,7 +103,7 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
   const int slot = blockIdx.y;
   const SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
-  if (!active_in(mode, half)) return;
+  if (!fwd_active(mode, half)) return;
   const Geo& g = A.g;
   const long long n = (long long)g.nz * g.nx;
   const int z0 = blockIdx.x * A.rows;
@@ -116,6 +126,8 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
   }
   const float2 sv = f2(S.c_sv), rt = f2(S.c_rt), yp = f2(S.c_yp), ys = f2(S.c_ys), pp = f2(S.c_pp), pv = f2(S.c_pv);
   if (mode == MODE_ITER_A) {
+    const bool restart = S.restart != 0;
+    float2* rh = A.B.rh + off;
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
       const float2 rk = r[k], vk = v[k], tk = t[k], pk = p[k], yk = y[k];
       const float2 s = rk + sv * vk;
@@ -123,6 +135,7 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
       const float2 yn = yk + yp * pk + ys * s;
       const float2 pn = rn + pp * pk + pv * vk;
       r[k] = rn; p[k] = pn; y[k] = yn;
+      if (restart) rh[k] = rn;
       sm[k] = pn;
     }
   } else if (mode == MODE_ITER_B) {
@@ -135,7 +148,7 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
     }
   }
   __syncthreads();
-  fft_lines<false>(sm, nr, g.nx, 1, false, A.tab.px);
+  fft_rows<false>(sm, nr, A.tab.px);
   float2* w = A.B.w + off;
   for (int k = threadIdx.x; k < cnt; k += blockDim.x) w[k] = sm[k];
 }
@@ -143,40 +156,40 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
 // ---------------------------------------------------------------------------
 // cols: column FFT, preconditioner multiply, inverse column FFT (in place).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_cols(SolveArgs A, int half) {
+template <int TC>
+__global__ void __launch_bounds__(512) k_cols(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
   const int slot = blockIdx.y;
   const int mode = A.B.slots[slot].mode;
-  if (!((half == 0 && mode == MODE_ITER_A) || (half == 1 && mode == MODE_ITER_B) || mode == MODE_RES)) return;
+  if (!cols_active(mode, half)) return;
   const Geo& g = A.g;
   const long long n = (long long)g.nz * g.nx;
   float2* ws = A.B.w + slot * n;
-  const int tc = A.tc;
-  const int c0 = blockIdx.x * tc;
-  const int ncol = min(tc, g.nx - c0);
-  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
-    int z = k / tc, c = k - z * tc;
+  const int c0 = blockIdx.x * TC;
+  const int ncol = min(TC, g.nx - c0);
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
     sm[k] = c < ncol ? ws[(long long)z * g.nx + c0 + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_lines<false>(sm, tc, 1, tc, true, A.tab.pz);
+  fft_cols<false, TC>(sm, A.tab.pz);
   const SysScalars s = sys_scalars(g, A.B.slots[slot].freq);
   const float kh2 = (float)s.kh2;
   const float inv_n = 1.0f / (float)n;
   const float2 shiftc = make_float2(kh2, (float)(s.kh2 * A.shift));
-  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
-    int z = k / tc, c = k - z * tc;
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
     if (c < ncol) {
-      float sym = -4.0f * (A.tab.s2z[z] + A.tab.s2x[c0 + c]);
+      const float sym = -4.0f * (A.tab.s2z[z] + A.tab.s2x[c0 + c]);
       float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
       if (A.adjoint) mul = conjc(mul);
       sm[k] = sm[k] * mul;
     }
   }
   __syncthreads();
-  fft_lines<true>(sm, tc, 1, tc, true, A.tab.pz);
-  for (int k = threadIdx.x; k < g.nz * tc; k += blockDim.x) {
-    int z = k / tc, c = k - z * tc;
+  fft_cols<true, TC>(sm, A.tab.pz);
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
     if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];
   }
 }
@@ -263,6 +276,10 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
     if (!isfinite(rel2)) { finish_system(A, S, NSR_NONFINITE, rel2); return; }
     if (rel2 < tol2) { finish_system(A, S, NSR_CONVERGED, sqrt(rel2)); return; }
     S.rho = make_double2(S.rnorm2, 0.0);
+    S.r0norm2 = S.rnorm2;
+    S.restart = 0;
+    S.force_restart = 0;
+    S.breakdowns = 0;
     S.alpha = S.omega = S.beta = make_double2(0.0, 0.0);
     const double2 z = make_double2(0.0, 0.0);
     S.c_sv = S.c_rt = S.c_yp = S.c_ys = S.c_pp = S.c_pv = z;
@@ -272,9 +289,14 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
   if (mode == MODE_ITER_A) {
     const double2 sigma = make_double2(sum[0], sum[1]);
     const double z2 = abs2(sigma);
+    S.restart = 0;
     if (!finite2(sigma) || !(z2 > 1e-60 * S.bnorm2 * S.bnorm2)) {
-      S.final_reason = NSR_BREAKDOWN;
+      // Lanczos breakdown: restart from the true residual (twice in a row: give up)
+      if (S.breakdowns >= 2 || !finite2(sigma)) S.final_reason = finite2(sigma) ? NSR_BREAKDOWN : NSR_NONFINITE;
+      S.force_restart = 1;
+      S.breakdowns += 1;
       S.c_sv = S.c_yp = S.c_ys = make_double2(0.0, 0.0);
+      S.omega = make_double2(0.0, 0.0);
       S.mode = MODE_RES;
       return;
     }
@@ -319,10 +341,14 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
       S.rho = rho_new;
       S.c_pp = S.beta;
       S.c_pv = make_double2(0.0, 0.0) - S.beta * omega;
+      S.breakdowns = 0;
     } else {
-      S.final_reason = NSR_BREAKDOWN;
+      // rho or omega vanished: restart from the true residual (three in a row: give up)
+      if (S.breakdowns >= 2) S.final_reason = NSR_BREAKDOWN;
+      S.force_restart = 1;
+      S.breakdowns += 1;
     }
-    if (S.final_reason >= 0 || S.rnorm2 < tol2 * S.bnorm2 || S.iters >= A.max_it ||
+    if (S.force_restart || S.final_reason >= 0 || S.rnorm2 < tol2 * S.bnorm2 || S.iters >= A.max_it ||
         (A.replace_every > 0 && S.iters % A.replace_every == 0)) {
       if (S.iters >= A.max_it && S.final_reason < 0) S.final_reason = NSR_ITERATION_BUDGET;
       S.mode = MODE_RES;
@@ -345,6 +371,17 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
     if (S.iters >= A.max_it) { finish_system(A, S, NSR_ITERATION_BUDGET, rel); return; }
     const double2 z = make_double2(0.0, 0.0);
     S.c_sv = S.c_rt = S.c_yp = S.c_ys = z;
+    if (S.force_restart || (A.restart2 > 0.0 && rr < A.restart2 * S.r0norm2)) {
+      // Restart: fresh shadow vector rhat = r (written by the next fwd pass), p = r.
+      S.restart = 1;
+      S.force_restart = 0;
+      S.r0norm2 = rr;
+      S.rho = make_double2(rr, 0.0);
+      S.rnorm2 = rr;
+      S.c_pp = S.c_pv = z;
+      S.mode = MODE_ITER_A;
+      return;
+    }
     if (abs2(S.omega) > 1e-60 && abs2(S.rho) > 0.0) {
       // Replace the recursive residual by the true one and rescale beta.
       S.beta = S.beta * divc(rhr, S.rho);
@@ -362,18 +399,155 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
 }
 
 // ---------------------------------------------------------------------------
-// inv: inverse row FFT + stencil + inner products; INIT/RES do the FP64
-// true residual instead.
+// Per-CTA partials, arrival, and the last CTA's finalize (no waiting).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reduce_and_finalize(const SolveArgs& A, SlotState& S, int slot, int mode,
+                                                    double* acc) {
+  __shared__ double red[NSR_NPART];
+  __shared__ double tot[NSR_NPART];
+  __shared__ int am_last;
+  block_sum<NSR_NPART>(acc, red);
+  double* part = A.B.partials + (long long)slot * A.nb_inv * NSR_NPART;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < NSR_NPART; ++q) part[blockIdx.x * NSR_NPART + q] = red[q];
+    __threadfence();
+    const int prev = atomicAdd(&A.B.arrive[slot], 1);
+    am_last = (prev == (int)gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  // Deterministic sum over CTAs: thread q sums column q in CTA order.
+  if (threadIdx.x < NSR_NPART) {
+    double sacc = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) sacc += __ldcg(&part[b * NSR_NPART + threadIdx.x]);
+    tot[threadIdx.x] = sacc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    A.B.arrive[slot] = 0;
+    finalize(A, S, mode, tot);
+    __threadfence();
+  }
+}
+
+// Stencil at an explicit 5-point neighbourhood.  Interior nodes (all six
+// stretches equal to one) take the real-flux path.
+template <bool ADJ>
+__device__ __forceinline__ float2 stencil_pts(const Geo& g, const SysScalars& sc, int i, int j, float a_c, float a_e,
+                                              float a_w, float a_s, float a_n, float b_c, float t_c, float2 pc,
+                                              float2 pe, float2 pw, float2 ps, float2 pn) {
+  const bool inner = i > g.n_pml && i < g.nz - 1 - g.n_pml && j > g.n_pml && j < g.nx - 1 - g.n_pml;
+  if (inner) {
+    const float e = t_c * (float)sc.fpow;
+    const float mb = (float)sc.kh2 * b_c;
+    const float2 mass = make_float2(mb * (1.0f - e * e), (ADJ ? -2.0f : 2.0f) * mb * e);
+    float2 y = mass * pc;
+    y = y + (0.5f * (a_c + a_e)) * (pe - pc);
+    y = y + (0.5f * (a_c + a_w)) * (pw - pc);
+    y = y + (0.5f * (a_c + a_s)) * (ps - pc);
+    y = y + (0.5f * (a_c + a_n)) * (pn - pc);
+    return y;
+  }
+  auto P = [&](int i2, int j2) -> float2 {
+    if (i2 == i && j2 == j) return pc;
+    if (i2 == i) return j2 > j ? pe : pw;
+    return i2 > i ? ps : pn;
+  };
+  auto Aa = [&](int i2, int j2) -> float {
+    if (i2 == i && j2 == j) return a_c;
+    if (i2 == i) return j2 > j ? a_e : a_w;
+    return i2 > i ? a_s : a_n;
+  };
+  return stencil<float, ADJ>(g, sc, i, j, b_c, t_c, P, Aa);
+}
+
+// ---------------------------------------------------------------------------
+// inv: inverse row FFT + stencil + inner products of the Krylov halves.
 // ---------------------------------------------------------------------------
 template <bool ADJ>
 __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
-  __shared__ double red[NSR_NPART];
-  __shared__ int am_last;
   const int slot = blockIdx.y;
   SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
-  if (!active_in(mode, half)) return;
+  if (mode != (half == 0 ? MODE_ITER_A : MODE_ITER_B)) return;
+  const Geo& g = A.g;
+  const long long n = (long long)g.nz * g.nx;
+  const int z0 = blockIdx.x * A.tz;
+  const int nb = min(A.tz, g.nz - z0);
+  const int nx = g.nx;
+  const long long soff = slot * n;
+  {
+    const float2* w = A.B.w + soff;
+    const int nl = nb + 2;
+    for (int rr = 0; rr < nl; ++rr) {
+      const int z = z0 - 1 + rr;
+      const bool in = z >= 0 && z < g.nz;
+      for (int j = threadIdx.x; j < nx; j += blockDim.x)
+        sm[rr * nx + j] = in ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_rows<true>(sm, nl, A.tab.px);
+  }
+  const SysScalars sc = sys_scalars(g, S.freq);
+  const float* ca = A.coef;
+  const float* cb = A.coef + n;
+  const float* ct = A.coef + 2 * n;
+  const float2* rh = A.B.rh + soff;
+  double acc[NSR_NPART];
+#pragma unroll
+  for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
+  const float2 sv = f2(S.c_sv);
+  float2* out = (half == 0 ? A.B.v : A.B.t) + soff;
+  const float2* r = A.B.r + soff;
+  const float2* v = A.B.v + soff;
+  for (int rr = 0; rr < nb; ++rr) {
+    const int i = z0 + rr;
+    const float2* row = sm + (rr + 1) * nx;
+    const float2* up = sm + rr * nx;
+    const float2* dn = sm + (rr + 2) * nx;
+    for (int j = threadIdx.x; j < nx; j += blockDim.x) {
+      const long long idx = (long long)i * nx + j;
+      const float2 z = make_float2(0.f, 0.f);
+      const float2 pc = row[j];
+      const float2 pe = j + 1 < nx ? row[j + 1] : z;
+      const float2 pw = j > 0 ? row[j - 1] : z;
+      const float a_c = __ldg(&ca[idx]);
+      const float a_e = j + 1 < nx ? __ldg(&ca[idx + 1]) : 1.0f;
+      const float a_w = j > 0 ? __ldg(&ca[idx - 1]) : 1.0f;
+      const float a_s = i + 1 < g.nz ? __ldg(&ca[idx + nx]) : 1.0f;
+      const float a_n = i > 0 ? __ldg(&ca[idx - nx]) : 1.0f;
+      const float2 av = stencil_pts<ADJ>(g, sc, i, j, a_c, a_e, a_w, a_s, a_n, __ldg(&cb[idx]), __ldg(&ct[idx]),
+                                         pc, pe, pw, dn[j], up[j]);
+      out[idx] = av;
+      const float2 rk = rh[idx];
+      if (half == 0) {
+        dot_acc(acc[0], acc[1], rk, av);       // <rhat, v>
+      } else {
+        const float2 s = r[idx] + sv * v[idx];
+        dot_acc(acc[0], acc[1], av, s);        // <t, s>
+        acc[2] += (double)av.x * av.x + (double)av.y * av.y;
+        acc[3] += (double)s.x * s.x + (double)s.y * s.y;
+        dot_acc(acc[4], acc[5], rk, av);       // <rhat, t>
+        dot_acc(acc[6], acc[7], rk, s);        // <rhat, s>
+      }
+    }
+  }
+  reduce_and_finalize(A, S, slot, mode, acc);
+}
+
+// ---------------------------------------------------------------------------
+// res: FP64 true residual r = b - A x of a replacement (x += M^-1 y) or of a
+// new system (x = x0); emit passes only arrive and hand the slot on.
+// ---------------------------------------------------------------------------
+template <bool ADJ>
+__global__ void __launch_bounds__(256) k_res(SolveArgs A) {
+  extern __shared__ float2 sm[];
+  const int slot = blockIdx.y;
+  SlotState& S = A.B.slots[slot];
+  const int mode = S.mode;
+  if (!(mode == MODE_RES || mode == MODE_INIT || mode == MODE_EMIT)) return;
   const Geo& g = A.g;
   const long long n = (long long)g.nz * g.nx;
   const int tz = A.tz;
@@ -384,10 +558,6 @@ __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
   const float* ca = A.coef;
   const float* cb = A.coef + n;
   const float* ct = A.coef + 2 * n;
-  auto Aa32 = [&](int i2, int j2) -> float {
-    if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return 1.0f;
-    return __ldg(&ca[(long long)i2 * nx + j2]);
-  };
   auto Aa64 = [&](int i2, int j2) -> double {
     if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return 1.0;
     return (double)__ldg(&ca[(long long)i2 * nx + j2]);
@@ -396,9 +566,7 @@ __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
 #pragma unroll
   for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
   const long long soff = slot * n;
-  const bool need_fft = (mode == MODE_ITER_A || mode == MODE_ITER_B || mode == MODE_RES);
-  if (need_fft) {
-    // rows z0-1 .. z0+nb of w into shared memory (zero outside the grid)
+  if (mode == MODE_RES) {
     const float2* w = A.B.w + soff;
     const int nl = nb + 2;
     for (int k = threadIdx.x; k < nl * nx; k += blockDim.x) {
@@ -407,43 +575,9 @@ __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
       sm[k] = (z >= 0 && z < g.nz) ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_lines<true>(sm, nl, nx, 1, false, A.tab.px);
+    fft_rows<true>(sm, nl, A.tab.px);
   }
-  if (mode == MODE_ITER_A || mode == MODE_ITER_B) {
-    auto P = [&](int i2, int j2) -> float2 {
-      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return make_float2(0.f, 0.f);
-      return sm[(i2 - z0 + 1) * nx + j2];
-    };
-    const float2* rh = A.B.rh + soff;
-    if (mode == MODE_ITER_A) {
-      float2* v = A.B.v + soff;
-      for (int k = threadIdx.x; k < nb * nx; k += blockDim.x) {
-        const int i = z0 + k / nx, j = k % nx;
-        const long long idx = (long long)i * nx + j;
-        const float2 av = stencil<float, ADJ>(g, sc, i, j, __ldg(&cb[idx]), __ldg(&ct[idx]), P, Aa32);
-        v[idx] = av;
-        dot_acc(acc[0], acc[1], rh[idx], av);
-      }
-    } else {
-      float2* t = A.B.t + soff;
-      const float2* r = A.B.r + soff;
-      const float2* v = A.B.v + soff;
-      const float2 sv = f2(S.c_sv);
-      for (int k = threadIdx.x; k < nb * nx; k += blockDim.x) {
-        const int i = z0 + k / nx, j = k % nx;
-        const long long idx = (long long)i * nx + j;
-        const float2 at = stencil<float, ADJ>(g, sc, i, j, __ldg(&cb[idx]), __ldg(&ct[idx]), P, Aa32);
-        t[idx] = at;
-        const float2 s = r[idx] + sv * v[idx];
-        const float2 rk = rh[idx];
-        dot_acc(acc[0], acc[1], at, s);        // <t, s>
-        acc[2] += (double)at.x * at.x + (double)at.y * at.y;
-        acc[3] += (double)s.x * s.x + (double)s.y * s.y;
-        dot_acc(acc[4], acc[5], rk, at);       // <rhat, t>
-        dot_acc(acc[6], acc[7], rk, s);        // <rhat, s>
-      }
-    }
-  } else if (mode == MODE_RES || mode == MODE_INIT) {
+  if (mode == MODE_RES || mode == MODE_INIT) {
     const double2* xo = A.B.x + (2LL * slot + S.xpar) * n;
     double2* xn = A.B.x + (2LL * slot + (S.xpar ^ 1)) * n;
     const float2* x0 = (A.x0 && S.sys >= 0) ? A.x0 + (long long)S.sys * n : nullptr;
@@ -485,32 +619,9 @@ __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
       }
     }
   }
-  // ---- per-CTA partials, arrival, last-CTA finalize -------------------------
-  block_sum<NSR_NPART>(acc, red);
-  double* part = A.B.partials + (long long)slot * A.nb_inv * NSR_NPART;
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < NSR_NPART; ++q) part[blockIdx.x * NSR_NPART + q] = red[q];
-    __threadfence();
-    const int prev = atomicAdd(&A.B.arrive[slot], 1);
-    am_last = (prev == (int)gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  // Deterministic sum over CTAs: thread q sums column q in CTA order.
-  __shared__ double tot[NSR_NPART];
-  if (threadIdx.x < NSR_NPART) {
-    double s = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(&part[b * NSR_NPART + threadIdx.x]);
-    tot[threadIdx.x] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    A.B.arrive[slot] = 0;
-    finalize(A, S, mode, tot);
-    __threadfence();
-  }
+  reduce_and_finalize(A, S, slot, mode, acc);
 }
+
 
 __global__ void k_solve_init(SolveArgs A, int n_slots) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -603,7 +714,8 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
   if (!residual || !iterations || !status || !workspace) return NSR_ERR_ARGUMENT;
   const int n_slots = params->n_slots;
   if (n_slots <= 0 || n_slots > 65535 || params->max_iterations <= 0 || !(params->tolerance > 0) ||
-      !(params->shift >= 0) || params->replace_every < 0) return NSR_ERR_ARGUMENT;
+      !(params->shift >= 0) || params->replace_every < 0 || !(params->restart_factor >= 0) ||
+      params->restart_factor >= 1.0) return NSR_ERR_ARGUMENT;
   if (n_systems == 0) return 0;
   const Layout L = layout(grid, n_slots);
   if (workspace_bytes < L.total) return NSR_ERR_WORKSPACE;
@@ -661,6 +773,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
     A.tz = band_rows(grid);
     A.nb_inv = L.nb_inv;
     A.tol2 = params->tolerance * params->tolerance;
+    A.restart2 = params->restart_factor * params->restart_factor;
     A.shift = params->shift;
     A.max_it = params->max_iterations;
     A.replace_every = params->replace_every;
@@ -675,9 +788,12 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
     const size_t col_smem = nsr_cols_smem(grid);
     const size_t inv_smem = sizeof(float2) * (A.tz + 2) * grid->nx;
     NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(k_inv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
     NSR_TRY(cudaFuncSetAttribute(k_inv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_res<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_res<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
 
     k_solve_init<<<64, 256, 0, st>>>(A, n_slots);
     NSR_TRY(cudaGetLastError());
@@ -687,11 +803,24 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
     const dim3 g_col((grid->nx + A.tc - 1) / A.tc, n_slots);
     const dim3 g_inv(L.nb_inv, n_slots);
     const int K = params->graph_iterations > 0 ? params->graph_iterations : 16;
-    auto launch_half = [&](int half, int which) {
-      if (which == 0) k_fwd<<<g_fwd, 256, fwd_smem, st>>>(A, half);
-      else if (which == 1) k_cols<<<g_col, 256, col_smem, st>>>(A, half);
-      else if (A.adjoint) k_inv<true><<<g_inv, 256, inv_smem, st>>>(A, half);
-      else k_inv<false><<<g_inv, 256, inv_smem, st>>>(A, half);
+    // One iteration = 7 launches: fwd, cols, inv of the first half, then fwd,
+    // cols, res, inv of the second half.
+    const int seq_half[NSR_LAUNCHES_PER_IT] = {0, 0, 0, 1, 1, 1, 1};
+    const int seq_kind[NSR_LAUNCHES_PER_IT] = {0, 1, 3, 0, 1, 2, 3};
+    auto launch = [&](int q) {
+      const int half = seq_half[q], which = seq_kind[q];
+      if (which == 0) {
+        k_fwd<<<g_fwd, 256, fwd_smem, st>>>(A, half);
+      } else if (which == 1) {
+        if (A.tc == 16) k_cols<16><<<g_col, 512, col_smem, st>>>(A, half);
+        else k_cols<8><<<g_col, 512, col_smem, st>>>(A, half);
+      } else if (which == 2) {
+        if (A.adjoint) k_res<true><<<g_inv, 256, inv_smem, st>>>(A);
+        else k_res<false><<<g_inv, 256, inv_smem, st>>>(A);
+      } else {
+        if (A.adjoint) k_inv<true><<<g_inv, 256, inv_smem, st>>>(A, half);
+        else k_inv<false><<<g_inv, 256, inv_smem, st>>>(A, half);
+      }
     };
 
     NSR_TRY(cudaEventCreate(&ev_loop[0]));
@@ -702,25 +831,23 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
     if (P < 0) P = 0;
     if (P > 256) P = 256;
     if (P > 0) {
-      n_prof_events = 6 * P + 1;
+      n_prof_events = NSR_LAUNCHES_PER_IT * P + 1;
       ev_prof = (cudaEvent_t*)calloc(n_prof_events, sizeof(cudaEvent_t));
       if (!ev_prof) { err = (int)cudaErrorMemoryAllocation; goto cleanup; }
       for (int e = 0; e < n_prof_events; ++e) NSR_TRY(cudaEventCreate(&ev_prof[e]));
       NSR_TRY(cudaEventRecord(ev_prof[0], st));
       for (int it = 0; it < P; ++it)
-        for (int half = 0; half < 2; ++half)
-          for (int which = 0; which < 3; ++which) {
-            launch_half(half, which);
-            NSR_TRY(cudaGetLastError());
-            NSR_TRY(cudaEventRecord(ev_prof[1 + it * 6 + half * 3 + which], st));
-          }
-      launches += 6LL * P;
+        for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) {
+          launch(q);
+          NSR_TRY(cudaGetLastError());
+          NSR_TRY(cudaEventRecord(ev_prof[1 + it * NSR_LAUNCHES_PER_IT + q], st));
+        }
+      launches += (long long)NSR_LAUNCHES_PER_IT * P;
     }
 
     NSR_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < K; ++it)
-      for (int half = 0; half < 2; ++half)
-        for (int which = 0; which < 3; ++which) launch_half(half, which);
+      for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) launch(q);
     ce = cudaStreamEndCapture(st, &graph);
     if (ce != cudaSuccess) { err = (int)ce; goto cleanup; }
     NSR_TRY(cudaGraphInstantiate(&exec, graph, 0));
@@ -736,7 +863,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
     while (launched < max_launch) {
       NSR_TRY(cudaGraphLaunch(exec, st));
       ++graph_launches;
-      launches += 6LL * K;
+      launches += (long long)NSR_LAUNCHES_PER_IT * K;
       const int slot_i = (int)(launched & 1);
       NSR_TRY(cudaMemcpyAsync(&host[slot_i], A.B.done, sizeof(int), cudaMemcpyDeviceToHost, st));
       NSR_TRY(cudaEventRecord(ev_poll[slot_i], st));
@@ -762,13 +889,14 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
       stats->graph_launches = graph_launches;
       // Skip the first two profiled iterations (slot initialisation).
       for (int it = (P > 2 ? 2 : 0); it < P; ++it)
-        for (int k = 0; k < 6; ++k) {
+        for (int k = 0; k < NSR_LAUNCHES_PER_IT; ++k) {
           float d = 0.f;
-          NSR_TRY(cudaEventElapsedTime(&d, ev_prof[it * 6 + k], ev_prof[it * 6 + k + 1]));
+          NSR_TRY(cudaEventElapsedTime(&d, ev_prof[it * NSR_LAUNCHES_PER_IT + k],
+                                       ev_prof[it * NSR_LAUNCHES_PER_IT + k + 1]));
           stats->kernel_ms[k] += d;
           stats->kernel_timed[k] += 1;
         }
-      for (int k = 0; k < 6; ++k)
+      for (int k = 0; k < NSR_LAUNCHES_PER_IT; ++k)
         if (stats->kernel_timed[k]) stats->kernel_ms[k] /= stats->kernel_timed[k];
     }
     NSR_TRY(cudaEventRecord(ev_out, st));

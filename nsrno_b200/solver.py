@@ -18,6 +18,7 @@ from . import _lib
 
 DEFAULT_SHIFT = 0.15          # shifted-Laplace shift of nsrno/dense_wave.py:194
 DEFAULT_REPLACE = 40          # true-residual period of nsrno/dense_wave.py:143
+DEFAULT_RESTART = 1e-2        # restart BiCGSTAB after a 100x true-residual reduction
 
 
 def _require_cuda(t: torch.Tensor, name: str):
@@ -128,7 +129,7 @@ _default_ws = Workspace()
 def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tolerance=1e-6,
                   max_iterations=2000, shift=DEFAULT_SHIFT, replace_every=DEFAULT_REPLACE, n_slots=16,
                   adjoint=False, return_fields=False, rx_index=None, graph_iterations=16,
-                  profile_iterations=0, workspace: Workspace | None = None,
+                  profile_iterations=0, restart_factor=DEFAULT_RESTART, workspace: Workspace | None = None,
                   out: BatchResult | None = None) -> BatchResult:
     """Solve every (frequency, angle) system of a record with batched BiCGSTAB.
 
@@ -173,7 +174,8 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                           status=torch.empty(S, dtype=torch.int32, device=dev),
                           fields=torch.empty((S, g.nz, g.nx), dtype=torch.complex64, device=dev)
                           if return_fields else None)
-    params = _lib.NsrSolveParams(float(tolerance), float(shift), int(max_iterations), int(replace_every),
+    params = _lib.NsrSolveParams(float(tolerance), float(shift), float(restart_factor), int(max_iterations),
+                                 int(replace_every),
                                  int(n_slots), int(bool(adjoint)), int(graph_iterations), int(profile_iterations))
     stats = _lib.NsrSolveStats()
     _lib.check(lib.nsr_solve_batched(

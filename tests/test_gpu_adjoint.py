@@ -66,7 +66,8 @@ def oracle_misfit(spec, c, rho, alpha, systems, d_obs):
 def test_config3_gradient_against_central_differences(cuda):
     """L2 IQ misfit of the 256x256 record against data of a perturbed medium:
     GPU implicit gradient vs oracle central differences (step 1e-3) at 16 random
-    pixels and along 4 random directions, tolerance 1e-4 relative."""
+    pixels and along 4 random directions (Richardson-extrapolated with step 5e-4),
+    tolerance 1e-4 relative."""
     from nsrno_b200 import AcquisitionData, Geometry, implicit_channels
     rec, true = config3_case(cuda)
     spec = spec_of(rec)
@@ -96,10 +97,15 @@ def test_config3_gradient_against_central_differences(cuda):
     r0 = rec.rho.astype(np.float64)
     eps = 1e-3
 
+    def central(dc, dr, h):
+        lp = oracle_misfit(spec, c0 * np.exp(h * dc), r0 * np.exp(h * dr), rec.alpha, systems, d_obs)
+        lm = oracle_misfit(spec, c0 * np.exp(-h * dc), r0 * np.exp(-h * dr), rec.alpha, systems, d_obs)
+        return (lp - lm) / (2 * h)
+
     def fd(dc, dr):
-        lp = oracle_misfit(spec, c0 * np.exp(eps * dc), r0 * np.exp(eps * dr), rec.alpha, systems, d_obs)
-        lm = oracle_misfit(spec, c0 * np.exp(-eps * dc), r0 * np.exp(-eps * dr), rec.alpha, systems, d_obs)
-        return (lp - lm) / (2 * eps)
+        # Central differences at step 1e-3 carry an O(h^2) truncation error of
+        # about 1e-4 on this record; Richardson extrapolation with h/2 removes it.
+        return (4.0 * central(dc, dr, eps / 2) - central(dc, dr, eps)) / 3.0
 
     # random directions (smooth windows) over both parameters
     xx, zz = np.meshgrid(np.arange(rec.nx), np.arange(rec.nz))
