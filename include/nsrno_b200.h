@@ -128,6 +128,23 @@ int nsr_precondition(const NsrGrid* grid, const double* freq_hz, int32_t n_syste
                      double shift, int32_t adjoint, const float* x, float* y,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free y = M^-1 x, for callers that cannot allocate device memory
+ * where they need it (for example while another framework captures a CUDA
+ * graph, under a latency budget that forbids the device-wide synchronisation
+ * of cudaMalloc, or inside a host application that owns all device memory).
+ * This entry point has no counterpart in the reference.  Same arguments and
+ * result as nsr_precondition, but its scratch space is a fixed 16 MiB
+ * file-scope device array (held by every GPU that loads the library until the
+ * process exits), so nothing is allocated.  Requests whose
+ * nsr_precondition_workspace_size exceeds 16 MiB return NSR_ERR_CAPACITY
+ * (e.g. at most two 1024 x 768 systems per call).  The first call on a device
+ * looks up the array's device address with that device current; make that
+ * first call before any stream capture.  Every call shares the array and it
+ * keeps the last call's contents: calls that overlap on the GPU (different
+ * streams or threads, same device) race and must be serialised by the caller. */
+int nsr_precondition_noalloc(const NsrGrid* grid, const double* freq_hz, int32_t n_systems,
+                             double shift, int32_t adjoint, const float* x, float* y, void* stream);
+
 /* Plane-wave right-hand side in SI units, b = -line(x)/h^2 on row `face`,
  * line = taper(x) exp(-i k0 x sin(theta)) (nsrno/wave_operator.py:111-115 and
  * theranostic/wave.py:260).  b: c128 [S][nz][nx]. */

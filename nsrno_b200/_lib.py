@@ -16,7 +16,7 @@ REASONS = {CONVERGED: "converged", ITERATION_BUDGET: "iteration_budget", BREAKDO
            DIVERGED: "diverged", NONFINITE: "nonfinite", NOT_RUN: "not_run"}
 
 EXPORTS = ("nsr_version", "nsr_error_string", "nsr_setup_material", "nsr_apply",
-           "nsr_precondition_workspace_size", "nsr_precondition", "nsr_plane_wave_rhs",
+           "nsr_precondition_workspace_size", "nsr_precondition", "nsr_precondition_noalloc", "nsr_plane_wave_rhs",
            "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_grad_accum")
 
 
@@ -68,6 +68,7 @@ def load():
     lib.nsr_precondition_workspace_size.restype = S
     lib.nsr_precondition_workspace_size.argtypes = [G, I]
     lib.nsr_precondition.argtypes = [G, P, I, D, I, P, P, P, S, P]
+    lib.nsr_precondition_noalloc.argtypes = [G, P, I, D, I, P, P, P]
     lib.nsr_plane_wave_rhs.argtypes = [G, P, P, I, P, P]
     lib.nsr_solve_workspace_size.restype = S
     lib.nsr_solve_workspace_size.argtypes = [G, I]
