@@ -78,6 +78,8 @@ typedef struct NsrSolveParams {
   int32_t profile_iterations;/* first iterations launched one by one with CUDA
                                 events between kernels (0: none); their average
                                 durations are reported in NsrSolveStats          */
+  int32_t fields_fp64;       /* 0: fields output is c64; 1: c128 (the FP64 iterate) */
+  int32_t reserved;
 } NsrSolveParams;
 
 /* Optional host-side statistics of one nsr_solve_batched call. */
@@ -98,23 +100,29 @@ int nsr_version(void);
 /* Text for a return code (status, NSR_ERR_* or cudaError_t). */
 const char* nsr_error_string(int code);
 
+/* Size in bytes of the material buffer of a grid (0 for an invalid grid). */
+size_t nsr_material_bytes(const NsrGrid* grid);
+
 /* Material planes: c [m/s], rho [kg/m^3], alpha [dB/cm/MHz^y] (float, [nz,nx])
- * -> coef = three float planes [3][nz][nx]: a = rho0/rho (1 + m_eta),
+ * -> material buffer (nsr_material_bytes bytes): a = rho0/rho (1 + m_eta),
  * b = rho0 c0^2/(rho c^2) (1 + m_kappa), t = attenuation slope with
- * e(f) = t (f/1 MHz)^(y-1) = alpha_Np(f) c / omega.  Computed in double and
- * rounded once.  Replaces the material part of Solver.matrix
- * (theranostic/wave.py:158-180) and of WaveResidualOperator.setup
- * (nsrno/wave_operator.py:48-67). */
+ * e(f) = t (f/1 MHz)^(y-1) = alpha_Np(f) c / omega, computed in double; the
+ * buffer holds them as float planes [3][nz][nx] at offset 0 (for the FP32
+ * Krylov kernels) and as double planes [3][nz][nx] at the next 256-byte
+ * boundary after them (for the FP64 residual, FP64 apply and gradient).
+ * Replaces the material part of Solver.matrix (theranostic/wave.py:158-180)
+ * and of WaveResidualOperator.setup (nsrno/wave_operator.py:48-67). */
 int nsr_setup_material(const NsrGrid* grid, const float* c, const float* rho,
-                       const float* alpha_db, float* coef, void* stream);
+                       const float* alpha_db, void* material, void* stream);
 
 /* y = A x (adjoint = 0) or A^H x (adjoint = 1) for S systems of frequencies
  * freq_hz[S] (device, double), fields [S][nz][nx].  A is the h^2-scaled
  * 5-point operator (the reference matrix of theranostic/wave.py:174-188 times
  * h^2, with the attenuation mass term).  precision 0: c64 in/out, float math;
- * precision 1: c128 in/out, double math.  Replaces Solver.matrix @ x and
+ * precision 1: c128 in/out, double math on the double planes.  Replaces
+ * Solver.matrix @ x and
  * WaveResidualOperator.apply_operator (nsrno/wave_operator.py:105-109). */
-int nsr_apply(const NsrGrid* grid, const float* coef, const double* freq_hz,
+int nsr_apply(const NsrGrid* grid, const void* material, const double* freq_hz,
               int32_t n_systems, int32_t adjoint, int32_t precision,
               const void* x, void* y, void* stream);
 
@@ -156,7 +164,7 @@ int nsr_plane_wave_rhs(const NsrGrid* grid, const double* freq_hz, const double*
  * refill.  Replaces solve_system/bicgstab (nsrno/dense_wave.py:118-148,
  * 167-225) and the GMRES loop of solve_frequency (nsrno/wave_solver.py:38-67)
  * for whole records.
- *   coef          material planes from nsr_setup_material
+ *   material      material buffer from nsr_setup_material
  *   freq_hz[S]    device double
  *   angle_rad[S]  device double (plane-wave source; ignored when rhs != NULL)
  *   rhs           NULL or c64 [S][nz][nx] explicit right-hand sides (SI units)
@@ -164,25 +172,54 @@ int nsr_plane_wave_rhs(const NsrGrid* grid, const double* freq_hz, const double*
  *   rx_index[n_rx] device int32 flat node indices of the receivers
  * Outputs (device): iq c128 [S][n_rx], residual f64 [S] (true relative
  * residual, FP64), iterations i32 [S], status i32 [S] (NSR_CONVERGED ...),
- * fields NULL or c64 [S][nz][nx]; stats NULL or a host NsrSolveStats.
+ * fields NULL or [S][nz][nx] (c64, or c128 when params->fields_fp64);
+ * stats NULL or a host NsrSolveStats.
  * The call synchronises its stream while it polls for completion. */
 size_t nsr_solve_workspace_size(const NsrGrid* grid, int32_t n_slots);
-int nsr_solve_batched(const NsrGrid* grid, const float* coef,
+int nsr_solve_batched(const NsrGrid* grid, const void* material,
                       const double* freq_hz, const double* angle_rad, int32_t n_systems,
                       const float* rhs, const float* x0,
                       const int32_t* rx_index, int32_t n_rx,
                       const NsrSolveParams* params,
                       void* workspace, size_t workspace_bytes,
                       double* iq, double* residual, int32_t* iterations, int32_t* status,
-                      float* fields, NsrSolveStats* stats, void* stream);
+                      void* fields, NsrSolveStats* stats, void* stream);
+
+/* Parameters of nsr_gmres_batched. */
+typedef struct NsrGmresParams {
+  double tolerance;          /* relative true residual ||b-Ax||/||b||          */
+  double shift;              /* shifted-Laplace preconditioner shift (0.15)    */
+  int32_t max_iterations;    /* Arnoldi steps per system                       */
+  int32_t restart;           /* restart length m (1..64)                       */
+  int32_t n_slots;           /* systems per batch                              */
+  int32_t adjoint;           /* 0: A x = b; 1: A^H x = b                       */
+  int32_t fields_fp64;       /* fields output c128 when set, else c64          */
+  int32_t reserved;
+} NsrGmresParams;
+
+/* Restarted right-preconditioned GMRES(m) with two classical Gram-Schmidt
+ * passes, FP64 Hessenberg/Givens recurrence and FP64 true residual at every
+ * restart, for S systems in batches of params->n_slots.  Replaces `gmres`
+ * (nsrno/wave_solver.py:9-36) as used by solve_frequency
+ * (nsrno/wave_solver.py:38-67) and the GMRES path of solve_system
+ * (nsrno/dense_wave.py:212-220).  Arguments and outputs as nsr_solve_batched;
+ * `iterations` counts Arnoldi steps (operator applications).  Synchronises
+ * its stream once per restart cycle. */
+size_t nsr_gmres_workspace_size(const NsrGrid* grid, int32_t n_slots, int32_t restart);
+int nsr_gmres_batched(const NsrGrid* grid, const void* material, const double* freq_hz,
+                      const double* angle_rad, int32_t n_systems, const float* rhs, const float* x0,
+                      const int32_t* rx_index, int32_t n_rx, const NsrGmresParams* params,
+                      void* workspace, size_t workspace_bytes, double* iq, double* residual,
+                      int32_t* iterations, int32_t* status, void* fields, void* stream);
 
 /* g_logc, g_logrho (double [nz][nx]) += -Re(lambda^H dA/dm u) summed over S
- * systems, u and lambda c64 [S][nz][nx] (SI fields), m = log c and log rho.
+ * systems, u and lambda [S][nz][nx] SI fields (precision 0: c64, 1: c128),
+ * m = log c and log rho.
  * The exact derivative of the 5-point discretisation that
  * theranostic/wave.py:331-389 (born_jacobian) forms column by column and
  * nsrno/dense_wave.py:250-255 obtains by autograd. */
-int nsr_grad_accum(const NsrGrid* grid, const float* coef, const double* freq_hz,
-                   int32_t n_systems, const float* u, const float* lam,
+int nsr_grad_accum(const NsrGrid* grid, const void* material, const double* freq_hz,
+                   int32_t n_systems, int32_t precision, const void* u, const void* lam,
                    double* g_logc, double* g_logrho, void* stream);
 
 #ifdef __cplusplus

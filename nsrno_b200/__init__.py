@@ -7,12 +7,12 @@ compute runs in hand-written sm_100a CUDA kernels behind the C ABI of
 ``include/nsrno_b200.h``; this package is the host side.
 """
 from . import _lib
-from .solver import (BatchResult, Geometry, Medium, Workspace, apply, grad_accum, plane_wave_rhs, precondition,
-                     receiver_response, solve_batched)
+from .solver import (BatchResult, Geometry, Medium, Workspace, apply, gmres_batched, grad_accum, plane_wave_rhs,
+                     precondition, receiver_response, solve_batched)
 from .api import (AcquisitionData, HelmholtzSurrogate, HelmholtzSystem, ImplicitChannels, PlaneWaveModel,
                   bin_frequency, implicit_channels, solve_frequency, solve_system)
 
-__all__ = ["BatchResult", "Geometry", "Medium", "Workspace", "apply", "grad_accum", "plane_wave_rhs",
+__all__ = ["BatchResult", "Geometry", "Medium", "Workspace", "apply", "gmres_batched", "grad_accum", "plane_wave_rhs",
            "precondition", "receiver_response", "solve_batched", "AcquisitionData", "HelmholtzSurrogate",
            "HelmholtzSystem", "ImplicitChannels", "PlaneWaveModel", "bin_frequency", "implicit_channels",
            "solve_frequency", "solve_system"]

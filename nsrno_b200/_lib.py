@@ -15,9 +15,10 @@ CONVERGED, ITERATION_BUDGET, BREAKDOWN, DIVERGED, NONFINITE, NOT_RUN = range(6)
 REASONS = {CONVERGED: "converged", ITERATION_BUDGET: "iteration_budget", BREAKDOWN: "breakdown",
            DIVERGED: "diverged", NONFINITE: "nonfinite", NOT_RUN: "not_run"}
 
-EXPORTS = ("nsr_version", "nsr_error_string", "nsr_setup_material", "nsr_apply",
+EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_material", "nsr_apply",
            "nsr_precondition_workspace_size", "nsr_precondition", "nsr_precondition_noalloc", "nsr_plane_wave_rhs",
-           "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_grad_accum")
+           "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_gmres_workspace_size", "nsr_gmres_batched",
+           "nsr_grad_accum")
 
 
 class NsrGrid(ctypes.Structure):
@@ -31,7 +32,15 @@ class NsrSolveParams(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double), ("restart_factor", ctypes.c_double),
                 ("max_iterations", ctypes.c_int32), ("replace_every", ctypes.c_int32),
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
-                ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32)]
+                ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32),
+                ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class NsrGmresParams(ctypes.Structure):
+    _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double),
+                ("max_iterations", ctypes.c_int32), ("restart", ctypes.c_int32),
+                ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
+                ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class NsrSolveStats(ctypes.Structure):
@@ -63,6 +72,8 @@ def load():
     lib.nsr_version.restype = ctypes.c_int
     lib.nsr_error_string.restype = ctypes.c_char_p
     lib.nsr_error_string.argtypes = [ctypes.c_int]
+    lib.nsr_material_bytes.restype = S
+    lib.nsr_material_bytes.argtypes = [G]
     lib.nsr_setup_material.argtypes = [G, P, P, P, P, P]
     lib.nsr_apply.argtypes = [G, P, P, I, I, I, P, P, P]
     lib.nsr_precondition_workspace_size.restype = S
@@ -74,7 +85,11 @@ def load():
     lib.nsr_solve_workspace_size.argtypes = [G, I]
     lib.nsr_solve_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrSolveParams),
                                       P, S, P, P, P, P, P, ctypes.POINTER(NsrSolveStats), P]
-    lib.nsr_grad_accum.argtypes = [G, P, P, I, P, P, P, P, P]
+    lib.nsr_grad_accum.argtypes = [G, P, P, I, I, P, P, P, P, P]
+    lib.nsr_gmres_workspace_size.restype = S
+    lib.nsr_gmres_workspace_size.argtypes = [G, I, I]
+    lib.nsr_gmres_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrGmresParams),
+                                      P, S, P, P, P, P, P, P]
     for name in EXPORTS:
         getattr(lib, name)
     _lib = lib

@@ -25,8 +25,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .solver import (DEFAULT_REPLACE, DEFAULT_SHIFT, Geometry, Medium, apply, grad_accum, plane_wave_rhs,
-                     receiver_response, solve_batched)
+from .solver import (DEFAULT_REPLACE, DEFAULT_SHIFT, Geometry, Medium, apply, gmres_batched, grad_accum,
+                     plane_wave_rhs, receiver_response, solve_batched)
 
 V5_CLOCK_HZ = 40e6
 V5_SAMPLES = 2401
@@ -61,8 +61,8 @@ def solve_frequency(model: PlaneWaveModel, medium, frequency_hz, angle_index, to
                     max_iterations=2560, restart=32):
     """Receiver spectrum and measured convergence status of one (frequency, angle) solve.
 
-    ``medium`` is ``[1, 2, nz, nx]`` (c, rho).  ``restart`` keeps the reference
-    signature; here it is the true-residual replacement period of BiCGSTAB.
+    ``medium`` is ``[1, 2, nz, nx]`` (c, rho).  Restarted GMRES(restart) with the
+    fixed shifted-Laplace preconditioner, as nsrno/wave_solver.py:58-63.
     """
     if isinstance(medium, torch.Tensor) and medium.requires_grad:
         raise ValueError("This reference has no implicit-adjoint backward; use the neural forward for input gradients.")
@@ -79,8 +79,8 @@ def solve_frequency(model: PlaneWaveModel, medium, frequency_hz, angle_index, to
     x0 = None
     if model.warm_start is not None:
         x0 = model.warm_start(med, [frequency_hz], [model.angles[angle_index]])
-    res = solve_batched(med, [frequency_hz], [model.angles[angle_index]], x0=x0, tolerance=tolerance,
-                        max_iterations=max_iterations, replace_every=restart, n_slots=1)
+    res = gmres_batched(med, [frequency_hz], [model.angles[angle_index]], x0=x0, tolerance=tolerance,
+                        max_iterations=max_iterations, restart=restart, n_slots=1)
     status = int(res.status[0])
     reason = "converged" if status == _lib.CONVERGED else "iteration_budget"
     iters = int(res.iterations[0])
@@ -107,16 +107,23 @@ class HelmholtzSystem:
 
 @torch.no_grad()
 def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=False, tolerance=1e-5,
-                 max_cycles=100, warm_steps=8, mixed=False, method="bicgstab", initial=None,
+                 max_cycles=100, warm_steps=8, mixed=False, method="gmres", initial=None,
                  max_iterations=None):
     """Solve ``A x = rhs`` (or ``A^H x = rhs``) for a batch of angles sharing one operator.
 
-    ``rhs`` is ``[A, nz, nx]`` complex (SI units).  The angle batch shares one
-    frequency like the reference; every angle is its own Krylov system here and
+    ``rhs`` is ``[A, nz, nx]`` complex (SI units).  ``method`` is ``'gmres'``
+    (restart 24, at most ``max_cycles`` cycles, nsrno/dense_wave.py:217-220) or
+    ``'bicgstab'``, whose unconverged angles fall back to GMRES as in
+    nsrno/dense_wave.py:210-216.  The angle batch shares one frequency like the
+    reference; every angle is its own Krylov system here and
     ``max_angle_residual`` is the largest of them.  ``residual`` is the
     combined ``||R|| / ||B||`` over all angles, as the reference measures it
-    (nsrno/dense_wave.py:221-225).
+    (nsrno/dense_wave.py:221-225).  ``preconditioner``, ``warm_steps`` and
+    ``mixed`` are accepted for signature compatibility: the solve always runs
+    FP32 Krylov vectors against an FP64 true residual.
     """
+    if method not in ("gmres", "bicgstab"):
+        raise ValueError("method must be 'gmres' or 'bicgstab'")
     started = time.perf_counter()
     med = system.medium
     g = med.geometry
@@ -131,8 +138,24 @@ def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=Fals
     x0 = None if initial is None else torch.as_tensor(initial).to(med.device, torch.complex64).reshape(b.shape).contiguous()
     if max_iterations is None:
         max_iterations = max_cycles * 24
-    res = solve_batched(med, [system.frequency] * A, rhs=b, x0=x0, tolerance=tolerance,
-                        max_iterations=max_iterations, adjoint=adjoint, return_fields=True, n_slots=A)
+    freqs = [system.frequency] * A
+    if method == "bicgstab":
+        res = solve_batched(med, freqs, rhs=b, x0=x0, tolerance=tolerance, max_iterations=max_iterations,
+                            adjoint=adjoint, return_fields=True, fields_dtype=torch.complex128, n_slots=A)
+        bad = [k for k, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
+        if bad:
+            # Fall back to GMRES for the angles BiCGSTAB did not converge.
+            fb = gmres_batched(med, [system.frequency] * len(bad), rhs=b[bad], tolerance=tolerance,
+                               max_iterations=max_cycles * 24, restart=24, adjoint=adjoint, return_fields=True,
+                               fields_dtype=torch.complex128, n_slots=len(bad))
+            idx = torch.as_tensor(bad, device=res.status.device)
+            for name in ("residual", "status", "fields"):
+                getattr(res, name)[idx] = getattr(fb, name)
+            res.iterations[idx] = res.iterations[idx] * 2 + fb.iterations
+    else:
+        res = gmres_batched(med, freqs, rhs=b, x0=x0, tolerance=tolerance, max_iterations=max_iterations,
+                            restart=24, adjoint=adjoint, return_fields=True, fields_dtype=torch.complex128,
+                            n_slots=A)
     bn = torch.linalg.vector_norm(rhs.reshape(A, -1).to(torch.complex128), dim=1).to(res.residual.device)
     combined = float(torch.sqrt((res.residual.square() * bn.square()).sum() / bn.square().sum().clamp_min(1e-300)))
     statuses = [int(s) for s in res.status.cpu()]
@@ -140,9 +163,10 @@ def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=Fals
     x = res.fields.to(torch.complex128)
     if squeeze:
         x = x[0]
-    return x, {"reason": reason, "steps": int(res.iterations.sum()) * 2, "residual": combined,
+    steps = int(res.iterations.sum()) * (2 if method == "bicgstab" else 1)
+    return x, {"reason": reason, "steps": steps, "residual": combined,
                "max_angle_residual": float(res.residual.max()), "seconds": time.perf_counter() - started,
-               "dtype": "complex64 Krylov / FP64 residual", "method": "BiCGSTAB",
+               "dtype": "complex64 Krylov / FP64 residual", "method": method,
                "iterations": [int(i) for i in res.iterations.cpu()]}
 
 
@@ -167,7 +191,7 @@ class ImplicitChannels(torch.autograd.Function):
         med = Medium(g, medium[0].detach(), medium[1].detach(), alpha.detach(), device=medium.device)
         th = [data.angles[a] for a in angles]
         res = solve_batched(med, [frequency_hz] * len(th), th, tolerance=tolerance, max_iterations=max_iterations,
-                            return_fields=True, n_slots=len(th))
+                            return_fields=True, fields_dtype=torch.complex128, n_slots=len(th))
         bad = [i for i, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
         if bad:
             raise RuntimeError("Forward failed to converge: " + str({"reasons": res.reasons(),
@@ -191,7 +215,8 @@ class ImplicitChannels(torch.autograd.Function):
             rx = torch.as_tensor(np.asarray(g.rx_cols), device=medium.device)
             rhs[:, g.face, rx] = (gradient * ctx.resp).to(torch.complex64)
             res = solve_batched(med, [ctx.frequency] * A, rhs=rhs, tolerance=ctx.tolerance,
-                                max_iterations=ctx.max_iterations, adjoint=True, return_fields=True, n_slots=A)
+                                max_iterations=ctx.max_iterations, adjoint=True, return_fields=True,
+                                fields_dtype=torch.complex128, n_slots=A)
             bad = [i for i, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
             if bad:
                 raise RuntimeError("Adjoint failed to converge: " + str({"reasons": res.reasons(),

@@ -79,6 +79,29 @@ __device__ __forceinline__ T pml_profile(T pos, int n, int n_pml) {
   return f * f;
 }
 
+// Material buffer: float planes a, b, t ([3][n], used by the FP32 Krylov
+// kernels) followed, at a 256-byte aligned offset, by the same planes in
+// double ([3][n], used by the FP64 true residual, the FP64 apply and the
+// gradient, so that those evaluate exactly the operator of the oracle).
+__host__ __device__ inline size_t nsr_material_off64(long long n) {
+  return ((size_t)(12 * n) + 255) & ~(size_t)255;
+}
+__host__ __device__ inline size_t nsr_material_size(long long n) { return nsr_material_off64(n) + 24 * (size_t)n; }
+
+struct MatPlanes {
+  const float *a32, *b32, *t32;
+  const double *a64, *b64, *t64;
+};
+
+__host__ __device__ inline MatPlanes nsr_planes(const void* mat, long long n) {
+  MatPlanes m;
+  const float* f = (const float*)mat;
+  const double* d = (const double*)((const char*)mat + nsr_material_off64(n));
+  m.a32 = f; m.b32 = f + n; m.t32 = f + 2 * n;
+  m.a64 = d; m.b64 = d + n; m.t64 = d + 2 * n;
+  return m;
+}
+
 // Per-system scalars of one frequency.
 struct SysScalars {
   double kh2;    // (k0 h)^2
@@ -176,6 +199,34 @@ __device__ __forceinline__ void small_dft(float2* x) {
     float2 a = x[0] + x[2], b = x[0] - x[2], c = x[1] + x[3], e = x[1] - x[3];
     float2 d = INV ? make_float2(-e.y, e.x) : make_float2(e.y, -e.x);
     x[0] = a + c; x[2] = a - c; x[1] = b + d; x[3] = b - d;
+  } else if (R == 16) {
+    // 16 = 4 x 4: DFT4 over n1 for each n2, twiddle W16^(n2 k1), DFT4 over n2.
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f, r2 = 0.70710678118654752440f;
+    float2 y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      float2 t[4] = {x[n2], x[4 + n2], x[8 + n2], x[12 + n2]};
+      small_dft<4, INV>(t);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = t[k1];
+    }
+    // W16^e for e = n2*k1 in {0..9}: exp(-+ 2 pi i e / 16)
+    const float2 w[10] = {make_float2(1.f, 0.f), make_float2(c1, INV ? s1 : -s1), make_float2(r2, INV ? r2 : -r2),
+                          make_float2(s1, INV ? c1 : -c1), make_float2(0.f, INV ? 1.f : -1.f),
+                          make_float2(-s1, INV ? c1 : -c1), make_float2(-r2, INV ? r2 : -r2),
+                          make_float2(-c1, INV ? s1 : -s1), make_float2(-1.f, 0.f),
+                          make_float2(-c1, INV ? -s1 : s1)};
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+      for (int k1 = 1; k1 < 4; ++k1) y[n2][k1] = y[n2][k1] * w[n2 * k1];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      float2 t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      small_dft<4, INV>(t);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) x[k1 + 4 * k2] = t[k2];
+    }
   } else if (R == 8) {
     float2 ev[4] = {x[0], x[2], x[4], x[6]};
     float2 od[4] = {x[1], x[3], x[5], x[7]};
@@ -237,7 +288,8 @@ __device__ void fft_lines(float2* s, int nl, int lstride, int estride, bool line
         case 2: fft_stage<2, false>(s, nl, lstride, estride, line_fast, P, L); break;
         case 3: fft_stage<3, false>(s, nl, lstride, estride, line_fast, P, L); break;
         case 4: fft_stage<4, false>(s, nl, lstride, estride, line_fast, P, L); break;
-        default: fft_stage<8, false>(s, nl, lstride, estride, line_fast, P, L); break;
+        case 8: fft_stage<8, false>(s, nl, lstride, estride, line_fast, P, L); break;
+        default: fft_stage<16, false>(s, nl, lstride, estride, line_fast, P, L); break;
       }
       __syncthreads();
       L /= R;
@@ -253,7 +305,8 @@ __device__ void fft_lines(float2* s, int nl, int lstride, int estride, bool line
         case 2: fft_stage<2, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
         case 3: fft_stage<3, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
         case 4: fft_stage<4, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
-        default: fft_stage<8, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+        case 8: fft_stage<8, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+        default: fft_stage<16, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
       }
       __syncthreads();
     }
@@ -270,17 +323,18 @@ struct RadixList {
 };
 
 __host__ __device__ constexpr RadixList nsr_radix_list(int n) {
+  // n = 2^a 3^b: the radix-3 stages first, then 2^(a mod 4) (one radix-2, -4 or
+  // -8 stage), then radix-16 stages, so that every size divisible by 16 ends
+  // with a radix-16 stage on contiguous 16-element groups.
   RadixList L{0, {0}};
   int a = 0, b = 0, m = n;
   while (m % 2 == 0) { m /= 2; ++a; }
   while (m % 3 == 0) { m /= 3; ++b; }
   int k = 0;
-  for (int i = 0; i < b; ++i) L.r[k++] = 3;
-  int eights = a / 3, rem = a % 3;
-  if (rem == 1 && eights > 0) { eights -= 1; L.r[k++] = 4; L.r[k++] = 4; rem = 0; }
-  for (int i = 0; i < eights; ++i) L.r[k++] = 8;
-  if (rem == 2) L.r[k++] = 4;
-  if (rem == 1) L.r[k++] = 2;
+  for (int i = 0; i < b && k < NSR_MAX_RADIX_STAGES; ++i) L.r[k++] = 3;
+  const int rem = a % 4;
+  if (rem > 0 && k < NSR_MAX_RADIX_STAGES) L.r[k++] = 1 << rem;
+  for (int i = 0; i < a / 4 && k < NSR_MAX_RADIX_STAGES; ++i) L.r[k++] = 16;
   L.nst = k;
   return L;
 }
@@ -294,29 +348,33 @@ __host__ __device__ constexpr int nsr_stage_len(int n, int stage) {
 
 // One stage, everything but the number of lines known at compile time.
 // Elements: s[l*LS + k*ES].  LF: thread index runs over lines first.
-template <int N, int R, int L, bool INV, bool LF, int LS, int ES>
+template <int N, int R, int L, bool INV, bool LF, int LS, int ES, bool PAD>
 __device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __restrict__ tw) {
   constexpr int m = L / R, per_line = N / R, tstep = N / L;
+  constexpr int U = R >= 16 ? 1 : 2;   // butterflies in flight per thread
   const int nb = nl * per_line;
-  for (int b0 = threadIdx.x; b0 < nb; b0 += 2 * blockDim.x) {
-    float2 v[2][R];
-    float2* base[2];
-    int jj[2];
-    const int b1 = b0 + blockDim.x;
-    const bool two = b1 < nb;
+  auto at = [](int k) { return PAD ? k + (k >> 4) : k; };
+  for (int b0 = threadIdx.x; b0 < nb; b0 += U * blockDim.x) {
+    float2 v[U][R];
+    float2* base[U];
+    int first[U], jj[U];
+    bool ok[U];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int b = u ? (two ? b1 : b0) : b0;
+    for (int u = 0; u < U; ++u) {
+      const int bq = b0 + u * blockDim.x;
+      ok[u] = (u == 0) || bq < nb;
+      const int b = ok[u] ? bq : b0;
       int l, bb;
       if (LF) { l = b % nl; bb = b / nl; } else { l = b / per_line; bb = b - l * per_line; }
       const int o = bb / m, j = bb - o * m;
       jj[u] = j;
-      base[u] = s + l * LS + (o * L + j) * ES;
+      base[u] = s + l * LS;
+      first[u] = o * L + j;
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[u][q] = base[u][q * m * ES];
+      for (int q = 0; q < R; ++q) v[u][q] = base[u][at(first[u] + q * m) * ES];
     }
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < U; ++u) {
       if (!INV) {
         small_dft<R, false>(v[u]);
 #pragma unroll
@@ -328,71 +386,84 @@ __device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __rest
       }
     }
 #pragma unroll
-    for (int q = 0; q < R; ++q) base[0][q * m * ES] = v[0][q];
-    if (two) {
+    for (int u = 0; u < U; ++u) {
+      if (ok[u]) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) base[1][q * m * ES] = v[1][q];
+        for (int q = 0; q < R; ++q) base[u][at(first[u] + q * m) * ES] = v[u][q];
+      }
     }
   }
 }
 
-template <int N, int S, bool LF, int LS, int ES>
+template <int N, int S, bool LF, int LS, int ES, bool PAD>
 __device__ __forceinline__ void ct_forward(float2* s, int nl, const float2* __restrict__ tw) {
   constexpr RadixList RL = nsr_radix_list(N);
   if constexpr (S < RL.nst) {
     constexpr int R = RL.r[S];
     constexpr int L = nsr_stage_len(N, S);
-    ct_stage<N, R, L, false, LF, LS, ES>(s, nl, tw);
+    ct_stage<N, R, L, false, LF, LS, ES, PAD>(s, nl, tw);
     __syncthreads();
-    ct_forward<N, S + 1, LF, LS, ES>(s, nl, tw);
+    ct_forward<N, S + 1, LF, LS, ES, PAD>(s, nl, tw);
   }
 }
 
-template <int N, int S, bool LF, int LS, int ES>
+template <int N, int S, bool LF, int LS, int ES, bool PAD>
 __device__ __forceinline__ void ct_inverse(float2* s, int nl, const float2* __restrict__ tw) {
   constexpr RadixList RL = nsr_radix_list(N);
   if constexpr (S >= 0) {
     constexpr int R = RL.r[S];
     constexpr int L = nsr_stage_len(N, S);
-    ct_stage<N, R, L, true, LF, LS, ES>(s, nl, tw);
+    ct_stage<N, R, L, true, LF, LS, ES, PAD>(s, nl, tw);
     __syncthreads();
-    ct_inverse<N, S - 1, LF, LS, ES>(s, nl, tw);
+    ct_inverse<N, S - 1, LF, LS, ES, PAD>(s, nl, tw);
   }
 }
 
-template <int N, bool INV, bool LF, int LS, int ES>
+template <int N, bool INV, bool LF, int LS, int ES, bool PAD>
 __device__ __forceinline__ void ct_fft(float2* s, int nl, const float2* __restrict__ tw) {
   constexpr RadixList RL = nsr_radix_list(N);
-  if (!INV) ct_forward<N, 0, LF, LS, ES>(s, nl, tw);
-  else ct_inverse<N, RL.nst - 1, LF, LS, ES>(s, nl, tw);
+  if (!INV) ct_forward<N, 0, LF, LS, ES, PAD>(s, nl, tw);
+  else ct_inverse<N, RL.nst - 1, LF, LS, ES, PAD>(s, nl, tw);
 }
 
-// Rows: nl lines of length n stored back to back (lstride n, estride 1).
+// Row layout in shared memory: the specialised sizes insert one pad element
+// after every 16 (element k of a row at k + k/16), which keeps every row FFT
+// stage free of shared-memory bank conflicts.
+__host__ __device__ inline bool nsr_row_padded(int n) {
+  switch (n) {
+    case 256: case 384: case 512: case 768: case 1024: case 1536: case 2048: return true;
+    default: return false;
+  }
+}
+__host__ __device__ inline int nsr_row_stride(int n) { return nsr_row_padded(n) ? n + (n >> 4) : n; }
+
+// Rows: nl lines of length n, row stride nsr_row_stride(n) (padded for the
+// specialised sizes, plain otherwise).
 template <bool INV>
 __device__ void fft_rows(float2* s, int nl, const FftPlan& P) {
   switch (P.n) {
-    case 256: ct_fft<256, INV, false, 256, 1>(s, nl, P.tw); return;
-    case 384: ct_fft<384, INV, false, 384, 1>(s, nl, P.tw); return;
-    case 512: ct_fft<512, INV, false, 512, 1>(s, nl, P.tw); return;
-    case 768: ct_fft<768, INV, false, 768, 1>(s, nl, P.tw); return;
-    case 1024: ct_fft<1024, INV, false, 1024, 1>(s, nl, P.tw); return;
-    case 1536: ct_fft<1536, INV, false, 1536, 1>(s, nl, P.tw); return;
-    case 2048: ct_fft<2048, INV, false, 2048, 1>(s, nl, P.tw); return;
+    case 256: ct_fft<256, INV, false, 256 + 16, 1, true>(s, nl, P.tw); return;
+    case 384: ct_fft<384, INV, false, 384 + 24, 1, true>(s, nl, P.tw); return;
+    case 512: ct_fft<512, INV, false, 512 + 32, 1, true>(s, nl, P.tw); return;
+    case 768: ct_fft<768, INV, false, 768 + 48, 1, true>(s, nl, P.tw); return;
+    case 1024: ct_fft<1024, INV, false, 1024 + 64, 1, true>(s, nl, P.tw); return;
+    case 1536: ct_fft<1536, INV, false, 1536 + 96, 1, true>(s, nl, P.tw); return;
+    case 2048: ct_fft<2048, INV, false, 2048 + 128, 1, true>(s, nl, P.tw); return;
     default: fft_lines<INV>(s, nl, P.n, 1, false, P); return;
   }
 }
 
-// Columns: TC lines side by side (lstride 1, estride TC).
+// Columns: TC lines side by side (lstride 1, estride TC), unpadded.
 template <bool INV, int TC>
 __device__ void fft_cols(float2* s, const FftPlan& P) {
   switch (P.n) {
-    case 256: ct_fft<256, INV, true, 1, TC>(s, TC, P.tw); return;
-    case 384: ct_fft<384, INV, true, 1, TC>(s, TC, P.tw); return;
-    case 512: ct_fft<512, INV, true, 1, TC>(s, TC, P.tw); return;
-    case 768: ct_fft<768, INV, true, 1, TC>(s, TC, P.tw); return;
-    case 1024: ct_fft<1024, INV, true, 1, TC>(s, TC, P.tw); return;
-    case 1536: ct_fft<1536, INV, true, 1, TC>(s, TC, P.tw); return;
-    case 2048: ct_fft<2048, INV, true, 1, TC>(s, TC, P.tw); return;
+    case 256: ct_fft<256, INV, true, 1, TC, false>(s, TC, P.tw); return;
+    case 384: ct_fft<384, INV, true, 1, TC, false>(s, TC, P.tw); return;
+    case 512: ct_fft<512, INV, true, 1, TC, false>(s, TC, P.tw); return;
+    case 768: ct_fft<768, INV, true, 1, TC, false>(s, TC, P.tw); return;
+    case 1024: ct_fft<1024, INV, true, 1, TC, false>(s, TC, P.tw); return;
+    case 1536: ct_fft<1536, INV, true, 1, TC, false>(s, TC, P.tw); return;
+    case 2048: ct_fft<2048, INV, true, 1, TC, false>(s, TC, P.tw); return;
     default: fft_lines<INV>(s, TC, 1, TC, true, P); return;
   }
 }
@@ -401,19 +472,13 @@ __device__ void fft_cols(float2* s, const FftPlan& P) {
 // into 8s with 4s and 2s so that stages stay balanced (1024 = 8*8*4*4).
 __host__ __device__ inline bool nsr_make_radices(int n, int* radix, int* nst) {
   if (n < 8 || n > NSR_MAX_LINE) return false;
-  int a = 0, b = 0, m = n;
-  while (m % 2 == 0) { m /= 2; ++a; }
-  while (m % 3 == 0) { m /= 3; ++b; }
+  int m = n;
+  while (m % 2 == 0) m /= 2;
+  while (m % 3 == 0) m /= 3;
   if (m != 1) return false;
-  int k = 0;
-  for (int i = 0; i < b; ++i) radix[k++] = 3;
-  int eights = a / 3, rem = a % 3;
-  if (rem == 1 && eights > 0) { eights -= 1; radix[k++] = 4; radix[k++] = 4; rem = 0; }
-  for (int i = 0; i < eights; ++i) radix[k++] = 8;
-  if (rem == 2) radix[k++] = 4;
-  if (rem == 1) radix[k++] = 2;
-  if (k > NSR_MAX_RADIX_STAGES) return false;
-  *nst = k;
+  const RadixList L = nsr_radix_list(n);
+  for (int k = 0; k < L.nst; ++k) radix[k] = L.r[k];
+  *nst = L.nst;
   return true;
 }
 

@@ -1,0 +1,127 @@
+// Device helpers shared by the Krylov solvers: block reductions and the
+// 5-point stencil at an explicit neighbourhood.
+#pragma once
+
+#include "nsr_common.cuh"
+#include "nsr_internal.cuh"
+
+#define NSR_NPART 8
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-reduce NV doubles into red[0..NV) (valid in thread 0 afterwards).
+template <int NV>
+__device__ __forceinline__ void block_sum(double* vals, double* red) {
+  __shared__ double wsum[32][NSR_NPART];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = warp_sum(vals[q]);
+    if (lane == 0) wsum[wid][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += wsum[w][q];
+      red[q] = s;
+    }
+  }
+}
+
+
+// Stencil at an explicit 5-point neighbourhood.  Interior nodes (all six
+// stretches equal to one) take the real-flux path.
+template <bool ADJ>
+__device__ __forceinline__ float2 stencil_pts(const Geo& g, const SysScalars& sc, int i, int j, float a_c, float a_e,
+                                              float a_w, float a_s, float a_n, float b_c, float t_c, float2 pc,
+                                              float2 pe, float2 pw, float2 ps, float2 pn) {
+  const bool inner = i > g.n_pml && i < g.nz - 1 - g.n_pml && j > g.n_pml && j < g.nx - 1 - g.n_pml;
+  if (inner) {
+    const float e = t_c * (float)sc.fpow;
+    const float mb = (float)sc.kh2 * b_c;
+    const float2 mass = make_float2(mb * (1.0f - e * e), (ADJ ? -2.0f : 2.0f) * mb * e);
+    float2 y = mass * pc;
+    y = y + (0.5f * (a_c + a_e)) * (pe - pc);
+    y = y + (0.5f * (a_c + a_w)) * (pw - pc);
+    y = y + (0.5f * (a_c + a_s)) * (ps - pc);
+    y = y + (0.5f * (a_c + a_n)) * (pn - pc);
+    return y;
+  }
+  auto P = [&](int i2, int j2) -> float2 {
+    if (i2 == i && j2 == j) return pc;
+    if (i2 == i) return j2 > j ? pe : pw;
+    return i2 > i ? ps : pn;
+  };
+  auto Aa = [&](int i2, int j2) -> float {
+    if (i2 == i && j2 == j) return a_c;
+    if (i2 == i) return j2 > j ? a_e : a_w;
+    return i2 > i ? a_s : a_n;
+  };
+  return stencil<float, ADJ>(g, sc, i, j, b_c, t_c, P, Aa);
+}
+
+
+// ---------------------------------------------------------------------------
+// Preconditioner passes shared by the Krylov solvers.
+// ---------------------------------------------------------------------------
+// Column pass on one field w: forward FFT along z, shifted-Laplace multiply in
+// the digit-reversed domain, inverse FFT along z.  Columns [c0, c0+TC) in place.
+template <int TC>
+__device__ __forceinline__ void cols_pass(float2* sm, const Geo& g, const PrecTables& tab, float2* __restrict__ ws,
+                                          double freq, double shift, int adjoint, int c0) {
+  const long long n = (long long)g.nz * g.nx;
+  const int ncol = min(TC, g.nx - c0);
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
+    sm[k] = c < ncol ? ws[(long long)z * g.nx + c0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_cols<false, TC>(sm, tab.pz);
+  const SysScalars s = sys_scalars(g, freq);
+  const float kh2 = (float)s.kh2;
+  const float inv_n = 1.0f / (float)n;
+  const float2 shiftc = make_float2(kh2, (float)(s.kh2 * shift));
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
+    if (c < ncol) {
+      const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
+      float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
+      if (adjoint) mul = conjc(mul);
+      sm[k] = sm[k] * mul;
+    }
+  }
+  __syncthreads();
+  fft_cols<true, TC>(sm, tab.pz);
+  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
+    if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];
+  }
+}
+
+// Rows z0-1 .. z0+nb of w (zero outside the grid) into the padded row layout
+// of shared memory, inverse row FFT.  Row rr of the band is sm[(rr+1)*rs].
+__device__ __forceinline__ void band_inverse_rows(float2* sm, const Geo& g, const PrecTables& tab,
+                                                  const float2* __restrict__ w, int z0, int nb) {
+  const int nx = g.nx;
+  const int rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
+  const int nl = nb + 2;
+  for (int rr = 0; rr < nl; ++rr) {
+    const int z = z0 - 1 + rr;
+    const bool in = z >= 0 && z < g.nz;
+#pragma unroll 4
+    for (int j = threadIdx.x; j < nx; j += blockDim.x)
+      sm[rr * rs + (pad ? j + (j >> 4) : j)] = in ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_rows<true>(sm, nl, tab.px);
+}
+
+// Stores `val` for element (l, c) of a row tile in the padded row layout.
+__device__ __forceinline__ int row_slot(int l, int c, int rs, bool pad) { return l * rs + (pad ? c + (c >> 4) : c); }

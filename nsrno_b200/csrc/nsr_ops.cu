@@ -47,40 +47,65 @@ static inline int last_error() {
 // Material planes.
 // ---------------------------------------------------------------------------
 __global__ void k_setup_material(Geo g, const float* __restrict__ c, const float* __restrict__ rho,
-                                 const float* __restrict__ alpha, float* __restrict__ coef, long long n) {
+                                 const float* __restrict__ alpha, void* __restrict__ mat, long long n) {
   const double neper = 100.0 * 2.302585092994045684 / 20.0;  // dB/cm -> Np/m
+  float* f = (float*)mat;
+  double* d = (double*)((char*)mat + nsr_material_off64(n));
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    double cc = c[k], rr = rho[k], al = alpha[k];
-    coef[k] = (float)(g.rho0 / rr);
-    coef[n + k] = (float)(g.rho0 * g.c0 * g.c0 / (rr * cc * cc));
-    coef[2 * n + k] = (float)(al * neper * cc / (2.0 * NSR_PI * 1e6));
+    const double cc = c[k], rr = rho[k], al = alpha[k];
+    const double a = g.rho0 / rr;
+    const double b = g.rho0 * g.c0 * g.c0 / (rr * cc * cc);
+    const double t = al * neper * cc / (2.0 * NSR_PI * 1e6);
+    d[k] = a; d[n + k] = b; d[2 * n + k] = t;
+    f[k] = (float)a; f[n + k] = (float)b; f[2 * n + k] = (float)t;
   }
 }
 
+extern "C" size_t nsr_material_bytes(const NsrGrid* grid) {
+  if (nsr_check_grid(grid, false)) return 0;
+  return nsr_material_size((long long)grid->nz * grid->nx);
+}
+
 extern "C" int nsr_setup_material(const NsrGrid* grid, const float* c, const float* rho,
-                                  const float* alpha_db, float* coef, void* stream) {
+                                  const float* alpha_db, void* material, void* stream) {
   int err = nsr_check_grid(grid, false);
   if (err) return err;
-  if (!c || !rho || !alpha_db || !coef) return NSR_ERR_ARGUMENT;
+  if (!c || !rho || !alpha_db || !material) return NSR_ERR_ARGUMENT;
   long long n = (long long)grid->nz * grid->nx;
   int blocks = (int)((n + 255) / 256);
   if (blocks > 148 * 32) blocks = 148 * 32;
-  k_setup_material<<<blocks, 256, 0, (cudaStream_t)stream>>>(make_geo(*grid), c, rho, alpha_db, coef, n);
+  k_setup_material<<<blocks, 256, 0, (cudaStream_t)stream>>>(make_geo(*grid), c, rho, alpha_db, material, n);
   return last_error();
 }
 
 // ---------------------------------------------------------------------------
 // Operator apply (one thread per node; used for checks and true residuals).
 // ---------------------------------------------------------------------------
+template <typename T> struct PlaneOf;
+template <> struct PlaneOf<float> {
+  static __device__ __forceinline__ const float* a(const MatPlanes& m) { return m.a32; }
+  static __device__ __forceinline__ const float* b(const MatPlanes& m) { return m.b32; }
+  static __device__ __forceinline__ const float* t(const MatPlanes& m) { return m.t32; }
+};
+template <> struct PlaneOf<double> {
+  static __device__ __forceinline__ const double* a(const MatPlanes& m) { return m.a64; }
+  static __device__ __forceinline__ const double* b(const MatPlanes& m) { return m.b64; }
+  static __device__ __forceinline__ const double* t(const MatPlanes& m) { return m.t64; }
+};
+
+// FP32 fields use the float planes, FP64 fields the double planes.
 template <typename T, bool ADJ>
-__global__ void k_apply(Geo g, const float* __restrict__ coef, const double* __restrict__ freq,
+__global__ void k_apply(Geo g, const void* __restrict__ mat, const double* __restrict__ freq,
                         const typename CxT<T>::type* __restrict__ x, typename CxT<T>::type* __restrict__ y) {
   typedef typename CxT<T>::type C;
   const long long n = (long long)g.nz * g.nx;
   const int sysi = blockIdx.y;
   const SysScalars s = sys_scalars(g, freq[sysi]);
   const C* xs = x + sysi * n;
-  const float* ca = coef;
+  const MatPlanes mp = nsr_planes(mat, n);
+  const T* ca = PlaneOf<T>::a(mp);
+  const T* cb = PlaneOf<T>::b(mp);
+  const T* ct = PlaneOf<T>::t(mp);
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(k / g.nx), j = (int)(k - (long long)i * g.nx);
     auto P = [&](int i2, int j2) -> C {
@@ -91,11 +116,11 @@ __global__ void k_apply(Geo g, const float* __restrict__ coef, const double* __r
       if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return T(1);
       return (T)ca[(long long)i2 * g.nx + j2];
     };
-    y[sysi * n + k] = stencil<T, ADJ>(g, s, i, j, (T)coef[n + k], (T)coef[2 * n + k], P, A);
+    y[sysi * n + k] = stencil<T, ADJ>(g, s, i, j, cb[k], ct[k], P, A);
   }
 }
 
-extern "C" int nsr_apply(const NsrGrid* grid, const float* coef, const double* freq_hz,
+extern "C" int nsr_apply(const NsrGrid* grid, const void* coef, const double* freq_hz,
                          int32_t n_systems, int32_t adjoint, int32_t precision,
                          const void* x, void* y, void* stream) {
   int err = nsr_check_grid(grid, false);
@@ -205,11 +230,19 @@ __global__ void __launch_bounds__(256) k_prec_rows_fwd(Geo g, PrecTables t, cons
   const int z0 = blockIdx.x * rows;
   const int nr = min(rows, g.nz - z0);
   const float2* xs = x + blockIdx.y * n + (long long)z0 * g.nx;
-  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) sm[k] = xs[k];
+  const int rs = nsr_row_stride(g.nx);
+  const bool pad = nsr_row_padded(g.nx);
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) {
+    const int l = k / g.nx, c = k - l * g.nx;
+    sm[l * rs + (pad ? c + (c >> 4) : c)] = xs[k];
+  }
   __syncthreads();
   fft_rows<false>(sm, nr, t.px);
   float2* ws = w + blockIdx.y * n + (long long)z0 * g.nx;
-  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) ws[k] = sm[k];
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) {
+    const int l = k / g.nx, c = k - l * g.nx;
+    ws[k] = sm[l * rs + (pad ? c + (c >> 4) : c)];
+  }
 }
 
 __global__ void __launch_bounds__(256) k_prec_rows_inv(Geo g, PrecTables t, const float2* __restrict__ w,
@@ -219,11 +252,19 @@ __global__ void __launch_bounds__(256) k_prec_rows_inv(Geo g, PrecTables t, cons
   const int z0 = blockIdx.x * rows;
   const int nr = min(rows, g.nz - z0);
   const float2* ws = w + blockIdx.y * n + (long long)z0 * g.nx;
-  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) sm[k] = ws[k];
+  const int rs = nsr_row_stride(g.nx);
+  const bool pad = nsr_row_padded(g.nx);
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) {
+    const int l = k / g.nx, c = k - l * g.nx;
+    sm[l * rs + (pad ? c + (c >> 4) : c)] = ws[k];
+  }
   __syncthreads();
   fft_rows<true>(sm, nr, t.px);
   float2* ys = y + blockIdx.y * n + (long long)z0 * g.nx;
-  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) ys[k] = sm[k];
+  for (int k = threadIdx.x; k < nr * g.nx; k += blockDim.x) {
+    const int l = k / g.nx, c = k - l * g.nx;
+    ys[k] = sm[l * rs + (pad ? c + (c >> 4) : c)];
+  }
 }
 
 extern "C" size_t nsr_precondition_workspace_size(const NsrGrid* grid, int32_t n_systems) {
@@ -246,7 +287,7 @@ extern "C" int nsr_precondition(const NsrGrid* grid, const double* freq_hz, int3
   float2* w = (float2*)((char*)workspace + nsr_prec_table_bytes(grid));
   Geo g = make_geo(*grid);
   const int rows = nsr_rows_per_cta(grid);
-  const size_t row_smem = sizeof(float2) * (size_t)rows * grid->nx;
+  const size_t row_smem = sizeof(float2) * (size_t)rows * nsr_row_stride(grid->nx);
   dim3 gr((grid->nz + rows - 1) / rows, n_systems);
   k_prec_rows_fwd<<<gr, 256, row_smem, st>>>(g, t, (const float2*)x, w, rows);
   const int tc = nsr_cols_tc(grid);
@@ -313,26 +354,30 @@ extern "C" int nsr_plane_wave_rhs(const NsrGrid* grid, const double* freq_hz, co
 // each edge e=(i,j): d(lam^H A u)/d log rho_i = a_i w_e conj(lam_j - lam_i)(u_j - u_i),
 // w_e = stretch_e / (2 h^2).
 // ---------------------------------------------------------------------------
-__global__ void k_grad(Geo g, const float* __restrict__ coef, const double* __restrict__ freq, int ns,
-                       const float2* __restrict__ u, const float2* __restrict__ lam,
+template <typename CT>
+__global__ void k_grad(Geo g, const void* __restrict__ mat, const double* __restrict__ freq, int ns,
+                       const CT* __restrict__ u, const CT* __restrict__ lam,
                        double* __restrict__ gc, double* __restrict__ gr) {
   const long long n = (long long)g.nz * g.nx;
   const double inv_h2 = 1.0 / (g.h * g.h);
+  const MatPlanes mp = nsr_planes(mat, n);
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(k / g.nx), j = (int)(k - (long long)i * g.nx);
-    const double a_c = coef[k], b_c = coef[n + k], t_c = coef[2 * n + k];
+    const double a_c = mp.a64[k], b_c = mp.b64[k], t_c = mp.t64[k];
     double acc_c = 0.0, acc_r = 0.0;
     for (int sidx = 0; sidx < ns; ++sidx) {
       const SysScalars s = sys_scalars(g, freq[sidx]);
-      const float2* us = u + sidx * n;
-      const float2* ls = lam + sidx * n;
+      const CT* us = u + sidx * n;
+      const CT* ls = lam + sidx * n;
       auto U = [&](int i2, int j2) -> double2 {
         if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return make_double2(0.0, 0.0);
-        return to_d(us[(long long)i2 * g.nx + j2]);
+        const CT q = us[(long long)i2 * g.nx + j2];
+        return make_double2((double)q.x, (double)q.y);
       };
       auto L = [&](int i2, int j2) -> double2 {
         if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return make_double2(0.0, 0.0);
-        return to_d(ls[(long long)i2 * g.nx + j2]);
+        const CT q = ls[(long long)i2 * g.nx + j2];
+        return make_double2((double)q.x, (double)q.y);
       };
       const double2 uc = U(i, j), lc = L(i, j);
       const double2 lu = conjc(lc) * uc;
@@ -368,17 +413,23 @@ __global__ void k_grad(Geo g, const float* __restrict__ coef, const double* __re
   }
 }
 
-extern "C" int nsr_grad_accum(const NsrGrid* grid, const float* coef, const double* freq_hz,
-                              int32_t n_systems, const float* u, const float* lam,
+extern "C" int nsr_grad_accum(const NsrGrid* grid, const void* coef, const double* freq_hz,
+                              int32_t n_systems, int32_t precision, const void* u, const void* lam,
                               double* g_logc, double* g_logrho, void* stream) {
   int err = nsr_check_grid(grid, false);
   if (err) return err;
   if (!coef || !freq_hz || !u || !lam || !g_logc || !g_logrho || n_systems < 0) return NSR_ERR_ARGUMENT;
+  if (precision != 0 && precision != 1) return NSR_ERR_ARGUMENT;
   if (n_systems == 0) return 0;
   long long n = (long long)grid->nz * grid->nx;
   int bx = (int)((n + 255) / 256);
   if (bx > 148 * 16) bx = 148 * 16;
-  k_grad<<<bx, 256, 0, (cudaStream_t)stream>>>(make_geo(*grid), coef, freq_hz, n_systems, (const float2*)u,
-                                              (const float2*)lam, g_logc, g_logrho);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == 0)
+    k_grad<float2><<<bx, 256, 0, st>>>(make_geo(*grid), coef, freq_hz, n_systems, (const float2*)u,
+                                        (const float2*)lam, g_logc, g_logrho);
+  else
+    k_grad<double2><<<bx, 256, 0, st>>>(make_geo(*grid), coef, freq_hz, n_systems, (const double2*)u,
+                                         (const double2*)lam, g_logc, g_logrho);
   return last_error();
 }

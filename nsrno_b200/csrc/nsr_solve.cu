@@ -20,13 +20,14 @@
 // iterations, breakdown/divergence reasons) and the fixed preconditioner of
 // nsrno/dense_wave.py:194-196.
 #include "nsr_internal.cuh"
+#include "nsr_device.cuh"
 
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES = 4, MODE_EMIT = 5 };
-#define NSR_NPART 8
+
 #define NSR_LAUNCHES_PER_IT 7
 
 struct __align__(16) SlotState {
@@ -54,7 +55,7 @@ struct SolveArgs {
   Geo g;
   PrecTables tab;
   SolveBufs B;
-  const float* coef;
+  MatPlanes mat;
   const double* freq;
   const double* angle;
   const float2* rhs;
@@ -76,7 +77,8 @@ struct SolveArgs {
   double* residual;
   int* iterations;
   int* status;
-  float2* fields;
+  void* fields;     // float2 or double2 [S][n]
+  int fields_fp64;
 };
 
 // Which slots a launch serves.  The first half of an iteration runs only the
@@ -98,7 +100,7 @@ __device__ __forceinline__ double abs2(double2 a) { return a.x * a.x + a.y * a.y
 // ---------------------------------------------------------------------------
 // fwd: elementwise update + forward row FFT into w.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
+__global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
   const int slot = blockIdx.y;
   const SlotState& S = A.B.slots[slot];
@@ -119,38 +121,67 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs A, int half) {
   if (mode == MODE_EMIT) {
     if (A.fields && S.sys >= 0) {
       const double2* x = A.B.x + (2LL * slot + S.xpar) * n + (long long)z0 * g.nx;
-      float2* f = A.fields + (long long)S.sys * n + (long long)z0 * g.nx;
-      for (int k = threadIdx.x; k < cnt; k += blockDim.x) f[k] = S.zero_rhs ? make_float2(0.f, 0.f) : f2(x[k]);
+      if (A.fields_fp64) {
+        double2* f = (double2*)A.fields + (long long)S.sys * n + (long long)z0 * g.nx;
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) f[k] = S.zero_rhs ? make_double2(0.0, 0.0) : x[k];
+      } else {
+        float2* f = (float2*)A.fields + (long long)S.sys * n + (long long)z0 * g.nx;
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) f[k] = S.zero_rhs ? make_float2(0.f, 0.f) : f2(x[k]);
+      }
     }
     return;
   }
   const float2 sv = f2(S.c_sv), rt = f2(S.c_rt), yp = f2(S.c_yp), ys = f2(S.c_ys), pp = f2(S.c_pp), pv = f2(S.c_pv);
+  const int nx = g.nx;
+  const int rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
+  float2* __restrict__ rr_ = r;
+  float2* __restrict__ pp_ = p;
+  float2* __restrict__ yy_ = y;
+  const float2* __restrict__ vv_ = v;
+  const float2* __restrict__ tt_ = t;
   if (mode == MODE_ITER_A) {
     const bool restart = S.restart != 0;
-    float2* rh = A.B.rh + off;
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-      const float2 rk = r[k], vk = v[k], tk = t[k], pk = p[k], yk = y[k];
-      const float2 s = rk + sv * vk;
-      const float2 rn = s + rt * tk;
-      const float2 yn = yk + yp * pk + ys * s;
-      const float2 pn = rn + pp * pk + pv * vk;
-      r[k] = rn; p[k] = pn; y[k] = yn;
-      if (restart) rh[k] = rn;
-      sm[k] = pn;
+    float2* __restrict__ rh = A.B.rh + off;
+    for (int l = 0; l < nr; ++l) {
+#pragma unroll 4
+      for (int c = threadIdx.x; c < nx; c += blockDim.x) {
+        const int k = l * nx + c;
+        const float2 rk = rr_[k], vk = vv_[k], tk = tt_[k], pk = pp_[k], yk = yy_[k];
+        const float2 s1 = rk + sv * vk;
+        const float2 rn = s1 + rt * tk;
+        const float2 yn = yk + yp * pk + ys * s1;
+        const float2 pn = rn + pp * pk + pv * vk;
+        rr_[k] = rn; pp_[k] = pn; yy_[k] = yn;
+        if (restart) rh[k] = rn;
+        sm[l * rs + (pad ? c + (c >> 4) : c)] = pn;
+      }
     }
   } else if (mode == MODE_ITER_B) {
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) sm[k] = r[k] + sv * v[k];
+    for (int l = 0; l < nr; ++l) {
+#pragma unroll 4
+      for (int c = threadIdx.x; c < nx; c += blockDim.x) {
+        const int k = l * nx + c;
+        sm[l * rs + (pad ? c + (c >> 4) : c)] = rr_[k] + sv * vv_[k];
+      }
+    }
   } else {  // MODE_RES: apply the pending update to y, transform y, clear it
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-      const float2 s = r[k] + sv * v[k];
-      sm[k] = y[k] + yp * p[k] + ys * s;
-      y[k] = make_float2(0.f, 0.f);
+    for (int l = 0; l < nr; ++l) {
+      for (int c = threadIdx.x; c < nx; c += blockDim.x) {
+        const int k = l * nx + c;
+        const float2 s1 = rr_[k] + sv * vv_[k];
+        sm[l * rs + (pad ? c + (c >> 4) : c)] = yy_[k] + yp * pp_[k] + ys * s1;
+        yy_[k] = make_float2(0.f, 0.f);
+      }
     }
   }
   __syncthreads();
   fft_rows<false>(sm, nr, A.tab.px);
-  float2* w = A.B.w + off;
-  for (int k = threadIdx.x; k < cnt; k += blockDim.x) w[k] = sm[k];
+  float2* __restrict__ w = A.B.w + off;
+  for (int l = 0; l < nr; ++l) {
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nx; c += blockDim.x) w[l * nx + c] = sm[l * rs + (pad ? c + (c >> 4) : c)];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -162,66 +193,8 @@ __global__ void __launch_bounds__(512) k_cols(SolveArgs A, int half) {
   const int slot = blockIdx.y;
   const int mode = A.B.slots[slot].mode;
   if (!cols_active(mode, half)) return;
-  const Geo& g = A.g;
-  const long long n = (long long)g.nz * g.nx;
-  float2* ws = A.B.w + slot * n;
-  const int c0 = blockIdx.x * TC;
-  const int ncol = min(TC, g.nx - c0);
-  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-    const int z = k / TC, c = k - z * TC;
-    sm[k] = c < ncol ? ws[(long long)z * g.nx + c0 + c] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  fft_cols<false, TC>(sm, A.tab.pz);
-  const SysScalars s = sys_scalars(g, A.B.slots[slot].freq);
-  const float kh2 = (float)s.kh2;
-  const float inv_n = 1.0f / (float)n;
-  const float2 shiftc = make_float2(kh2, (float)(s.kh2 * A.shift));
-  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-    const int z = k / TC, c = k - z * TC;
-    if (c < ncol) {
-      const float sym = -4.0f * (A.tab.s2z[z] + A.tab.s2x[c0 + c]);
-      float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
-      if (A.adjoint) mul = conjc(mul);
-      sm[k] = sm[k] * mul;
-    }
-  }
-  __syncthreads();
-  fft_cols<true, TC>(sm, A.tab.pz);
-  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-    const int z = k / TC, c = k - z * TC;
-    if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Reduction helpers.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Block-reduce NV doubles into red[0..NV) (valid in thread 0 afterwards).
-template <int NV>
-__device__ __forceinline__ void block_sum(double* vals, double* red) {
-  __shared__ double wsum[32][NSR_NPART];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    double s = warp_sum(vals[q]);
-    if (lane == 0) wsum[wid][q] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int nw = blockDim.x >> 5;
-    for (int q = 0; q < NV; ++q) {
-      double s = 0.0;
-      for (int w = 0; w < nw; ++w) s += wsum[w][q];
-      red[q] = s;
-    }
-  }
+  const long long n = (long long)A.g.nz * A.g.nx;
+  cols_pass<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.slots[slot].freq, A.shift, A.adjoint, blockIdx.x * TC);
 }
 
 __device__ void pop_next(const SolveArgs& A, SlotState& S) {
@@ -431,37 +404,6 @@ __device__ __forceinline__ void reduce_and_finalize(const SolveArgs& A, SlotStat
   }
 }
 
-// Stencil at an explicit 5-point neighbourhood.  Interior nodes (all six
-// stretches equal to one) take the real-flux path.
-template <bool ADJ>
-__device__ __forceinline__ float2 stencil_pts(const Geo& g, const SysScalars& sc, int i, int j, float a_c, float a_e,
-                                              float a_w, float a_s, float a_n, float b_c, float t_c, float2 pc,
-                                              float2 pe, float2 pw, float2 ps, float2 pn) {
-  const bool inner = i > g.n_pml && i < g.nz - 1 - g.n_pml && j > g.n_pml && j < g.nx - 1 - g.n_pml;
-  if (inner) {
-    const float e = t_c * (float)sc.fpow;
-    const float mb = (float)sc.kh2 * b_c;
-    const float2 mass = make_float2(mb * (1.0f - e * e), (ADJ ? -2.0f : 2.0f) * mb * e);
-    float2 y = mass * pc;
-    y = y + (0.5f * (a_c + a_e)) * (pe - pc);
-    y = y + (0.5f * (a_c + a_w)) * (pw - pc);
-    y = y + (0.5f * (a_c + a_s)) * (ps - pc);
-    y = y + (0.5f * (a_c + a_n)) * (pn - pc);
-    return y;
-  }
-  auto P = [&](int i2, int j2) -> float2 {
-    if (i2 == i && j2 == j) return pc;
-    if (i2 == i) return j2 > j ? pe : pw;
-    return i2 > i ? ps : pn;
-  };
-  auto Aa = [&](int i2, int j2) -> float {
-    if (i2 == i && j2 == j) return a_c;
-    if (i2 == i) return j2 > j ? a_e : a_w;
-    return i2 > i ? a_s : a_n;
-  };
-  return stencil<float, ADJ>(g, sc, i, j, b_c, t_c, P, Aa);
-}
-
 // ---------------------------------------------------------------------------
 // inv: inverse row FFT + stencil + inner products of the Krylov halves.
 // ---------------------------------------------------------------------------
@@ -478,48 +420,54 @@ __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
   const int nb = min(A.tz, g.nz - z0);
   const int nx = g.nx;
   const long long soff = slot * n;
+  const int rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
+  auto at = [pad](int j) { return pad ? j + (j >> 4) : j; };
   {
-    const float2* w = A.B.w + soff;
+    const float2* __restrict__ w = A.B.w + soff;
     const int nl = nb + 2;
     for (int rr = 0; rr < nl; ++rr) {
       const int z = z0 - 1 + rr;
       const bool in = z >= 0 && z < g.nz;
+#pragma unroll 4
       for (int j = threadIdx.x; j < nx; j += blockDim.x)
-        sm[rr * nx + j] = in ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
+        sm[rr * rs + at(j)] = in ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     fft_rows<true>(sm, nl, A.tab.px);
   }
   const SysScalars sc = sys_scalars(g, S.freq);
-  const float* ca = A.coef;
-  const float* cb = A.coef + n;
-  const float* ct = A.coef + 2 * n;
-  const float2* rh = A.B.rh + soff;
+  const float* __restrict__ ca = A.mat.a32;
+  const float* __restrict__ cb = A.mat.b32;
+  const float* __restrict__ ct = A.mat.t32;
+  const float2* __restrict__ rh = A.B.rh + soff;
   double acc[NSR_NPART];
 #pragma unroll
   for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
   const float2 sv = f2(S.c_sv);
-  float2* out = (half == 0 ? A.B.v : A.B.t) + soff;
-  const float2* r = A.B.r + soff;
-  const float2* v = A.B.v + soff;
+  float2* __restrict__ out = (half == 0 ? A.B.v : A.B.t) + soff;
+  const float2* __restrict__ r = A.B.r + soff;
+  const float2* __restrict__ v = A.B.v + soff;
   for (int rr = 0; rr < nb; ++rr) {
     const int i = z0 + rr;
-    const float2* row = sm + (rr + 1) * nx;
-    const float2* up = sm + rr * nx;
-    const float2* dn = sm + (rr + 2) * nx;
+    const float2* row = sm + (rr + 1) * rs;
+    const float2* up = sm + rr * rs;
+    const float2* dn = sm + (rr + 2) * rs;
+#pragma unroll 2
     for (int j = threadIdx.x; j < nx; j += blockDim.x) {
       const long long idx = (long long)i * nx + j;
       const float2 z = make_float2(0.f, 0.f);
-      const float2 pc = row[j];
-      const float2 pe = j + 1 < nx ? row[j + 1] : z;
-      const float2 pw = j > 0 ? row[j - 1] : z;
+      const int aj = at(j);
+      const float2 pc = row[aj];
+      const float2 pe = j + 1 < nx ? row[at(j + 1)] : z;
+      const float2 pw = j > 0 ? row[at(j - 1)] : z;
       const float a_c = __ldg(&ca[idx]);
       const float a_e = j + 1 < nx ? __ldg(&ca[idx + 1]) : 1.0f;
       const float a_w = j > 0 ? __ldg(&ca[idx - 1]) : 1.0f;
       const float a_s = i + 1 < g.nz ? __ldg(&ca[idx + nx]) : 1.0f;
       const float a_n = i > 0 ? __ldg(&ca[idx - nx]) : 1.0f;
       const float2 av = stencil_pts<ADJ>(g, sc, i, j, a_c, a_e, a_w, a_s, a_n, __ldg(&cb[idx]), __ldg(&ct[idx]),
-                                         pc, pe, pw, dn[j], up[j]);
+                                         pc, pe, pw, dn[aj], up[aj]);
       out[idx] = av;
       const float2 rk = rh[idx];
       if (half == 0) {
@@ -555,24 +503,26 @@ __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
   const int nb = min(tz, g.nz - z0);
   const int nx = g.nx;
   const SysScalars sc = sys_scalars(g, S.freq);
-  const float* ca = A.coef;
-  const float* cb = A.coef + n;
-  const float* ct = A.coef + 2 * n;
+  const double* ca = A.mat.a64;
+  const double* cb = A.mat.b64;
+  const double* ct = A.mat.t64;
   auto Aa64 = [&](int i2, int j2) -> double {
     if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return 1.0;
-    return (double)__ldg(&ca[(long long)i2 * nx + j2]);
+    return __ldg(&ca[(long long)i2 * nx + j2]);
   };
   double acc[NSR_NPART];
 #pragma unroll
   for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
   const long long soff = slot * n;
+  const int rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
   if (mode == MODE_RES) {
     const float2* w = A.B.w + soff;
     const int nl = nb + 2;
     for (int k = threadIdx.x; k < nl * nx; k += blockDim.x) {
       const int zr = k / nx, j = k - zr * nx;
       const int z = z0 - 1 + zr;
-      sm[k] = (z >= 0 && z < g.nz) ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
+      sm[zr * rs + (pad ? j + (j >> 4) : j)] = (z >= 0 && z < g.nz) ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     fft_rows<true>(sm, nl, A.tab.px);
@@ -585,7 +535,7 @@ __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
       if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return make_double2(0.0, 0.0);
       const long long id = (long long)i2 * nx + j2;
       if (mode == MODE_INIT) return x0 ? to_d(x0[id]) : make_double2(0.0, 0.0);
-      return xo[id] + to_d(sm[(i2 - z0 + 1) * nx + j2]);
+      return xo[id] + to_d(sm[(i2 - z0 + 1) * rs + (pad ? j2 + (j2 >> 4) : j2)]);
     };
     const double h2 = g.h * g.h;
     const float2* rhs = A.rhs ? A.rhs + (long long)S.sys * n : nullptr;
@@ -604,7 +554,7 @@ __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
       } else {
         b = make_double2(0.0, 0.0);
       }
-      const double2 ax = stencil<double, ADJ>(g, sc, i, j, (double)__ldg(&cb[idx]), (double)__ldg(&ct[idx]), P, Aa64);
+      const double2 ax = stencil<double, ADJ>(g, sc, i, j, __ldg(&cb[idx]), __ldg(&ct[idx]), P, Aa64);
       const double2 res = b - ax;
       xn[idx] = P(i, j);
       const float2 rf = to_f(res);
@@ -698,14 +648,14 @@ static int* pinned_counter() {
   return p;
 }
 
-extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
+extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
                                  const double* freq_hz, const double* angle_rad, int32_t n_systems,
                                  const float* rhs, const float* x0,
                                  const int32_t* rx_index, int32_t n_rx,
                                  const NsrSolveParams* params,
                                  void* workspace, size_t workspace_bytes,
                                  double* iq, double* residual, int32_t* iterations, int32_t* status,
-                                 float* fields, NsrSolveStats* stats, void* stream) {
+                                 void* fields, NsrSolveStats* stats, void* stream) {
   int err = nsr_check_grid(grid, true);
   if (err) return err;
   if (!params || !coef || !freq_hz || n_systems < 0 || n_rx < 0 || (n_rx > 0 && !rx_index)) return NSR_ERR_ARGUMENT;
@@ -760,7 +710,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
     float2** vecs[7] = {&A.B.r, &A.B.rh, &A.B.p, &A.B.v, &A.B.t, &A.B.y, &A.B.w};
     for (int q = 0; q < 7; ++q) *vecs[q] = (float2*)(ws + L.vec + q * vb);
     A.B.x = (double2*)(ws + L.x);
-    A.coef = coef;
+    A.mat = nsr_planes(coef, (long long)grid->nz * grid->nx);
     A.freq = freq_hz;
     A.angle = rhs ? nullptr : angle_rad;
     A.rhs = (const float2*)rhs;
@@ -782,11 +732,12 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const float* coef,
     A.residual = residual;
     A.iterations = iterations;
     A.status = status;
-    A.fields = (float2*)fields;
+    A.fields = fields;
+    A.fields_fp64 = params->fields_fp64 ? 1 : 0;
 
-    const size_t fwd_smem = sizeof(float2) * A.rows * grid->nx;
+    const size_t fwd_smem = sizeof(float2) * A.rows * nsr_row_stride(grid->nx);
     const size_t col_smem = nsr_cols_smem(grid);
-    const size_t inv_smem = sizeof(float2) * (A.tz + 2) * grid->nx;
+    const size_t inv_smem = sizeof(float2) * (A.tz + 2) * nsr_row_stride(grid->nx);
     NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));

@@ -87,14 +87,31 @@ class Medium:
                     torch.isfinite(self.rho).all() and (self.rho > 0).all() and torch.isfinite(self.alpha).all()):
             raise ValueError("c and rho must be finite and positive; alpha must be finite")
         _require_cuda(self.c, "medium")
-        self.coef = torch.empty((3,) + shape, dtype=torch.float32, device=device)
         self._grid = geometry.struct()
-        _lib.check(_lib.load().nsr_setup_material(ctypes.byref(self._grid), _ptr(self.c), _ptr(self.rho),
-                                                  _ptr(self.alpha), _ptr(self.coef), _stream()))
+        lib = _lib.load()
+        nbytes = lib.nsr_material_bytes(ctypes.byref(self._grid))
+        if nbytes == 0:
+            raise ValueError("invalid grid")
+        self.material = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        _lib.check(lib.nsr_setup_material(ctypes.byref(self._grid), _ptr(self.c), _ptr(self.rho),
+                                          _ptr(self.alpha), _ptr(self.material), _stream()))
 
     @property
     def device(self):
-        return self.coef.device
+        return self.material.device
+
+    @property
+    def coef(self):
+        """Float planes (a, b, t) ``[3, nz, nx]`` used by the FP32 Krylov kernels."""
+        g = self.geometry
+        return self.material[: 12 * g.n].view(torch.float32).view(3, g.nz, g.nx)
+
+    @property
+    def coef64(self):
+        """Double planes (a, b, t) ``[3, nz, nx]`` used by the FP64 residual, apply and gradient."""
+        g = self.geometry
+        off = (12 * g.n + 255) // 256 * 256
+        return self.material[off: off + 24 * g.n].view(torch.float64).view(3, g.nz, g.nx)
 
 
 @dataclass
@@ -129,8 +146,8 @@ _default_ws = Workspace()
 def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tolerance=1e-6,
                   max_iterations=2000, shift=DEFAULT_SHIFT, replace_every=DEFAULT_REPLACE, n_slots=16,
                   adjoint=False, return_fields=False, rx_index=None, graph_iterations=16,
-                  profile_iterations=0, restart_factor=DEFAULT_RESTART, workspace: Workspace | None = None,
-                  out: BatchResult | None = None) -> BatchResult:
+                  profile_iterations=0, restart_factor=DEFAULT_RESTART, fields_dtype=torch.complex64,
+                  workspace: Workspace | None = None, out: BatchResult | None = None) -> BatchResult:
     """Solve every (frequency, angle) system of a record with batched BiCGSTAB.
 
     ``freqs``/``angles`` are 1-D (one entry per system).  ``rhs`` (complex64
@@ -172,19 +189,77 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                           residual=torch.empty(S, dtype=torch.float64, device=dev),
                           iterations=torch.empty(S, dtype=torch.int32, device=dev),
                           status=torch.empty(S, dtype=torch.int32, device=dev),
-                          fields=torch.empty((S, g.nz, g.nx), dtype=torch.complex64, device=dev)
+                          fields=torch.empty((S, g.nz, g.nx), dtype=fields_dtype, device=dev)
                           if return_fields else None)
+    if fields_dtype not in (torch.complex64, torch.complex128):
+        raise ValueError("fields_dtype must be complex64 or complex128")
+    if out.fields is not None and (out.fields.dtype != fields_dtype or tuple(out.fields.shape) != (S, g.nz, g.nx)):
+        raise ValueError("out.fields does not match fields_dtype and the system count")
     params = _lib.NsrSolveParams(float(tolerance), float(shift), float(restart_factor), int(max_iterations),
                                  int(replace_every),
-                                 int(n_slots), int(bool(adjoint)), int(graph_iterations), int(profile_iterations))
+                                 int(n_slots), int(bool(adjoint)), int(graph_iterations), int(profile_iterations),
+                                 int(fields_dtype == torch.complex128), 0)
     stats = _lib.NsrSolveStats()
     _lib.check(lib.nsr_solve_batched(
-        ctypes.byref(grid), _ptr(medium.coef), _ptr(freqs), _ptr(angles), S,
+        ctypes.byref(grid), _ptr(medium.material), _ptr(freqs), _ptr(angles), S,
         _ptr(rhs), _ptr(x0), _ptr(rx_index), n_rx, ctypes.byref(params),
         _ptr(ws), ws.numel(), _ptr(out.iq), _ptr(out.residual), _ptr(out.iterations), _ptr(out.status),
         _ptr(out.fields), ctypes.byref(stats), _stream()))
     out.extra["stats"] = stats.as_dict()
     out.extra["n_slots"] = n_slots
+    return out
+
+
+def gmres_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tolerance=1e-6, max_iterations=2560,
+                  restart=32, shift=DEFAULT_SHIFT, n_slots=16, adjoint=False, return_fields=False,
+                  fields_dtype=torch.complex64, rx_index=None, workspace: Workspace | None = None) -> BatchResult:
+    """Restarted GMRES(restart) for every system (nsrno/wave_solver.py:9-36 on the device).
+
+    Same inputs and outputs as :func:`solve_batched`; ``iterations`` counts
+    Arnoldi steps, i.e. operator applications.
+    """
+    lib = _lib.load()
+    g = medium.geometry
+    dev = medium.device
+    freqs = torch.as_tensor(freqs, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+    S = int(freqs.numel())
+    if angles is None and rhs is None:
+        raise ValueError("either angles (plane-wave sources) or rhs must be given")
+    if angles is not None:
+        angles = torch.as_tensor(angles, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+        if angles.numel() != S:
+            raise ValueError("freqs and angles must have the same length")
+
+    def field_arg(t, name):
+        if t is None:
+            return None
+        t = torch.as_tensor(t)
+        if tuple(t.shape) != (S, g.nz, g.nx) or not t.is_complex():
+            raise ValueError(f"{name} must be a complex tensor of shape {(S, g.nz, g.nx)}")
+        return t.to(dev, torch.complex64).contiguous()
+
+    rhs = field_arg(rhs, "rhs")
+    x0 = field_arg(x0, "x0")
+    if rx_index is None:
+        rx_index = g.rx_index(dev)
+    n_rx = int(rx_index.numel())
+    n_slots = max(1, min(int(n_slots), S)) if S else 1
+    grid = medium._grid
+    ws_bytes = lib.nsr_gmres_workspace_size(ctypes.byref(grid), n_slots, int(restart))
+    if ws_bytes == 0:
+        raise ValueError("unsupported grid or restart length for GMRES")
+    ws = (workspace or _default_ws).get(ws_bytes, dev)
+    out = BatchResult(iq=torch.empty((S, n_rx), dtype=torch.complex128, device=dev),
+                      residual=torch.empty(S, dtype=torch.float64, device=dev),
+                      iterations=torch.empty(S, dtype=torch.int32, device=dev),
+                      status=torch.empty(S, dtype=torch.int32, device=dev),
+                      fields=torch.empty((S, g.nz, g.nx), dtype=fields_dtype, device=dev) if return_fields else None)
+    params = _lib.NsrGmresParams(float(tolerance), float(shift), int(max_iterations), int(restart), int(n_slots),
+                                 int(bool(adjoint)), int(fields_dtype == torch.complex128), 0)
+    _lib.check(lib.nsr_gmres_batched(
+        ctypes.byref(grid), _ptr(medium.material), _ptr(freqs), _ptr(angles), S, _ptr(rhs), _ptr(x0),
+        _ptr(rx_index), n_rx, ctypes.byref(params), _ptr(ws), ws.numel(), _ptr(out.iq), _ptr(out.residual),
+        _ptr(out.iterations), _ptr(out.status), _ptr(out.fields), _stream()))
     return out
 
 
@@ -199,7 +274,7 @@ def apply(medium: Medium, x: torch.Tensor, freqs, adjoint=False):
     if freqs.numel() != x.shape[0]:
         raise ValueError("one frequency per field")
     y = torch.empty_like(x)
-    _lib.check(_lib.load().nsr_apply(ctypes.byref(medium._grid), _ptr(medium.coef), _ptr(freqs), x.shape[0],
+    _lib.check(_lib.load().nsr_apply(ctypes.byref(medium._grid), _ptr(medium.material), _ptr(freqs), x.shape[0],
                                      int(bool(adjoint)), 0 if x.dtype == torch.complex64 else 1,
                                      _ptr(x), _ptr(y), _stream()))
     return y
@@ -243,17 +318,19 @@ def grad_accum(medium: Medium, freqs, u: torch.Tensor, lam: torch.Tensor, g_logc
     dev = medium.device
     for name, t in (("u", u), ("lam", lam)):
         _require_cuda(t, name)
-        if t.dtype != torch.complex64 or t.dim() != 3 or tuple(t.shape[1:]) != (g.nz, g.nx):
-            raise ValueError(f"{name} must be complex64 [S, nz, nx]")
-    u = u.contiguous()
-    lam = lam.contiguous()
+        if t.dtype not in (torch.complex64, torch.complex128) or t.dim() != 3 or tuple(t.shape[1:]) != (g.nz, g.nx):
+            raise ValueError(f"{name} must be complex64 or complex128 [S, nz, nx]")
+    dtype = torch.complex128 if torch.complex128 in (u.dtype, lam.dtype) else torch.complex64
+    u = u.to(dtype).contiguous()
+    lam = lam.to(dtype).contiguous()
     freqs = torch.as_tensor(freqs, dtype=torch.float64, device=dev).reshape(-1).contiguous()
     if g_logc is None:
         g_logc = torch.zeros((g.nz, g.nx), dtype=torch.float64, device=dev)
     if g_logrho is None:
         g_logrho = torch.zeros((g.nz, g.nx), dtype=torch.float64, device=dev)
-    _lib.check(_lib.load().nsr_grad_accum(ctypes.byref(medium._grid), _ptr(medium.coef), _ptr(freqs), u.shape[0],
-                                          _ptr(u), _ptr(lam), _ptr(g_logc), _ptr(g_logrho), _stream()))
+    _lib.check(_lib.load().nsr_grad_accum(ctypes.byref(medium._grid), _ptr(medium.material), _ptr(freqs), u.shape[0],
+                                          int(dtype == torch.complex128), _ptr(u), _ptr(lam), _ptr(g_logc),
+                                          _ptr(g_logrho), _stream()))
     return g_logc, g_logrho
 
 

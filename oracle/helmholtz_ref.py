@@ -268,17 +268,21 @@ def bicgstab(apply, rhs, x=None, tolerance=1e-3, max_iterations=800, replace_eve
     return x, dict(reason=reason, iterations=used, residual=actual, method="BiCGSTAB")
 
 
-def gmres(apply, rhs, x=None, restart=30, max_cycles=200, tolerance=1e-7, callback=None):
-    """Restarted GMRES with two classical Gram-Schmidt passes (wave_solver.py:9-36).
+def gmres(apply, rhs, x=None, restart=30, max_cycles=200, tolerance=1e-7, callback=None, precondition=None):
+    """Restarted right-preconditioned GMRES with two classical Gram-Schmidt passes (wave_solver.py:9-36).
 
-    Happy breakdown below 1e-12; the small least-squares problem is solved in
-    complex128 with ``lstsq`` as in the reference.  Returns ``(x, reason, steps)``.
+    ``precondition`` is the right preconditioner (identity when None); the
+    preconditioned directions are kept as in the reference.  Happy breakdown
+    below 1e-12; the small least-squares problem is solved in complex128 with
+    ``lstsq`` as in the reference.  Returns ``(x, reason, steps)``.
     """
     rhs = np.asarray(rhs, dtype=np.complex128)
     x = np.zeros_like(rhs) if x is None else np.array(x, dtype=np.complex128)
     scale = max(np.linalg.norm(rhs), 1e-30)
     n = rhs.size
     basis = np.empty((restart + 1, n), dtype=np.complex128)
+    directions = np.empty((restart, n), dtype=np.complex128)
+    precondition = precondition or (lambda v: v)
     steps = 0
     for _ in range(max_cycles):
         residual = rhs - apply(x)
@@ -291,7 +295,8 @@ def gmres(apply, rhs, x=None, restart=30, max_cycles=200, tolerance=1e-7, callba
         h = np.zeros((restart + 1, restart), dtype=np.complex128)
         used = restart
         for j in range(restart):
-            w = apply(basis[j])
+            directions[j] = precondition(basis[j])
+            w = apply(directions[j])
             steps += 1
             for _ in range(2):
                 coefficients = basis[: j + 1].conj() @ w
@@ -305,7 +310,7 @@ def gmres(apply, rhs, x=None, restart=30, max_cycles=200, tolerance=1e-7, callba
         target = np.zeros(used + 1, dtype=np.complex128)
         target[0] = beta
         y = np.linalg.lstsq(h[: used + 1, :used], target, rcond=None)[0]
-        x = x + basis[:used].T @ y
+        x = x + directions[:used].T @ y
     final = float(np.linalg.norm(rhs - apply(x)) / scale)
     if callback is not None:
         callback(steps, final)

@@ -61,7 +61,7 @@ def test_argument_errors_need_no_device(lib):
     good = grid()
     assert lib.nsr_setup_material(ctypes.byref(good), null, null, null, null, null) == 1001
     assert lib.nsr_apply(ctypes.byref(good), null, null, 1, 0, 0, null, null, null) == 1001
-    assert lib.nsr_grad_accum(ctypes.byref(good), null, null, 1, null, null, null, null, null) == 1001
+    assert lib.nsr_grad_accum(ctypes.byref(good), null, null, 1, 0, null, null, null, null, null) == 1001
 
 
 def test_workspace_queries(lib):

@@ -1,0 +1,74 @@
+"""Reference-facing contracts on the GPU: solve_frequency, solve_system and the
+DenseSurrogate drop-in (nsrno/wave_solver.py:38-67, nsrno/dense_wave.py:167-259,
+nsrno/dense_surrogate.py:9-36)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel, spec_of
+from oracle import helmholtz_ref as H
+
+pytestmark = pytest.mark.gpu
+
+
+def blob(dev):
+    from nsrno_b200 import Geometry
+    from nsrno_b200.media import blob_record
+    rec = blob_record()
+    return rec, Geometry.from_record(rec)
+
+
+def oracle_iq(rec, f, th):
+    spec = spec_of(rec)
+    u = H.solve_lu(H.operator(spec, rec.c, rec.rho, rec.alpha, f), H.plane_wave_rhs(spec, f, th))
+    return H.receivers(spec, u), u
+
+
+def test_solve_frequency_contract(cuda):
+    from nsrno_b200 import PlaneWaveModel, solve_frequency
+    rec, geo = blob(cuda)
+    model = PlaneWaveModel(geo, np.rad2deg(rec.angles), alpha=rec.alpha)
+    medium = torch.as_tensor(np.stack((rec.c, rec.rho))[None], device=cuda)
+    pred, status = solve_frequency(model, medium, 1.5e6, 1, tolerance=1e-6, max_iterations=2560, restart=32)
+    assert set(status) >= {"reason", "initial_neural_iterations", "solver_iterations", "relative_residual",
+                           "seconds", "trace"}
+    assert status["reason"] == "converged" and status["relative_residual"] < 1e-6
+    assert pred.dtype == torch.complex64 and pred.shape == (192,)
+    ref, _ = oracle_iq(rec, 1.5e6, rec.angles[1])
+    assert rel(pred.cpu().numpy(), ref) < 1e-4
+
+
+@pytest.mark.parametrize("method", ["gmres", "bicgstab"])
+def test_solve_system_contract(cuda, method):
+    from nsrno_b200 import HelmholtzSystem, Medium, plane_wave_rhs, solve_system
+    rec, geo = blob(cuda)
+    med = Medium(geo, rec.c, rec.rho, rec.alpha, device=cuda)
+    f = 1.0e6
+    rhs = plane_wave_rhs(med, [f] * 3, rec.angles)
+    x, info = solve_system(HelmholtzSystem(med, f), rhs, tolerance=1e-7, method=method)
+    assert set(info) >= {"reason", "steps", "residual", "max_angle_residual", "seconds", "dtype", "method"}
+    assert info["reason"] == "converged" and info["max_angle_residual"] < 1e-7
+    for k in range(3):
+        _, u = oracle_iq(rec, f, rec.angles[k])
+        assert rel(x[k].cpu().numpy().ravel(), u) < 1e-5
+
+
+def test_surrogate_forward_backward_and_truncated(cuda):
+    from nsrno_b200 import HelmholtzSurrogate, bin_frequency
+    rec, geo = blob(cuda)
+    # a 256x256 record at 0.1 mm with bins in the 1 MHz range of this grid
+    sur = HelmholtzSurrogate(geo, np.rad2deg(rec.angles), bins=[60, 61], response=False)
+    medium = torch.as_tensor(np.stack((rec.c, rec.rho)).astype(np.float64), device=cuda).requires_grad_(True)
+    alpha = torch.as_tensor(rec.alpha.astype(np.float64), device=cuda)
+    out = sur(medium, alpha, 60, tolerance=1e-8)
+    assert out.shape == (3, 192) and out.dtype == torch.complex128
+    ref = np.stack([oracle_iq(rec, bin_frequency(60), th)[0] for th in rec.angles])
+    assert rel(out.detach().cpu().numpy(), ref) < 1e-5
+    out.abs().square().sum().backward()
+    assert torch.isfinite(medium.grad).all() and float(medium.grad.abs().max()) > 0
+    ch, res = sur.truncated(medium.detach(), alpha, 60, iterations=4)
+    assert ch.shape == (3, 192) and 0 < res < 1
+    with pytest.raises(RuntimeError, match="Forward failed to converge"):
+        from nsrno_b200 import AcquisitionData, implicit_channels
+        implicit_channels(medium, alpha, AcquisitionData(geo, np.rad2deg(rec.angles), response=False),
+                          bin_frequency(60), [0], tolerance=1e-12, max_iterations=2)

@@ -28,7 +28,7 @@ def medium_of(rec, dev):
 
 
 def planes(med):
-    a, b, t = med.coef.double().cpu().numpy()
+    a, b, t = med.coef64.cpu().numpy()
     return a, b, t
 
 
@@ -40,6 +40,9 @@ def test_material_planes_match_rounded_double(cuda):
     for ref, got in ((a, ga), (b, gb), (t, gt)):
         ulps = np.abs(ref.astype(np.float32).view(np.int32) - got.view(np.int32))
         assert ulps.max() <= 1
+    da, db, dt = med.coef64.cpu().numpy()
+    for ref, got in ((a, da), (b, db), (t, dt)):
+        assert np.max(np.abs(ref - got) / np.maximum(np.abs(ref), 1e-300)) < 1e-15
 
 
 @pytest.mark.parametrize("adjoint", [False, True])
@@ -120,7 +123,8 @@ def test_plane_wave_rhs_matches_oracle(cuda):
         assert rel(b[s].ravel(), H.plane_wave_rhs(spec, f, th)) < 1e-14
 
 
-def test_grad_accum_matches_oracle(cuda):
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+def test_grad_accum_matches_oracle(cuda, dtype):
     from nsrno_b200 import grad_accum
     rec = small_record()
     spec = spec_of(rec)
@@ -128,8 +132,8 @@ def test_grad_accum_matches_oracle(cuda):
     a, b, t = planes(med)
     rng = np.random.default_rng(4)
     S = 2
-    u = (rng.standard_normal((S, rec.nz, rec.nx)) + 1j * rng.standard_normal((S, rec.nz, rec.nx))).astype(np.complex64)
-    lam = (rng.standard_normal((S, rec.nz, rec.nx)) + 1j * rng.standard_normal((S, rec.nz, rec.nx))).astype(np.complex64)
+    u = (rng.standard_normal((S, rec.nz, rec.nx)) + 1j * rng.standard_normal((S, rec.nz, rec.nx))).astype(dtype)
+    lam = (rng.standard_normal((S, rec.nz, rec.nx)) + 1j * rng.standard_normal((S, rec.nz, rec.nx))).astype(dtype)
     gc, gr = grad_accum(med, rec.frequencies, torch.as_tensor(u, device=cuda), torch.as_tensor(lam, device=cuda))
     ref_c = np.zeros((rec.nz, rec.nx))
     ref_r = np.zeros((rec.nz, rec.nx))

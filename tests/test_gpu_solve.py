@@ -27,7 +27,7 @@ def test_blob_record_matches_lu(cuda):
     from nsrno_b200 import solve_batched
     rec, med = blob_case(cuda)
     spec = spec_of(rec)
-    a, b, t = med.coef.double().cpu().numpy()
+    a, b, t = med.coef64.cpu().numpy()
     f, th = rec.systems()
     res = solve_batched(med, f, th, tolerance=1e-7, max_iterations=2000, return_fields=True, n_slots=4)
     assert res.reasons() == ["converged"] * len(f)
@@ -115,7 +115,7 @@ def test_adjoint_solve_matches_lu(cuda):
     from nsrno_b200 import solve_batched
     rec, med = blob_case(cuda)
     spec = spec_of(rec)
-    a, b, t = med.coef.double().cpu().numpy()
+    a, b, t = med.coef64.cpu().numpy()
     rng = np.random.default_rng(9)
     g = np.zeros((1, rec.nz, rec.nx), np.complex64)
     g[0, rec.face, rec.rx_cols] = (rng.standard_normal(len(rec.rx_cols)) + 1j * rng.standard_normal(len(rec.rx_cols)))
