@@ -222,6 +222,34 @@ int nsr_grad_accum(const NsrGrid* grid, const void* material, const double* freq
                    int32_t n_systems, int32_t precision, const void* u, const void* lam,
                    double* g_logc, double* g_logrho, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * The dense path's 8th-order staggered split-PML operator
+ * (nsrno/conditioned_wave.py:52-80 projected as nsrno/dense_wave.py:66-68) and
+ * its analytic adjoint (nsrno/dense_wave.py:70-82), evaluated as a direct
+ * radius-4 stencil on the padded grid instead of 11 FFTs.
+ * ------------------------------------------------------------------------- */
+typedef struct NsrDenseGrid {
+  int32_t H, W;              /* padded grid (rows, columns)                    */
+  int32_t pz, px;            /* offset of the native region                    */
+  int32_t h, w;              /* native region (the mask)                       */
+  double dx;                 /* node spacing [m]                               */
+} NsrDenseGrid;
+
+/* Coefficients of one medium at one frequency, double, packed as
+ * ax[H][W], az[H][W], mass[H][W] (c128), then along x (c128 [W] each)
+ * svx, gvx, lx = mx/(D-arx), rx = 1 + (1-mx)/(D-arx), then along z
+ * (c128 [H] each) svz, gvz, lz, rz.  Built by nsrno_b200.dense. */
+size_t nsr_dense_coef_bytes(const NsrDenseGrid* grid);
+size_t nsr_dense_workspace_size(const NsrDenseGrid* grid, int32_t n_fields, int32_t precision);
+
+/* y = A x (adjoint 0) or A^H x (adjoint 1) for n_fields fields [n][H][W]
+ * sharing one coefficient set; scal = (D-1)/(D k0^2).  precision 0: c64,
+ * 1: c128.  Replaces projected_operator / adjoint_operator
+ * (nsrno/dense_wave.py:66-82). */
+int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, double scal_re, double scal_im,
+                    int32_t n_fields, int32_t adjoint, int32_t precision, const void* x, void* y,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,7 +18,7 @@ REASONS = {CONVERGED: "converged", ITERATION_BUDGET: "iteration_budget", BREAKDO
 EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_material", "nsr_apply",
            "nsr_precondition_workspace_size", "nsr_precondition", "nsr_precondition_noalloc", "nsr_plane_wave_rhs",
            "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_gmres_workspace_size", "nsr_gmres_batched",
-           "nsr_grad_accum")
+           "nsr_grad_accum", "nsr_dense_coef_bytes", "nsr_dense_workspace_size", "nsr_dense_apply")
 
 
 class NsrGrid(ctypes.Structure):
@@ -34,6 +34,11 @@ class NsrSolveParams(ctypes.Structure):
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
                 ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32),
                 ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class NsrDenseGrid(ctypes.Structure):
+    _fields_ = [("H", ctypes.c_int32), ("W", ctypes.c_int32), ("pz", ctypes.c_int32), ("px", ctypes.c_int32),
+                ("h", ctypes.c_int32), ("w", ctypes.c_int32), ("dx", ctypes.c_double)]
 
 
 class NsrGmresParams(ctypes.Structure):
@@ -90,6 +95,12 @@ def load():
     lib.nsr_gmres_workspace_size.argtypes = [G, I, I]
     lib.nsr_gmres_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrGmresParams),
                                       P, S, P, P, P, P, P, P]
+    DG = ctypes.POINTER(NsrDenseGrid)
+    lib.nsr_dense_coef_bytes.restype = S
+    lib.nsr_dense_coef_bytes.argtypes = [DG]
+    lib.nsr_dense_workspace_size.restype = S
+    lib.nsr_dense_workspace_size.argtypes = [DG, I, I]
+    lib.nsr_dense_apply.argtypes = [DG, P, D, D, I, I, I, P, P, P, S, P]
     for name in EXPORTS:
         getattr(lib, name)
     _lib = lib

@@ -1,0 +1,221 @@
+// The dense path's operator (nsrno/conditioned_wave.py:52-80, projected as in
+// nsrno/dense_wave.py:66-68) and its analytic adjoint (nsrno/dense_wave.py:70-82),
+// evaluated as a direct radius-4 staggered stencil instead of 11 FFTs.
+//
+// The reference evaluates the 8th-order staggered derivative D (forward, at
+// n + 1/2) and its negative adjoint (divergence) by FFT on a padded grid.  The
+// field is masked to the native region and the padding is at least 8 nodes
+// wide, so the periodic FFT evaluation equals the direct stencil with zero
+// values outside the grid:
+//   (D p)[n]     = (1/dx) sum_k a_k (p[n+1+k] - p[n-k])
+//   (-D^H f)[n]  = (1/dx) sum_k a_k (f[n+k]   - f[n-1-k])
+// with a = (1225/1024, -245/3072, 49/5120, -5/7168).
+// Pass 1 writes the staggered fluxes, pass 2 takes their divergence.
+#include "nsr_internal.cuh"
+
+__constant__ double c_dense_a[4] = {1225.0 / 1024.0, -245.0 / 3072.0, 49.0 / 5120.0, -5.0 / 7168.0};
+
+struct DenseCoef {
+  // planes [H][W]
+  const double* ax;
+  const double* az;
+  const double2* mass;
+  // profiles along x [W] and z [H]
+  const double2 *svx, *gvx, *lx, *rx;
+  const double2 *svz, *gvz, *lz, *rz;
+};
+
+struct DenseGeo {
+  int H, W, pz, px, h, w;
+  double dx;
+  double2 scal;   // (D - 1) / (D k0^2)
+};
+
+__host__ __device__ inline size_t dense_coef_doubles(int H, int W) { return (size_t)H * W * 4 + 8 * (size_t)W + 8 * (size_t)H; }
+
+__host__ __device__ inline DenseCoef dense_unpack(const double* c, int H, int W) {
+  DenseCoef d;
+  const size_t n = (size_t)H * W;
+  d.ax = c;
+  d.az = c + n;
+  d.mass = (const double2*)(c + 2 * n);
+  const double2* px = (const double2*)(c + 4 * n);
+  d.svx = px; d.gvx = px + W; d.lx = px + 2 * W; d.rx = px + 3 * W;
+  const double2* pz = px + 4 * W;
+  d.svz = pz; d.gvz = pz + H; d.lz = pz + 2 * H; d.rz = pz + 3 * H;
+  return d;
+}
+
+template <typename T> struct DC;
+template <> struct DC<float> { typedef float2 C; static __device__ C from(double2 a) { return make_float2((float)a.x, (float)a.y); } };
+template <> struct DC<double> { typedef double2 C; static __device__ C from(double2 a) { return a; } };
+
+__device__ __forceinline__ bool dense_inside(const DenseGeo& g, int i, int j) {
+  return i >= g.pz && i < g.pz + g.h && j >= g.px && j < g.px + g.w;
+}
+
+// Pass 1.  Forward: X = ax svx D_x(mask p), gX = gvx X, and the same along z.
+// Adjoint: w = conj(scal) mask p, flux_x = conj(ax svx) (-D_x(conj(lx) w) - conj(gvx) D_x(conj(rx) w)).
+template <typename T, bool ADJ>
+__global__ void k_dense_flux(DenseGeo g, const double* __restrict__ coef, const typename DC<T>::C* __restrict__ p,
+                             typename DC<T>::C* __restrict__ tmp, int nf) {
+  typedef typename DC<T>::C C;
+  const DenseCoef dc = dense_unpack(coef, g.H, g.W);
+  const long long n = (long long)g.H * g.W;
+  const int f = blockIdx.y;
+  const C* pf = p + f * n;
+  C* t = tmp + f * 4 * n;
+  const C zero = cx<C>(T(0), T(0));
+  const T inv_dx = (T)(1.0 / g.dx);
+  const C wscal = DC<T>::from(conjc(g.scal));
+  auto PM = [&](int i2, int j2) -> C {
+    if (i2 < 0 || i2 >= g.H || j2 < 0 || j2 >= g.W || !dense_inside(g, i2, j2)) return zero;
+    return pf[(long long)i2 * g.W + j2];
+  };
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.W), j = (int)(k - (long long)i * g.W);
+    if (!ADJ) {
+      C gx = zero, gz = zero;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const T a = (T)c_dense_a[q];
+        gx = gx + a * (PM(i, j + 1 + q) - PM(i, j - q));
+        gz = gz + a * (PM(i + 1 + q, j) - PM(i - q, j));
+      }
+      const C X = (inv_dx * (T)dc.ax[k]) * (DC<T>::from(dc.svx[j]) * gx);
+      const C Z = (inv_dx * (T)dc.az[k]) * (DC<T>::from(dc.svz[i]) * gz);
+      t[k] = X;
+      t[n + k] = DC<T>::from(dc.gvx[j]) * X;
+      t[2 * n + k] = Z;
+      t[3 * n + k] = DC<T>::from(dc.gvz[i]) * Z;
+    } else {
+      // along x the left/right factors depend on the column of each node
+      C fl = zero, fr = zero, zl = zero, zr = zero;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const T a = (T)c_dense_a[q];
+        const int je = j + 1 + q, jw = j - q;
+        const C we = PM(i, je), ww = PM(i, jw);
+        const C le = je < g.W ? conjc(DC<T>::from(dc.lx[je])) * we : zero;
+        const C lw = jw >= 0 ? conjc(DC<T>::from(dc.lx[jw])) * ww : zero;
+        const C re = je < g.W ? conjc(DC<T>::from(dc.rx[je])) * we : zero;
+        const C rw = jw >= 0 ? conjc(DC<T>::from(dc.rx[jw])) * ww : zero;
+        fl = fl + a * (le - lw);
+        fr = fr + a * (re - rw);
+        const int is = i + 1 + q, in = i - q;
+        const C ws = PM(is, j), wn = PM(in, j);
+        const C ls = is < g.H ? conjc(DC<T>::from(dc.lz[is])) * ws : zero;
+        const C ln = in >= 0 ? conjc(DC<T>::from(dc.lz[in])) * wn : zero;
+        const C rs = is < g.H ? conjc(DC<T>::from(dc.rz[is])) * ws : zero;
+        const C rn = in >= 0 ? conjc(DC<T>::from(dc.rz[in])) * wn : zero;
+        zl = zl + a * (ls - ln);
+        zr = zr + a * (rs - rn);
+      }
+      // w = conj(scal) mask p was left out of the sums: apply it once here
+      const C fx = (T(-1) * inv_dx) * (wscal * (fl + conjc(DC<T>::from(dc.gvx[j])) * fr));
+      const C fz = (T(-1) * inv_dx) * (wscal * (zl + conjc(DC<T>::from(dc.gvz[i])) * zr));
+      t[k] = conjc(DC<T>::from(dc.svx[j]) * cx<C>((T)dc.ax[k], T(0))) * fx;
+      t[2 * n + k] = conjc(DC<T>::from(dc.svz[i]) * cx<C>((T)dc.az[k], T(0))) * fz;
+    }
+  }
+}
+
+// Pass 2.  Forward: y = mask (scal (lx divX + rx div gX + lz divZ + rz div gZ) + mass p) + (1 - mask) p.
+// Adjoint: y = mask (D^H flux_x + D^H flux_z + conj(mass) p) + (1 - mask) p.
+template <typename T, bool ADJ>
+__global__ void k_dense_div(DenseGeo g, const double* __restrict__ coef, const typename DC<T>::C* __restrict__ p,
+                            const typename DC<T>::C* __restrict__ tmp, typename DC<T>::C* __restrict__ y, int nf) {
+  typedef typename DC<T>::C C;
+  const DenseCoef dc = dense_unpack(coef, g.H, g.W);
+  const long long n = (long long)g.H * g.W;
+  const int f = blockIdx.y;
+  const C* pf = p + f * n;
+  const C* t = tmp + f * 4 * n;
+  C* yf = y + f * n;
+  const C zero = cx<C>(T(0), T(0));
+  const T inv_dx = (T)(1.0 / g.dx);
+  auto F = [&](int plane, int i2, int j2) -> C {
+    if (i2 < 0 || i2 >= g.H || j2 < 0 || j2 >= g.W) return zero;
+    return t[plane * n + (long long)i2 * g.W + j2];
+  };
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.W), j = (int)(k - (long long)i * g.W);
+    const C pk = pf[k];
+    if (!dense_inside(g, i, j)) { yf[k] = pk; continue; }
+    if (!ADJ) {
+      C dX = zero, dgX = zero, dZ = zero, dgZ = zero;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const T a = (T)c_dense_a[q];
+        dX = dX + a * (F(0, i, j + q) - F(0, i, j - 1 - q));
+        dgX = dgX + a * (F(1, i, j + q) - F(1, i, j - 1 - q));
+        dZ = dZ + a * (F(2, i + q, j) - F(2, i - 1 - q, j));
+        dgZ = dgZ + a * (F(3, i + q, j) - F(3, i - 1 - q, j));
+      }
+      const C part = DC<T>::from(dc.lx[j]) * dX + DC<T>::from(dc.rx[j]) * dgX +
+                     DC<T>::from(dc.lz[i]) * dZ + DC<T>::from(dc.rz[i]) * dgZ;
+      yf[k] = DC<T>::from(g.scal) * (inv_dx * part) + DC<T>::from(dc.mass[k]) * pk;
+    } else {
+      C dX = zero, dZ = zero;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const T a = (T)c_dense_a[q];
+        dX = dX + a * (F(0, i, j + q) - F(0, i, j - 1 - q));
+        dZ = dZ + a * (F(2, i + q, j) - F(2, i - 1 - q, j));
+      }
+      // D^H f = -(-D^H f)
+      yf[k] = (T(-1) * inv_dx) * (dX + dZ) + conjc(DC<T>::from(dc.mass[k])) * pk;
+    }
+  }
+}
+
+extern "C" size_t nsr_dense_coef_bytes(const NsrDenseGrid* g) {
+  if (!g || g->H <= 0 || g->W <= 0) return 0;
+  return sizeof(double) * dense_coef_doubles(g->H, g->W);
+}
+
+extern "C" size_t nsr_dense_workspace_size(const NsrDenseGrid* g, int32_t n_fields, int32_t precision) {
+  if (!g || g->H <= 0 || g->W <= 0 || n_fields < 0 || (precision != 0 && precision != 1)) return 0;
+  return (size_t)4 * g->H * g->W * n_fields * (precision ? 16 : 8);
+}
+
+extern "C" int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, double scal_re, double scal_im,
+                               int32_t n_fields, int32_t adjoint, int32_t precision, const void* x, void* y,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  if (!grid || !coef || !x || !y || n_fields < 0 || n_fields > 65535) return NSR_ERR_ARGUMENT;
+  if (grid->H < 3 || grid->W < 3 || grid->h < 1 || grid->w < 1 || grid->pz < 0 || grid->px < 0 ||
+      grid->pz + grid->h > grid->H || grid->px + grid->w > grid->W || !(grid->dx > 0))
+    return NSR_ERR_ARGUMENT;
+  if (precision != 0 && precision != 1) return NSR_ERR_ARGUMENT;
+  if (n_fields == 0) return 0;
+  if (!workspace || workspace_bytes < nsr_dense_workspace_size(grid, n_fields, precision)) return NSR_ERR_WORKSPACE;
+  DenseGeo g;
+  g.H = grid->H; g.W = grid->W; g.pz = grid->pz; g.px = grid->px; g.h = grid->h; g.w = grid->w; g.dx = grid->dx;
+  g.scal = make_double2(scal_re, scal_im);
+  const long long n = (long long)g.H * g.W;
+  int bx = (int)((n + 255) / 256);
+  if (bx > 4096) bx = 4096;
+  const dim3 gr(bx, n_fields);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == 0) {
+    float2* t = (float2*)workspace;
+    if (adjoint) {
+      k_dense_flux<float, true><<<gr, 256, 0, st>>>(g, coef, (const float2*)x, t, n_fields);
+      k_dense_div<float, true><<<gr, 256, 0, st>>>(g, coef, (const float2*)x, t, (float2*)y, n_fields);
+    } else {
+      k_dense_flux<float, false><<<gr, 256, 0, st>>>(g, coef, (const float2*)x, t, n_fields);
+      k_dense_div<float, false><<<gr, 256, 0, st>>>(g, coef, (const float2*)x, t, (float2*)y, n_fields);
+    }
+  } else {
+    double2* t = (double2*)workspace;
+    if (adjoint) {
+      k_dense_flux<double, true><<<gr, 256, 0, st>>>(g, coef, (const double2*)x, t, n_fields);
+      k_dense_div<double, true><<<gr, 256, 0, st>>>(g, coef, (const double2*)x, t, (double2*)y, n_fields);
+    } else {
+      k_dense_flux<double, false><<<gr, 256, 0, st>>>(g, coef, (const double2*)x, t, n_fields);
+      k_dense_div<double, false><<<gr, 256, 0, st>>>(g, coef, (const double2*)x, t, (double2*)y, n_fields);
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}

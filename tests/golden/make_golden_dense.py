@@ -1,0 +1,65 @@
+"""Generate golden vectors of the reference's 8th-order dense operator
+(run in a container that has the reference checked out; not needed on the GPU box).
+
+    python tests/golden/make_golden_dense.py /root/reference
+
+Writes ``tests/golden/reference_dense.npz`` with a synthetic acquisition spec
+(the V5 metadata is not part of the reference checkout), a seeded medium and
+attenuation map, and, for a seeded complex128 probe field p on the padded
+grid, ``projected_operator(system, p)`` and ``adjoint_operator(system, p)``
+(nsrno/dense_wave.py:66-82, nsrno/conditioned_wave.py:52-80) restricted to the
+native (masked) region -- outside it both operators are the identity.
+The probe is ``default_rng(PROBE_SEED)`` normal real + 1j normal imag, [H, W].
+"""
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+PROBE_SEED = 20261203
+SPEC = {"medium_shape": [32, 40], "dx_m": 5e-5, "x0_m": -0.001, "z0_m": -0.0002, "native_dt_s": 2.5e-9,
+        "pml": 6, "eta_per_unit_alpha": [0.012, 0.021], "taus_s": [2.0e-8, 1.5e-7],
+        "source_c_lookup_zx": [10, 20]}
+FREQS = [4.5e6, 7.2e6]
+
+
+def main(reference_root):
+    sys.path.insert(0, str(reference_root))
+    import torch
+    from nsrno.conditioned_wave import ConditionedFrequencySystem, FrequencyGeometry
+    from nsrno.dense_wave import adjoint_operator, projected_operator
+
+    torch.set_default_dtype(torch.float64)
+    g = FrequencyGeometry(SPEC)
+    h, w = SPEC["medium_shape"]
+    rng = np.random.default_rng(5)
+    c = 1540.0 + 60.0 * rng.standard_normal((h, w))
+    rho = 1000.0 + 50.0 * rng.standard_normal((h, w))
+    alpha = rng.uniform(0.2, 1.2, (h, w))
+    medium = torch.tensor(np.stack((c, rho)))
+    out = {"spec": json.dumps(SPEC), "medium": np.stack((c, rho)), "alpha": alpha, "freqs": np.array(FREQS),
+           "probe_seed": PROBE_SEED, "H": g.H, "W": g.W, "pz": g.pz, "px": g.px}
+    prng = np.random.default_rng(PROBE_SEED)
+    p = prng.standard_normal((g.H, g.W)) + 1j * prng.standard_normal((g.H, g.W))
+    pt = torch.tensor(p)[None]
+    for k, f in enumerate(FREQS):
+        s = ConditionedFrequencySystem(g, medium, torch.tensor(alpha), f)
+        y = projected_operator(s, pt)[0].numpy()
+        yh = adjoint_operator(s, pt)[0].numpy()
+        inner = (slice(g.pz, g.pz + h), slice(g.px, g.px + w))
+        out[f"y{k}"] = y[inner]
+        out[f"yh{k}"] = yh[inner]
+        # outside the native region both operators leave p unchanged
+        mask = np.zeros((g.H, g.W), bool)
+        mask[inner] = True
+        assert np.allclose(y[~mask], p[~mask]) and np.allclose(yh[~mask], p[~mask])
+    path = Path(__file__).resolve().parent / "reference_dense.npz"
+    np.savez_compressed(path, **out)
+    print(path, {k: np.shape(v) for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

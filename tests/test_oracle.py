@@ -164,3 +164,26 @@ def test_time_lu_frequency_reports_residual():
     fields, seconds, res = H.time_lu_frequency(spec, rec.c, rec.rho, rec.alpha, 1e6, rec.angles)
     assert fields.shape == (3, spec.n)
     assert res < 1e-10 and seconds > 0
+
+
+def test_dense_oracle_matches_reference_operator():
+    """The dense (8th-order, split-PML) operator and its adjoint against the reference's own output."""
+    import json
+    from conftest import GOLDEN
+    from oracle import dense_ref as D
+    with np.load(GOLDEN / "reference_dense.npz") as z:
+        gold = {k: z[k] for k in z.files}
+    spec = json.loads(str(gold["spec"]))
+    g = D.DenseGeometry(spec)
+    assert (g.H, g.W, g.pz, g.px) == (int(gold["H"]), int(gold["W"]), int(gold["pz"]), int(gold["px"]))
+    prng = np.random.default_rng(int(gold["probe_seed"]))
+    p = prng.standard_normal((g.H, g.W)) + 1j * prng.standard_normal((g.H, g.W))
+    inner = (slice(g.pz, g.pz + g.h), slice(g.px, g.px + g.w))
+    for k, f in enumerate(gold["freqs"]):
+        s = D.DenseSystem(g, gold["medium"], gold["alpha"], f)
+        assert rel(s.apply(p)[inner], gold[f"y{k}"]) < 1e-12
+        assert rel(s.adjoint(p)[inner], gold[f"yh{k}"]) < 1e-12
+        q = prng.standard_normal((g.H, g.W)) + 1j * prng.standard_normal((g.H, g.W))
+        left = np.vdot(q, s.apply(p))
+        right = np.vdot(s.adjoint(q), p)
+        assert abs(left - right) / abs(left) < 1e-12
