@@ -70,6 +70,9 @@ typedef struct NsrSolveParams {
   double restart_factor;     /* restart (fresh shadow vector) once the true
                                 residual fell by this factor since the last
                                 restart (1e-2; 0 disables)                     */
+  double warm_gate;          /* an initial field x0 whose relative residual
+                                exceeds this is discarded and the system starts
+                                from zero (1.0; 0 accepts every x0)            */
   int32_t max_iterations;    /* BiCGSTAB iterations per system                 */
   int32_t replace_every;     /* true-residual replacement period (40)          */
   int32_t n_slots;           /* systems resident at once                       */
@@ -91,6 +94,8 @@ typedef struct NsrSolveStats {
   int32_t kernel_timed[8];   /* launches averaged in kernel_ms                  */
   int64_t launches;          /* kernels launched by the call                    */
   int32_t graph_launches;    /* CUDA graph launches                             */
+  int32_t warm_accepted;     /* initial fields kept                             */
+  int32_t warm_rejected;     /* initial fields discarded by the warm_gate       */
   int32_t reserved;
 } NsrSolveStats;
 

@@ -30,7 +30,7 @@ class NsrGrid(ctypes.Structure):
 
 class NsrSolveParams(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double), ("restart_factor", ctypes.c_double),
-                ("max_iterations", ctypes.c_int32), ("replace_every", ctypes.c_int32),
+                ("warm_gate", ctypes.c_double), ("max_iterations", ctypes.c_int32), ("replace_every", ctypes.c_int32),
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
                 ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32),
                 ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32)]
@@ -51,12 +51,14 @@ class NsrGmresParams(ctypes.Structure):
 class NsrSolveStats(ctypes.Structure):
     _fields_ = [("loop_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double * 8),
                 ("kernel_timed", ctypes.c_int32 * 8), ("launches", ctypes.c_int64),
-                ("graph_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("graph_launches", ctypes.c_int32), ("warm_accepted", ctypes.c_int32),
+                ("warm_rejected", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
     KERNELS = ("fwd_h0", "cols_h0", "inv_h0", "fwd_h1", "cols_h1", "res_h1", "inv_h1")
 
     def as_dict(self):
         return dict(loop_ms=self.loop_ms, launches=int(self.launches), graph_launches=int(self.graph_launches),
+                    warm_accepted=int(self.warm_accepted), warm_rejected=int(self.warm_rejected),
                     kernel_ms={k: self.kernel_ms[i] for i, k in enumerate(self.KERNELS)},
                     kernel_timed={k: int(self.kernel_timed[i]) for i, k in enumerate(self.KERNELS)})
 

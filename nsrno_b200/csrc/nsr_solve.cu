@@ -33,7 +33,9 @@ enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES
 struct __align__(16) SlotState {
   int sys, mode, iters, final_reason;
   int xpar, zero_rhs, restart, force_restart;
-  int breakdowns, pad_b0, pad_b1, pad_b2;   // consecutive restarts forced by a breakdown
+  int breakdowns;   // consecutive restarts forced by a breakdown
+  int x0_off;       // the initial field was rejected: start from zero
+  int pad_b1, pad_b2;
   double bnorm2, rnorm2, resid, r0norm2;
   double freq, angle;
   double2 rho, alpha, omega, beta;
@@ -46,6 +48,7 @@ struct SolveBufs {
   int* arrive;        // [n_slots]
   int* queue;         // next system to start
   int* done;          // systems finished
+  int* warm;          // [2]: initial fields accepted, rejected
   double* partials;   // [n_slots][nb_inv][NSR_NPART]
   float2 *r, *rh, *p, *v, *t, *y, *w;   // [n_slots][n]
   double2* x;         // [n_slots][2][n]
@@ -70,6 +73,7 @@ struct SolveArgs {
   double tol2;
   double shift;
   double restart2;   // squared restart factor
+  double warm_gate2; // squared acceptance bound of an initial field's relative residual (0: none)
   int max_it;
   int replace_every;
   int adjoint;
@@ -202,6 +206,7 @@ __device__ void pop_next(const SolveArgs& A, SlotState& S) {
   if (nxt < A.n_systems) {
     S.sys = nxt;
     S.mode = MODE_INIT;
+    S.x0_off = 0;
     S.freq = A.freq[nxt];
     S.angle = A.angle ? A.angle[nxt] : 0.0;
   } else {
@@ -246,6 +251,16 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
       return;
     }
     const double rel2 = S.rnorm2 / S.bnorm2;
+    const bool used_x0 = A.x0 != nullptr && !S.x0_off;
+    if (used_x0 && A.warm_gate2 > 0.0 && !(rel2 <= A.warm_gate2)) {
+      // The initial field is worse than the gate: discard it and start from zero.
+      S.x0_off = 1;
+      S.xpar ^= 1;
+      atomicAdd(&A.B.warm[1], 1);
+      S.mode = MODE_INIT;
+      return;
+    }
+    if (used_x0) atomicAdd(&A.B.warm[0], 1);
     if (!isfinite(rel2)) { finish_system(A, S, NSR_NONFINITE, rel2); return; }
     if (rel2 < tol2) { finish_system(A, S, NSR_CONVERGED, sqrt(rel2)); return; }
     S.rho = make_double2(S.rnorm2, 0.0);
@@ -530,7 +545,7 @@ __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
   if (mode == MODE_RES || mode == MODE_INIT) {
     const double2* xo = A.B.x + (2LL * slot + S.xpar) * n;
     double2* xn = A.B.x + (2LL * slot + (S.xpar ^ 1)) * n;
-    const float2* x0 = (A.x0 && S.sys >= 0) ? A.x0 + (long long)S.sys * n : nullptr;
+    const float2* x0 = (A.x0 && S.sys >= 0 && !S.x0_off) ? A.x0 + (long long)S.sys * n : nullptr;
     auto P = [&](int i2, int j2) -> double2 {
       if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return make_double2(0.0, 0.0);
       const long long id = (long long)i2 * nx + j2;
@@ -599,6 +614,8 @@ __global__ void k_solve_init(SolveArgs A, int n_slots) {
   if (tid == 0) {
     *A.B.queue = min(A.n_systems, n_slots);
     *A.B.done = 0;
+    A.B.warm[0] = 0;
+    A.B.warm[1] = 0;
   }
 }
 
@@ -627,7 +644,7 @@ static Layout layout(const NsrGrid* g, int n_slots) {
   L.tables = off; off += nsr_align(nsr_prec_table_bytes(g));
   L.slots = off; off += nsr_align(sizeof(SlotState) * n_slots);
   L.arrive = off; off += nsr_align(sizeof(int) * n_slots);
-  L.queue = off; off += nsr_align(sizeof(int) * 2);
+  L.queue = off; off += nsr_align(sizeof(int) * 4);
   L.partials = off; off += nsr_align(sizeof(double) * NSR_NPART * (size_t)L.nb_inv * n_slots);
   L.vec = off; off += 7 * nsr_align(sizeof(float2) * n * n_slots);
   L.x = off; off += nsr_align(sizeof(double2) * n * 2 * n_slots);
@@ -705,6 +722,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     A.B.arrive = (int*)(ws + L.arrive);
     A.B.queue = (int*)(ws + L.queue);
     A.B.done = A.B.queue + 1;
+    A.B.warm = A.B.queue + 2;
     A.B.partials = (double*)(ws + L.partials);
     const size_t vb = nsr_align(sizeof(float2) * n * n_slots);
     float2** vecs[7] = {&A.B.r, &A.B.rh, &A.B.p, &A.B.v, &A.B.t, &A.B.y, &A.B.w};
@@ -724,6 +742,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     A.nb_inv = L.nb_inv;
     A.tol2 = params->tolerance * params->tolerance;
     A.restart2 = params->restart_factor * params->restart_factor;
+    A.warm_gate2 = params->warm_gate > 0.0 ? params->warm_gate * params->warm_gate : 0.0;
     A.shift = params->shift;
     A.max_it = params->max_iterations;
     A.replace_every = params->replace_every;
@@ -833,6 +852,11 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     NSR_TRY(cudaStreamSynchronize(st));
     if (!drained) err = NSR_ERR_INTERNAL;
     if (stats) {
+      int warm_host[2] = {0, 0};
+      NSR_TRY(cudaMemcpyAsync(warm_host, A.B.warm, sizeof(warm_host), cudaMemcpyDeviceToHost, st));
+      NSR_TRY(cudaStreamSynchronize(st));
+      stats->warm_accepted = warm_host[0];
+      stats->warm_rejected = warm_host[1];
       float ms = 0.f;
       NSR_TRY(cudaEventElapsedTime(&ms, ev_loop[0], ev_loop[1]));
       stats->loop_ms = ms;

@@ -146,7 +146,7 @@ _default_ws = Workspace()
 def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tolerance=1e-6,
                   max_iterations=2000, shift=DEFAULT_SHIFT, replace_every=DEFAULT_REPLACE, n_slots=16,
                   adjoint=False, return_fields=False, rx_index=None, graph_iterations=16,
-                  profile_iterations=0, restart_factor=DEFAULT_RESTART, fields_dtype=torch.complex64,
+                  profile_iterations=0, restart_factor=DEFAULT_RESTART, warm_gate=1.0, fields_dtype=torch.complex64,
                   workspace: Workspace | None = None, out: BatchResult | None = None) -> BatchResult:
     """Solve every (frequency, angle) system of a record with batched BiCGSTAB.
 
@@ -195,7 +195,8 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
         raise ValueError("fields_dtype must be complex64 or complex128")
     if out.fields is not None and (out.fields.dtype != fields_dtype or tuple(out.fields.shape) != (S, g.nz, g.nx)):
         raise ValueError("out.fields does not match fields_dtype and the system count")
-    params = _lib.NsrSolveParams(float(tolerance), float(shift), float(restart_factor), int(max_iterations),
+    params = _lib.NsrSolveParams(float(tolerance), float(shift), float(restart_factor), float(warm_gate),
+                                 int(max_iterations),
                                  int(replace_every),
                                  int(n_slots), int(bool(adjoint)), int(graph_iterations), int(profile_iterations),
                                  int(fields_dtype == torch.complex128), 0)

@@ -157,3 +157,20 @@ def test_warm_start_from_solution_needs_no_iterations(cuda):
     w = solve_batched(med, f[:3], th[:3], tolerance=1e-5, x0=r.fields.contiguous())
     assert w.reasons() == ["converged"] * 3
     assert (w.iterations.cpu() == 0).all()
+
+
+def test_warm_start_gate_discards_bad_initial_fields(cuda):
+    """An initial field whose relative residual exceeds the gate (1.0) is dropped:
+    the system then runs exactly like a zero start (config 4's fallback rule)."""
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    cold = solve_batched(med, f[:3], th[:3], tolerance=1e-6)
+    rng = np.random.default_rng(4)
+    noise = torch.as_tensor((rng.standard_normal((3, rec.nz, rec.nx)) * 1e3).astype(np.complex64), device=cuda)
+    bad = solve_batched(med, f[:3], th[:3], tolerance=1e-6, x0=noise)
+    assert bad.extra["stats"]["warm_rejected"] == 3 and bad.extra["stats"]["warm_accepted"] == 0
+    assert torch.equal(bad.iterations, cold.iterations)
+    assert torch.equal(bad.iq, cold.iq)
+    ok = solve_batched(med, f[:3], th[:3], tolerance=1e-6, x0=noise, warm_gate=0.0)
+    assert ok.extra["stats"]["warm_accepted"] == 3 and ok.reasons() == ["converged"] * 3
