@@ -64,6 +64,28 @@ typedef struct NsrGrid {
 } NsrGrid;
 
 /* Krylov parameters of nsr_solve_batched. */
+/* Learned preconditioner of the reference's LearnedPreconditioner
+ * (nsrno/conditioned_wave.py:94-117, learned_apply nsrno/dense_wave.py:150-165)
+ * on the 5-point grid:  M r = outer * IFFT(m * FFT(inner * r)), the complex
+ * conjugate of the reference map (exp(-i omega t) convention) in the units of
+ * the h^2-scaled operator.  `params` is the flat float32 parameter vector in the
+ * reference module's state_dict order: spectral[2][4], log_shift,
+ * context.0.weight[16][5][3][3], context.0.bias[16], context.2.weight[16][16][3][3],
+ * context.2.bias[16], context.4.weight[4][16][3][3], context.4.bias[4]. */
+#define NSR_LEARNED_PARAMS 3645
+
+typedef struct NsrLearned {
+  const float* params;       /* device float[NSR_LEARNED_PARAMS]                */
+  const void* gains;         /* device c64 [n_gain][2][nz][nx] (inner, outer)
+                                from nsr_learned_setup; NULL: spectral
+                                multiplier only (no diagonal gains)            */
+  const int32_t* gain_index; /* device int32 [n_systems]: gain pair of each
+                                system; NULL: system s uses pair s. Checked on
+                                the host (one small copy) before any launch     */
+  int32_t n_gain;            /* gain pairs in `gains`                          */
+  int32_t reserved;
+} NsrLearned;
+
 typedef struct NsrSolveParams {
   double tolerance;          /* relative true residual ||b-Ax||/||b||          */
   double shift;              /* shifted-Laplace preconditioner shift (0.15)    */
@@ -83,6 +105,9 @@ typedef struct NsrSolveParams {
                                 durations are reported in NsrSolveStats          */
   int32_t fields_fp64;       /* 0: fields output is c64; 1: c128 (the FP64 iterate) */
   int32_t reserved;
+  const NsrLearned* learned; /* host pointer; NULL: fixed shifted-Laplace
+                                preconditioner. Otherwise the learned one
+                                (`shift` is then unused)                        */
 } NsrSolveParams;
 
 /* Optional host-side statistics of one nsr_solve_batched call. */
@@ -200,6 +225,7 @@ typedef struct NsrGmresParams {
   int32_t adjoint;           /* 0: A x = b; 1: A^H x = b                       */
   int32_t fields_fp64;       /* fields output c128 when set, else c64          */
   int32_t reserved;
+  const NsrLearned* learned; /* host pointer; NULL: fixed preconditioner      */
 } NsrGmresParams;
 
 /* Restarted right-preconditioned GMRES(m) with two classical Gram-Schmidt
@@ -254,6 +280,64 @@ size_t nsr_dense_workspace_size(const NsrDenseGrid* grid, int32_t n_fields, int3
 int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, double scal_re, double scal_im,
                     int32_t n_fields, int32_t adjoint, int32_t precision, const void* x, void* y,
                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Learned preconditioner: inference -------------------------------- */
+
+/* Bytes of the low-resolution network state of n_freq frequencies. */
+size_t nsr_learned_state_bytes(const NsrGrid* grid, int32_t n_freq);
+
+/* Network and gains of one medium at n_freq frequencies: the 8x pooled context
+ * (log(c/1540)/.06, log(rho/1000)/.08, log1p(alpha), f/6e6-1, 1), three 3x3
+ * convolutions with tanh, bilinear upsampling and the gains
+ * inner = (1 + tanh(m0)/2) exp(-i tanh(m1)/2), outer likewise of m2, m3.
+ * Replaces LearnedPreconditioner.setup (nsrno/conditioned_wave.py:103-117).
+ * c, rho, alpha: float [nz][nx]; state: nsr_learned_state_bytes; gains: c64
+ * [n_freq][2][nz][nx] (NULL: network only). */
+int nsr_learned_setup(const NsrGrid* grid, const float* c, const float* rho, const float* alpha,
+                      const double* freq_hz, int32_t n_freq, const float* params, void* state,
+                      void* gains, void* stream);
+
+/* y = M x (adjoint = 0) or M^H x (adjoint = 1) of the learned preconditioner
+ * for n_systems c64 fields; workspace of nsr_precondition_workspace_size.
+ * Replaces learned_apply (nsrno/dense_wave.py:150-165). */
+int nsr_learned_precondition(const NsrGrid* grid, const NsrLearned* learned, const double* freq_hz,
+                             int32_t n_systems, int32_t adjoint, const float* x, float* y,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Learned preconditioner: training (backward kernels) ---------------- */
+/* Replace the autograd of DenseTrainingModel / differentiable_gmres
+ * (nsrno/train_dense_wave.py:14-21, nsrno/conditioned_wave.py:119-139).
+ * Cotangents follow dL = 2 Re sum conj(G) dz for complex z. */
+
+size_t nsr_learned_backward_workspace_size(const NsrGrid* grid, int32_t n_freq);
+
+/* Gain cotangents g_inner, g_outer (c64 [n_freq][nz][nx], dL/d conj(gain)) ->
+ * map cotangents d_maps (float [n_freq][4][nz/8][nx/8], overwritten). */
+int nsr_learned_map_backward(const NsrGrid* grid, const void* state, int32_t n_freq,
+                             const float* g_inner, const float* g_outer, float* d_maps,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* Map cotangents -> gradients of the convolution weights and biases, ADDED to
+ * d_params[9 .. NSR_LEARNED_PARAMS). */
+int nsr_learned_network_backward(const NsrGrid* grid, const float* params, const void* state,
+                                 int32_t n_freq, const float* d_maps, float* d_params,
+                                 void* workspace, size_t workspace_bytes, void* stream);
+
+size_t nsr_learned_spectral_workspace_size(const NsrGrid* grid, int32_t n_systems);
+
+/* Gradient of the spectral weights and log_shift, ADDED to d_params[0..9), for
+ * z = outer * F^-1(m * F(x)) with x = inner * r and y = conj(outer) * dL/d conj(z)
+ * (c64 [n_systems][nz][nx]). */
+int nsr_learned_spectral_backward(const NsrGrid* grid, const float* params, const double* freq_hz,
+                                  int32_t n_systems, const float* x, const float* y, float* d_params,
+                                  void* workspace, size_t workspace_bytes, void* stream);
+
+/* One Adam step with gradient-norm clipping (clip_norm <= 0: none), in place on
+ * params, m, v (float [n]); writes the unclipped gradient norm to grad_norm
+ * (device float, may be NULL).  The optimiser of nsrno/train_dense_wave.py:37,72-76. */
+int nsr_learned_adam(float* params, const float* grad, float* m, float* v, int32_t n, int32_t step,
+                     double lr, double beta1, double beta2, double eps, double clip_norm,
+                     float* grad_norm, void* stream);
 
 #ifdef __cplusplus
 }

@@ -18,7 +18,12 @@ REASONS = {CONVERGED: "converged", ITERATION_BUDGET: "iteration_budget", BREAKDO
 EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_material", "nsr_apply",
            "nsr_precondition_workspace_size", "nsr_precondition", "nsr_precondition_noalloc", "nsr_plane_wave_rhs",
            "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_gmres_workspace_size", "nsr_gmres_batched",
-           "nsr_grad_accum", "nsr_dense_coef_bytes", "nsr_dense_workspace_size", "nsr_dense_apply")
+           "nsr_grad_accum", "nsr_dense_coef_bytes", "nsr_dense_workspace_size", "nsr_dense_apply",
+           "nsr_learned_state_bytes", "nsr_learned_setup", "nsr_learned_precondition",
+           "nsr_learned_backward_workspace_size", "nsr_learned_map_backward", "nsr_learned_network_backward",
+           "nsr_learned_spectral_workspace_size", "nsr_learned_spectral_backward", "nsr_learned_adam")
+
+LEARNED_PARAMS = 3645
 
 
 class NsrGrid(ctypes.Structure):
@@ -28,12 +33,18 @@ class NsrGrid(ctypes.Structure):
                 ("alpha_power", ctypes.c_double), ("aperture_half_width", ctypes.c_double)]
 
 
+class NsrLearned(ctypes.Structure):
+    _fields_ = [("params", ctypes.c_void_p), ("gains", ctypes.c_void_p), ("gain_index", ctypes.c_void_p),
+                ("n_gain", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class NsrSolveParams(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double), ("restart_factor", ctypes.c_double),
                 ("warm_gate", ctypes.c_double), ("max_iterations", ctypes.c_int32), ("replace_every", ctypes.c_int32),
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
                 ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32),
-                ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("learned", ctypes.POINTER(NsrLearned))]
 
 
 class NsrDenseGrid(ctypes.Structure):
@@ -45,7 +56,8 @@ class NsrGmresParams(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double),
                 ("max_iterations", ctypes.c_int32), ("restart", ctypes.c_int32),
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
-                ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("learned", ctypes.POINTER(NsrLearned))]
 
 
 class NsrSolveStats(ctypes.Structure):
@@ -103,6 +115,19 @@ def load():
     lib.nsr_dense_workspace_size.restype = S
     lib.nsr_dense_workspace_size.argtypes = [DG, I, I]
     lib.nsr_dense_apply.argtypes = [DG, P, D, D, I, I, I, P, P, P, S, P]
+    L = ctypes.POINTER(NsrLearned)
+    lib.nsr_learned_state_bytes.restype = S
+    lib.nsr_learned_state_bytes.argtypes = [G, I]
+    lib.nsr_learned_setup.argtypes = [G, P, P, P, P, I, P, P, P, P]
+    lib.nsr_learned_precondition.argtypes = [G, L, P, I, I, P, P, P, S, P]
+    lib.nsr_learned_backward_workspace_size.restype = S
+    lib.nsr_learned_backward_workspace_size.argtypes = [G, I]
+    lib.nsr_learned_map_backward.argtypes = [G, P, I, P, P, P, P, S, P]
+    lib.nsr_learned_network_backward.argtypes = [G, P, P, I, P, P, P, S, P]
+    lib.nsr_learned_spectral_workspace_size.restype = S
+    lib.nsr_learned_spectral_workspace_size.argtypes = [G, I]
+    lib.nsr_learned_spectral_backward.argtypes = [G, P, P, I, P, P, P, P, S, P]
+    lib.nsr_learned_adam.argtypes = [P, P, P, P, I, I, D, D, D, D, D, P, P]
     for name in EXPORTS:
         getattr(lib, name)
     _lib = lib

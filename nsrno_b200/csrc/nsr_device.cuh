@@ -72,9 +72,42 @@ __device__ __forceinline__ float2 stencil_pts(const Geo& g, const SysScalars& sc
 // ---------------------------------------------------------------------------
 // Column pass on one field w: forward FFT along z, shifted-Laplace multiply in
 // the digit-reversed domain, inverse FFT along z.  Columns [c0, c0+TC) in place.
+// Learned spectral multiplier of the 5-point path (the conjugate map of
+// nsrno/conditioned_wave.py:112-115): with q2 = 4 (s2z + s2x)/(k0 h)^2, the
+// angular term 4 s2x / (4 (s2x + s2z) + h^2) and the basis
+// (1, q2/(1+q2), angular, angular q2/(1+q2)),
+//   m = exp(tanh(mod0)/2 - i tanh(mod1)/2) / (sym + (k0h)^2 (1 + i s)),
+// s = clamp(exp(log_shift), 0.01, 1).  `lp` holds spectral[2][4], log_shift.
+struct LearnedSpec {
+  float sp[8];
+  float shift;
+};
+
+__device__ __forceinline__ LearnedSpec load_learned_spec(const float* __restrict__ lp) {
+  LearnedSpec L;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) L.sp[k] = __ldg(&lp[k]);
+  L.shift = fminf(fmaxf(expf(__ldg(&lp[8])), 0.01f), 1.0f);
+  return L;
+}
+
+__device__ __forceinline__ float2 learned_symbol(const LearnedSpec& L, float s2z, float s2x, float kh2, float h2) {
+  const float q2 = 4.0f * (s2z + s2x) / kh2;
+  const float rq = q2 / (1.0f + q2);
+  const float ang = 4.0f * s2x / (4.0f * (s2x + s2z) + h2);
+  const float mod0 = L.sp[0] + L.sp[1] * rq + L.sp[2] * ang + L.sp[3] * ang * rq;
+  const float mod1 = L.sp[4] + L.sp[5] * rq + L.sp[6] * ang + L.sp[7] * ang * rq;
+  const float mag = expf(0.5f * tanhf(mod0));
+  float sn, cs;
+  sincosf(0.5f * tanhf(mod1), &sn, &cs);
+  const float sym = -4.0f * (s2z + s2x);
+  return divc(make_float2(mag * cs, -mag * sn), make_float2(sym + kh2, kh2 * L.shift));
+}
+
 template <int TC>
 __device__ __forceinline__ void cols_pass(float2* sm, const Geo& g, const PrecTables& tab, float2* __restrict__ ws,
-                                          double freq, double shift, int adjoint, int c0) {
+                                          double freq, double shift, int adjoint, int c0,
+                                          const float* __restrict__ lp = nullptr) {
   const long long n = (long long)g.nz * g.nx;
   const int ncol = min(TC, g.nx - c0);
   for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
@@ -87,13 +120,26 @@ __device__ __forceinline__ void cols_pass(float2* sm, const Geo& g, const PrecTa
   const float kh2 = (float)s.kh2;
   const float inv_n = 1.0f / (float)n;
   const float2 shiftc = make_float2(kh2, (float)(s.kh2 * shift));
-  for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-    const int z = k / TC, c = k - z * TC;
-    if (c < ncol) {
-      const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
-      float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
-      if (adjoint) mul = conjc(mul);
-      sm[k] = sm[k] * mul;
+  if (lp) {
+    const LearnedSpec L = load_learned_spec(lp);
+    const float h2 = (float)(g.h * g.h);
+    for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+      const int z = k / TC, c = k - z * TC;
+      if (c < ncol) {
+        float2 mul = inv_n * learned_symbol(L, tab.s2z[z], tab.s2x[c0 + c], kh2, h2);
+        if (adjoint) mul = conjc(mul);
+        sm[k] = sm[k] * mul;
+      }
+    }
+  } else {
+    for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+      const int z = k / TC, c = k - z * TC;
+      if (c < ncol) {
+        const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
+        float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
+        if (adjoint) mul = conjc(mul);
+        sm[k] = sm[k] * mul;
+      }
     }
   }
   __syncthreads();
@@ -125,3 +171,53 @@ __device__ __forceinline__ void band_inverse_rows(float2* sm, const Geo& g, cons
 
 // Stores `val` for element (l, c) of a row tile in the padded row layout.
 __device__ __forceinline__ int row_slot(int l, int c, int rs, bool pad) { return l * rs + (pad ? c + (c >> 4) : c); }
+
+// Diagonal gains of the learned preconditioner.  Plane 0 of a gain pair is the
+// inner gain (applied before the FFTs), plane 1 the outer one (after them);
+// the adjoint applies the conjugated outer gain first and the conjugated
+// inner gain last (nsrno/dense_wave.py:163-164).
+struct GainPair {
+  const float2* pre;    // multiplies the field before the forward FFT (nullptr: none)
+  const float2* post;   // multiplies it after the inverse FFT (nullptr: none)
+  bool conj;
+};
+
+__device__ __forceinline__ GainPair gain_pair(const float2* gains, int gidx, long long n, int adjoint) {
+  GainPair G;
+  if (!gains) {
+    G.pre = G.post = nullptr;
+    G.conj = false;
+    return G;
+  }
+  const float2* base = gains + 2LL * gidx * n;
+  G.pre = adjoint ? base + n : base;
+  G.post = adjoint ? base : base + n;
+  G.conj = adjoint != 0;
+  return G;
+}
+
+__device__ __forceinline__ float2 gain_mul(const float2* plane, long long idx, bool cj, float2 v) {
+  float2 gv = __ldg(&plane[idx]);
+  if (cj) gv.y = -gv.y;
+  return gv * v;
+}
+
+// After band_inverse_rows: multiply band rows z0-1 .. z0+nb (those inside the
+// grid) by the post gain.
+__device__ __forceinline__ void band_post_gain(float2* sm, const Geo& g, const float2* __restrict__ post, bool cj,
+                                               int z0, int nb) {
+  if (!post) return;
+  const int nx = g.nx;
+  const int rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
+  __syncthreads();
+  for (int rr = 0; rr < nb + 2; ++rr) {
+    const int z = z0 - 1 + rr;
+    if (z < 0 || z >= g.nz) continue;
+    for (int j = threadIdx.x; j < nx; j += blockDim.x) {
+      float2& v = sm[rr * rs + (pad ? j + (j >> 4) : j)];
+      v = gain_mul(post, (long long)z * nx + j, cj, v);
+    }
+  }
+  __syncthreads();
+}

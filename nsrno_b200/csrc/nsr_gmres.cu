@@ -35,7 +35,7 @@ struct __align__(16) GSlot {
   int used;       // Arnoldi steps of the current cycle
   int stop;       // the current cycle ends after step `used`
   int xpar;       // which x buffer holds the iterate
-  int pad;
+  int gidx;       // gain pair of the learned preconditioner
   double bnorm;   // ||b||
   double beta;    // ||r|| at the start of the cycle
   double resid;   // true relative residual at the start of the cycle
@@ -74,6 +74,10 @@ struct GArgs {
   const double* angle;
   const float2* rhs;
   const float2* x0;
+  // Learned preconditioner (all null: the fixed shifted-Laplace one).
+  const float* lp;
+  const float2* gains;
+  const int* gain_index;
 };
 
 __device__ __forceinline__ bool g_active(const GSlot& S, int j) {
@@ -138,11 +142,12 @@ __global__ void __launch_bounds__(256) gk_fwd(GArgs A, int j) {
   float2* vj = A.V + ((long long)slot * (A.m + 1) + j) * n + off;
   const int nx = g.nx, rs = nsr_row_stride(nx);
   const bool pad = nsr_row_padded(nx);
+  const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
   for (int l = 0; l < nr; ++l)
     for (int c = threadIdx.x; c < nx; c += blockDim.x) {
       const float2 v = scale * src[l * nx + c];
       vj[l * nx + c] = v;
-      sm[row_slot(l, c, rs, pad)] = v;
+      sm[row_slot(l, c, rs, pad)] = G.pre ? gain_mul(G.pre, off + l * nx + c, G.conj, v) : v;
     }
   __syncthreads();
   fft_rows<false>(sm, nr, A.tab.px);
@@ -160,7 +165,7 @@ __global__ void __launch_bounds__(512) gk_cols(GArgs A, int j) {
   const bool on = j >= 0 ? g_active(S, j) : (S.sys >= 0 && !S.done && S.used > 0);
   if (!on) return;
   const long long n = (long long)A.g.nz * A.g.nx;
-  cols_pass<TC>(sm, A.g, A.tab, A.W + slot * n, S.freq, A.shift, A.adjoint, blockIdx.x * TC);
+  cols_pass<TC>(sm, A.g, A.tab, A.W + slot * n, S.freq, A.shift, A.adjoint, blockIdx.x * TC, A.lp);
 }
 
 // inv: w = A M^-1 v_j (FP32 stencil on the inverse row FFT of W)
@@ -177,6 +182,7 @@ __global__ void __launch_bounds__(256) gk_inv(GArgs A, int j) {
   const int nx = g.nx, rs = nsr_row_stride(nx);
   const bool pad = nsr_row_padded(nx);
   band_inverse_rows(sm, g, A.tab, A.W + slot * n, z0, nb);
+  band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
   const SysScalars sc = sys_scalars(g, S.freq);
   float2* __restrict__ w = A.w + slot * n;
   const float* ca = A.mat.a32;
@@ -350,11 +356,12 @@ __global__ void __launch_bounds__(256) gk_comb(GArgs A) {
   const long long off = (long long)z0 * g.nx;
   const int nx = g.nx, rs = nsr_row_stride(nx);
   const bool pad = nsr_row_padded(nx);
+  const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
   for (int l = 0; l < nr; ++l)
     for (int c = threadIdx.x; c < nx; c += blockDim.x) {
       float2 acc = make_float2(0.f, 0.f);
       for (int i = 0; i < u; ++i) acc = acc + yc[i] * A.V[((long long)slot * (m + 1) + i) * n + off + l * nx + c];
-      sm[row_slot(l, c, rs, pad)] = acc;
+      sm[row_slot(l, c, rs, pad)] = G.pre ? gain_mul(G.pre, off + l * nx + c, G.conj, acc) : acc;
     }
   __syncthreads();
   fft_rows<false>(sm, nr, A.tab.px);
@@ -377,7 +384,10 @@ __global__ void __launch_bounds__(256) gk_res(GArgs A, int init) {
   const int nb = min(A.tz, g.nz - z0);
   const int nx = g.nx, rs = nsr_row_stride(nx);
   const bool pad = nsr_row_padded(nx);
-  if (!init) band_inverse_rows(sm, g, A.tab, A.W + slot * n, z0, nb);
+  if (!init) {
+    band_inverse_rows(sm, g, A.tab, A.W + slot * n, z0, nb);
+    band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
+  }
   const SysScalars sc = sys_scalars(g, S.freq);
   const double2* xo = A.x + (2LL * slot + S.xpar) * n;
   double2* xn = A.x + (2LL * slot + (S.xpar ^ 1)) * n;
@@ -504,6 +514,7 @@ __global__ void gk_load(GArgs A, int first, int count, const double* freq, const
   memset(&S, 0, sizeof(S));
   if (slot < count) {
     S.sys = first + slot;
+    S.gidx = A.gain_index ? A.gain_index[first + slot] : first + slot;
     S.freq = freq[first + slot];
     S.angle = angle ? angle[first + slot] : 0.0;
   } else {
@@ -589,6 +600,7 @@ extern "C" int nsr_gmres_batched(const NsrGrid* grid, const void* material, cons
   if (m < 1 || m > NSR_GMRES_MAX_M || n_slots <= 0 || n_slots > 65535 || !(params->tolerance > 0) ||
       params->max_iterations <= 0 || !(params->shift >= 0))
     return NSR_ERR_ARGUMENT;
+  if (params->learned && !params->learned->params) return NSR_ERR_ARGUMENT;
   if (n_systems == 0) return 0;
   const GLayout L = g_layout(grid, n_slots, m);
   if (workspace_bytes < L.total) return NSR_ERR_WORKSPACE;
@@ -607,6 +619,8 @@ extern "C" int nsr_gmres_batched(const NsrGrid* grid, const void* material, cons
     NSR_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
     NSR_TRY(cudaEventRecord(ev_in, caller));
     NSR_TRY(cudaStreamWaitEvent(st, ev_in, 0));
+    err = nsr_check_learned(params->learned, n_systems, st);
+    if (err) goto cleanup;
     char* ws = (char*)workspace;
     GArgs A;
     memset(&A, 0, sizeof(A));
@@ -644,6 +658,11 @@ extern "C" int nsr_gmres_batched(const NsrGrid* grid, const void* material, cons
     A.angle = rhs ? nullptr : angle_rad;
     A.rhs = (const float2*)rhs;
     A.x0 = (const float2*)x0;
+    if (params->learned) {
+      A.lp = params->learned->params;
+      A.gains = (const float2*)params->learned->gains;
+      A.gain_index = params->learned->gain_index;
+    }
 
     const int rs = nsr_row_stride(grid->nx);
     const size_t fwd_smem = sizeof(float2) * A.rows * rs;

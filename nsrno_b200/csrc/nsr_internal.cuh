@@ -19,3 +19,4 @@ int nsr_cols_tc(const NsrGrid* g);
 size_t nsr_cols_smem(const NsrGrid* g);
 int nsr_rows_per_cta(const NsrGrid* g);
 
+int nsr_check_learned(const NsrLearned* L, int n_systems, cudaStream_t st);

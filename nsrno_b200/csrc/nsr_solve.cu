@@ -35,7 +35,8 @@ struct __align__(16) SlotState {
   int xpar, zero_rhs, restart, force_restart;
   int breakdowns;   // consecutive restarts forced by a breakdown
   int x0_off;       // the initial field was rejected: start from zero
-  int pad_b1, pad_b2;
+  int gidx;         // gain pair of the learned preconditioner
+  int pad_b2;
   double bnorm2, rnorm2, resid, r0norm2;
   double freq, angle;
   double2 rho, alpha, omega, beta;
@@ -83,6 +84,10 @@ struct SolveArgs {
   int* status;
   void* fields;     // float2 or double2 [S][n]
   int fields_fp64;
+  // Learned preconditioner (all null: the fixed shifted-Laplace one).
+  const float* lp;        // parameters (spectral multiplier)
+  const float2* gains;    // [n_gain][2][n]
+  const int* gain_index;  // [n_systems] (null: system s uses pair s)
 };
 
 // Which slots a launch serves.  The first half of an iteration runs only the
@@ -137,6 +142,8 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   }
   const float2 sv = f2(S.c_sv), rt = f2(S.c_rt), yp = f2(S.c_yp), ys = f2(S.c_ys), pp = f2(S.c_pp), pv = f2(S.c_pv);
   const int nx = g.nx;
+  const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
+  const long long goff = (long long)z0 * g.nx;   // node index of this tile's first element
   const int rs = nsr_row_stride(nx);
   const bool pad = nsr_row_padded(nx);
   float2* __restrict__ rr_ = r;
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
         const float2 pn = rn + pp * pk + pv * vk;
         rr_[k] = rn; pp_[k] = pn; yy_[k] = yn;
         if (restart) rh[k] = rn;
-        sm[l * rs + (pad ? c + (c >> 4) : c)] = pn;
+        sm[l * rs + (pad ? c + (c >> 4) : c)] = G.pre ? gain_mul(G.pre, goff + k, G.conj, pn) : pn;
       }
     }
   } else if (mode == MODE_ITER_B) {
@@ -166,7 +173,8 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
 #pragma unroll 4
       for (int c = threadIdx.x; c < nx; c += blockDim.x) {
         const int k = l * nx + c;
-        sm[l * rs + (pad ? c + (c >> 4) : c)] = rr_[k] + sv * vv_[k];
+        const float2 s1 = rr_[k] + sv * vv_[k];
+        sm[l * rs + (pad ? c + (c >> 4) : c)] = G.pre ? gain_mul(G.pre, goff + k, G.conj, s1) : s1;
       }
     }
   } else {  // MODE_RES: apply the pending update to y, transform y, clear it
@@ -174,7 +182,8 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
       for (int c = threadIdx.x; c < nx; c += blockDim.x) {
         const int k = l * nx + c;
         const float2 s1 = rr_[k] + sv * vv_[k];
-        sm[l * rs + (pad ? c + (c >> 4) : c)] = yy_[k] + yp * pp_[k] + ys * s1;
+        const float2 yn = yy_[k] + yp * pp_[k] + ys * s1;
+        sm[l * rs + (pad ? c + (c >> 4) : c)] = G.pre ? gain_mul(G.pre, goff + k, G.conj, yn) : yn;
         yy_[k] = make_float2(0.f, 0.f);
       }
     }
@@ -198,7 +207,7 @@ __global__ void __launch_bounds__(512) k_cols(SolveArgs A, int half) {
   const int mode = A.B.slots[slot].mode;
   if (!cols_active(mode, half)) return;
   const long long n = (long long)A.g.nz * A.g.nx;
-  cols_pass<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.slots[slot].freq, A.shift, A.adjoint, blockIdx.x * TC);
+  cols_pass<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.slots[slot].freq, A.shift, A.adjoint, blockIdx.x * TC, A.lp);
 }
 
 __device__ void pop_next(const SolveArgs& A, SlotState& S) {
@@ -207,6 +216,7 @@ __device__ void pop_next(const SolveArgs& A, SlotState& S) {
     S.sys = nxt;
     S.mode = MODE_INIT;
     S.x0_off = 0;
+    S.gidx = A.gain_index ? A.gain_index[nxt] : nxt;
     S.freq = A.freq[nxt];
     S.angle = A.angle ? A.angle[nxt] : 0.0;
   } else {
@@ -450,6 +460,7 @@ __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
     }
     __syncthreads();
     fft_rows<true>(sm, nl, A.tab.px);
+    band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
   }
   const SysScalars sc = sys_scalars(g, S.freq);
   const float* __restrict__ ca = A.mat.a32;
@@ -541,6 +552,7 @@ __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
     }
     __syncthreads();
     fft_rows<true>(sm, nl, A.tab.px);
+    band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
   }
   if (mode == MODE_RES || mode == MODE_INIT) {
     const double2* xo = A.B.x + (2LL * slot + S.xpar) * n;
@@ -602,6 +614,7 @@ __global__ void k_solve_init(SolveArgs A, int n_slots) {
     if (s < A.n_systems) {
       st.sys = s;
       st.mode = MODE_INIT;
+      st.gidx = A.gain_index ? A.gain_index[s] : s;
       st.freq = A.freq[s];
       st.angle = A.angle ? A.angle[s] : 0.0;
     } else {
@@ -683,6 +696,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
   if (n_slots <= 0 || n_slots > 65535 || params->max_iterations <= 0 || !(params->tolerance > 0) ||
       !(params->shift >= 0) || params->replace_every < 0 || !(params->restart_factor >= 0) ||
       params->restart_factor >= 1.0) return NSR_ERR_ARGUMENT;
+  if (params->learned && !params->learned->params) return NSR_ERR_ARGUMENT;
   if (n_systems == 0) return 0;
   const Layout L = layout(grid, n_slots);
   if (workspace_bytes < L.total) return NSR_ERR_WORKSPACE;
@@ -711,6 +725,8 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     NSR_TRY(cudaEventCreateWithFlags(&ev_poll[1], cudaEventDisableTiming));
     NSR_TRY(cudaEventRecord(ev_in, caller));
     NSR_TRY(cudaStreamWaitEvent(st, ev_in, 0));
+    err = nsr_check_learned(params->learned, n_systems, st);
+    if (err) goto cleanup;
 
     char* ws = (char*)workspace;
     SolveArgs A;
@@ -753,6 +769,11 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     A.status = status;
     A.fields = fields;
     A.fields_fp64 = params->fields_fp64 ? 1 : 0;
+    if (params->learned) {
+      A.lp = params->learned->params;
+      A.gains = (const float2*)params->learned->gains;
+      A.gain_index = params->learned->gain_index;
+    }
 
     const size_t fwd_smem = sizeof(float2) * A.rows * nsr_row_stride(grid->nx);
     const size_t col_smem = nsr_cols_smem(grid);

@@ -147,12 +147,16 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                   max_iterations=2000, shift=DEFAULT_SHIFT, replace_every=DEFAULT_REPLACE, n_slots=16,
                   adjoint=False, return_fields=False, rx_index=None, graph_iterations=16,
                   profile_iterations=0, restart_factor=DEFAULT_RESTART, warm_gate=1.0, fields_dtype=torch.complex64,
+                  learned=None, gain_index=None,
                   workspace: Workspace | None = None, out: BatchResult | None = None) -> BatchResult:
     """Solve every (frequency, angle) system of a record with batched BiCGSTAB.
 
     ``freqs``/``angles`` are 1-D (one entry per system).  ``rhs`` (complex64
     [S, nz, nx], SI units) replaces the plane-wave source when given.
-    ``x0`` (complex64 [S, nz, nx]) is a warm start.
+    ``x0`` (complex64 [S, nz, nx]) is a warm start.  ``learned`` (a
+    :class:`nsrno_b200.learned.LearnedSetup`) replaces the fixed preconditioner
+    by the learned one; ``gain_index`` (int [S]) picks each system's gain pair
+    (default: its position in ``learned.freqs``).
     """
     lib = _lib.load()
     g = medium.geometry
@@ -200,20 +204,37 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                                  int(replace_every),
                                  int(n_slots), int(bool(adjoint)), int(graph_iterations), int(profile_iterations),
                                  int(fields_dtype == torch.complex128), 0)
+    keep = _learned_params(params, learned, gain_index, freqs)
     stats = _lib.NsrSolveStats()
     _lib.check(lib.nsr_solve_batched(
         ctypes.byref(grid), _ptr(medium.material), _ptr(freqs), _ptr(angles), S,
         _ptr(rhs), _ptr(x0), _ptr(rx_index), n_rx, ctypes.byref(params),
         _ptr(ws), ws.numel(), _ptr(out.iq), _ptr(out.residual), _ptr(out.iterations), _ptr(out.status),
         _ptr(out.fields), ctypes.byref(stats), _stream()))
+    del keep
     out.extra["stats"] = stats.as_dict()
     out.extra["n_slots"] = n_slots
     return out
 
 
+def _learned_params(params, learned, gain_index, freqs):
+    """Attach the learned preconditioner to solver parameters; returns what must stay alive."""
+    if learned is None:
+        return None
+    if gain_index is None:
+        gain_index = learned.index_of(freqs)
+    gain_index = torch.as_tensor(gain_index, dtype=torch.int32, device=freqs.device).reshape(-1).contiguous()
+    if gain_index.numel() != freqs.numel():
+        raise ValueError("gain_index needs one entry per system")
+    struct = learned.struct(gain_index)
+    params.learned = ctypes.pointer(struct)
+    return (struct, gain_index)
+
+
 def gmres_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tolerance=1e-6, max_iterations=2560,
                   restart=32, shift=DEFAULT_SHIFT, n_slots=16, adjoint=False, return_fields=False,
-                  fields_dtype=torch.complex64, rx_index=None, workspace: Workspace | None = None) -> BatchResult:
+                  fields_dtype=torch.complex64, rx_index=None, learned=None, gain_index=None,
+                  workspace: Workspace | None = None) -> BatchResult:
     """Restarted GMRES(restart) for every system (nsrno/wave_solver.py:9-36 on the device).
 
     Same inputs and outputs as :func:`solve_batched`; ``iterations`` counts
@@ -257,6 +278,7 @@ def gmres_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                       fields=torch.empty((S, g.nz, g.nx), dtype=fields_dtype, device=dev) if return_fields else None)
     params = _lib.NsrGmresParams(float(tolerance), float(shift), int(max_iterations), int(restart), int(n_slots),
                                  int(bool(adjoint)), int(fields_dtype == torch.complex128), 0)
+    keep = _learned_params(params, learned, gain_index, freqs)  # noqa: F841 (kept alive for the call)
     _lib.check(lib.nsr_gmres_batched(
         ctypes.byref(grid), _ptr(medium.material), _ptr(freqs), _ptr(angles), S, _ptr(rhs), _ptr(x0),
         _ptr(rx_index), n_rx, ctypes.byref(params), _ptr(ws), ws.numel(), _ptr(out.iq), _ptr(out.residual),
