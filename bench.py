@@ -2,11 +2,15 @@
 
 Workload: the synthetic breast record, 1024 (x) x 768 (z) nodes at 0.05 mm,
 11 plane-wave angles x 294 frequency bins (4.015-8.896 MHz) = 3234 systems,
-BiCGSTAB with the FFT shifted-Laplace preconditioner to a true relative residual
-of 1e-6.  One step solves a batch of SYSTEMS_PER_STEP systems (4 bins x 11
-angles, bins spread over the band by a fixed stride permutation) through the
-resident-slot queue.  Under torchrun every rank takes different bins (weak
-scaling, no collective on the data path).
+BiCGSTAB to a true relative residual of 1e-6.  One step solves a batch of
+SYSTEMS_PER_STEP systems (4 bins x 11 angles, bins spread over the band by a
+fixed stride permutation) through the resident-slot queue.  Under torchrun
+every rank takes different bins (weak scaling, no collective on the data path).
+
+Two arms run on the same GPU and the same steps: the headline "learned-init"
+arm (the trained learned preconditioner: its network set-up for the step's
+bins is inside the timed region) and the "plain Krylov" arm (the fixed
+shifted-Laplace preconditioner, shift 0.15), reported under ``plain_krylov``.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -48,7 +52,11 @@ FALLBACK_HBM_GBS = 6650.0
 # and writes w; inv h1 reads w, rhat, r, v and writes t.  res h1 (the FP64
 # true residual) has no work in the timed iterations of a fresh batch.
 KERNEL_BYTES = {"fwd_h0": 72, "cols_h0": 16, "inv_h0": 24, "fwd_h1": 24, "cols_h1": 16, "res_h1": 0, "inv_h1": 40}
+# The learned preconditioner adds one complex64 gain read per node to every
+# fwd launch (inner gain) and to every inv launch (outer gain).
+LEARNED_BYTES = {k: v + (8 if k.startswith(("fwd", "inv")) else 0) for k, v in KERNEL_BYTES.items()}
 COEF_BYTES = {"inv_h0": 12, "inv_h1": 12}
+LEARNED_SETUP_LAUNCHES = 5     # pool, three convolutions, gains
 
 
 def parse():
@@ -59,6 +67,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-sample-bins", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true", help="skip the plain-Krylov comparison arm")
     return p.parse_args()
 
 
@@ -228,6 +237,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     from nsrno_b200 import Geometry, Medium, Workspace, _lib, solve_batched
+    from nsrno_b200.learned import LearnedPreconditioner
     from nsrno_b200.media import breast_record
 
     rank, world, local = dist_env()
@@ -238,62 +248,86 @@ def run_ours(args):
     rec = breast_record()
     geo = Geometry.from_record(rec)
     med = Medium(geo, rec.c, rec.rho, rec.alpha, device=dev)
+    net = LearnedPreconditioner.load(device=dev)
     ws = Workspace()
 
-    def one_step(step, profile=0):
+    def one_step(step, learned, medium=med, profile=0, host=False):
         f, a = step_systems(rec, step, rank, world)
-        return solve_batched(med, f, a, tolerance=TOL, max_iterations=MAX_ITERS, n_slots=N_SLOTS,
-                             profile_iterations=profile, workspace=ws)
+        if host:
+            f = torch.from_numpy(f).pin_memory().to(dev, non_blocking=True)
+            a = torch.from_numpy(a).pin_memory().to(dev, non_blocking=True)
+        setup = None
+        if learned:
+            setup = net.setup(medium, torch.unique(torch.as_tensor(f, device=dev)))
+        return solve_batched(medium, f, a, tolerance=TOL, max_iterations=MAX_ITERS, n_slots=N_SLOTS,
+                             profile_iterations=profile, workspace=ws, learned=setup)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    for w in range(args.warmup):
-        one_step(-(w + 1))
-    barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
     stream = torch.cuda.current_stream()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    results = []
-    t0.record(stream)
-    for k in range(args.steps):
-        results.append(one_step(k, profile=PROFILE_ITERS))
-    t1.record(stream)
-    barrier()
-    clock_info = clocks.stop()
-    ms = t0.elapsed_time(t1)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t)
-    solves = SYSTEMS_PER_STEP * args.steps * world
-    value = solves / (ms_max / 1e3)
-    status = torch.cat([r.status for r in results]).cpu().numpy()
-    iters = torch.cat([r.iterations for r in results]).cpu().numpy()
-    resid = torch.cat([r.residual for r in results]).cpu().numpy()
-    converged = int((status == _lib.CONVERGED).sum())
 
-    # per-kernel durations measured by events between launches (first iterations of every step)
-    kms = {k: float(np.mean([r.extra["stats"]["kernel_ms"][k] for r in results])) for k in KERNEL_BYTES}
-    launches = int(sum(r.extra["stats"]["launches"] for r in results))
+    def timed(learned, sample_clocks=False):
+        for w in range(args.warmup):
+            one_step(-(w + 1), learned)
+        barrier()
+        clocks = ClockSampler(local) if sample_clocks else None
+        if clocks:
+            clocks.start()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        results = []
+        t0.record(stream)
+        for k in range(args.steps):
+            results.append(one_step(k, learned, profile=PROFILE_ITERS))
+        t1.record(stream)
+        barrier()
+        clock_info = clocks.stop() if clocks else None
+        ms_t = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        return float(ms_t), results, clock_info
+
     n = rec.nz * rec.nx
     slots = min(N_SLOTS, SYSTEMS_PER_STEP)
-    dominant = max(kms, key=kms.get)
-    alg_bytes = {k: n * (KERNEL_BYTES[k] * slots + COEF_BYTES.get(k, 0)) for k in KERNEL_BYTES}
     peak, peak_kind = peak_hbm()
-    achieved = alg_bytes[dominant] / (kms[dominant] / 1e3) / 1e9
-    iter_ms = sum(kms.values())
-    iter_bytes = sum(alg_bytes.values())
+    solves = SYSTEMS_PER_STEP * args.steps * world
+
+    def summarise(ms_max, results, per_node):
+        status = torch.cat([r.status for r in results]).cpu().numpy()
+        iters = torch.cat([r.iterations for r in results]).cpu().numpy()
+        resid = torch.cat([r.residual for r in results]).cpu().numpy()
+        # per-kernel durations measured by events between launches (first iterations of every step)
+        kms = {k: float(np.mean([r.extra["stats"]["kernel_ms"][k] for r in results])) for k in per_node}
+        alg = {k: n * (per_node[k] * slots + COEF_BYTES.get(k, 0)) for k in per_node}
+        dominant = max(kms, key=kms.get)
+        iter_ms = sum(kms.values())
+        return dict(value=solves / (ms_max / 1e3), ms_per_step=ms_max / max(1, args.steps), kms=kms, alg=alg,
+                    dominant=dominant, achieved=alg[dominant] / (kms[dominant] / 1e3) / 1e9,
+                    iteration_achieved=sum(alg.values()) / (iter_ms / 1e3) / 1e9,
+                    launches=int(sum(r.extra["stats"]["launches"] for r in results)),
+                    solves={"total": int(len(status)), "converged": int((status == _lib.CONVERGED).sum()),
+                            "iterations_mean": float(iters.mean()), "iterations_max": int(iters.max()),
+                            "residual_max": float(resid.max())})
+
+    ms_l, res_l, clock_info = timed(True, sample_clocks=True)
+    L = summarise(ms_l, res_l, LEARNED_BYTES)
+    P = None
+    if not args.no_plain:
+        ms_p, res_p, _ = timed(False)
+        P = summarise(ms_p, res_p, KERNEL_BYTES)
+    value = L["value"]
+    dominant = L["dominant"]
+    achieved = L["achieved"]
+    launches = L["launches"] + LEARNED_SETUP_LAUNCHES * args.steps
     traffic_per_node, traffic_kernel = profiled_traffic()
     traffic = None
     if traffic_per_node is not None and traffic_kernel == dominant:
         traffic = traffic_per_node * n * slots
 
-    # end to end through the public API with host buffers
+    # end to end through the public API with host buffers (learned arm)
     e2e_value = None
     h2d = d2h = 0
     if args.steps > 0:
@@ -305,15 +339,11 @@ def run_ours(args):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for k in range(args.steps):
-            f, a = step_systems(rec, k, rank, world)
-            fh = torch.from_numpy(f).pin_memory()
-            ah = torch.from_numpy(a).pin_memory()
             m2 = Medium(geo, host_c.to(dev, non_blocking=True), host_r.to(dev, non_blocking=True),
                         host_a.to(dev, non_blocking=True), device=dev)
-            r = solve_batched(m2, fh.to(dev, non_blocking=True), ah.to(dev, non_blocking=True), tolerance=TOL,
-                              max_iterations=MAX_ITERS, n_slots=N_SLOTS, workspace=ws)
+            r = one_step(k, True, medium=m2, host=True)
             out = (r.iq.cpu(), r.residual.cpu(), r.status.cpu(), r.iterations.cpu())
-            h2d = 3 * n * 4 + 2 * f.nbytes
+            h2d = 3 * n * 4 + 2 * SYSTEMS_PER_STEP * 8
             d2h = sum(t.numel() * t.element_size() for t in out)
         e1.record(stream)
         barrier()
@@ -332,11 +362,12 @@ def run_ours(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / max(1, args.steps), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": L["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64/f64", "data": "synthetic",
             "config": {"workload": "breast record 1024x768 nodes dx=0.05mm, 11 angles x 294 bins "
-                                   "(3234 systems); BiCGSTAB + FFT shifted-Laplace (shift 0.15) to true "
-                                   "rel-res 1e-6; plain Krylov (zero initial field)",
+                                   "(3234 systems); BiCGSTAB to true rel-res 1e-6 with the trained learned "
+                                   "preconditioner (network set-up of each step's bins timed); plain Krylov "
+                                   "(fixed shifted-Laplace, shift 0.15) under plain_krylov",
                        "systems_per_step": SYSTEMS_PER_STEP, "n_slots": N_SLOTS, "grid_zx": [rec.nz, rec.nx],
                        "l2": f"inputs larger than L2: {slots * n * 88 / 1e9:.2f} GB resident Krylov state per GPU",
                        "parallelism": f"frequency-sharded x{world}"},
@@ -344,14 +375,17 @@ def run_ours(args):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                         "iteration_achieved": iter_bytes / (iter_ms / 1e3) / 1e9,
-                         "iteration_frac": iter_bytes / (iter_ms / 1e3) / 1e9 / peak,
-                         "kernel_ms": kms},
+                         "iteration_achieved": L["iteration_achieved"],
+                         "iteration_frac": L["iteration_achieved"] / peak,
+                         "kernel_ms": L["kms"]},
             "cpu_baseline": cpu,
             "clocks": clock_info,
-            "solves": {"total": int(len(status)), "converged": converged,
-                       "iterations_mean": float(iters.mean()), "iterations_max": int(iters.max()),
-                       "residual_max": float(resid.max())},
+            "solves": L["solves"],
+            "plain_krylov": None if P is None else {
+                "value": P["value"], "unit": UNIT, "ms_per_step": P["ms_per_step"], "solves": P["solves"],
+                "learned_speedup": value / P["value"],
+                "roofline": {"kernel": P["dominant"], "achieved": P["achieved"], "frac": P["achieved"] / peak,
+                             "iteration_frac": P["iteration_achieved"] / peak, "kernel_ms": P["kms"]}},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -112,18 +112,23 @@ def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=Fals
     """Solve ``A x = rhs`` (or ``A^H x = rhs``) for a batch of angles sharing one operator.
 
     ``rhs`` is ``[A, nz, nx]`` complex (SI units).  ``method`` is ``'gmres'``
-    (restart 24, at most ``max_cycles`` cycles, nsrno/dense_wave.py:217-220) or
-    ``'bicgstab'``, whose unconverged angles fall back to GMRES as in
-    nsrno/dense_wave.py:210-216.  The angle batch shares one frequency like the
-    reference; every angle is its own Krylov system here and
-    ``max_angle_residual`` is the largest of them.  ``residual`` is the
-    combined ``||R|| / ||B||`` over all angles, as the reference measures it
-    (nsrno/dense_wave.py:221-225).  ``preconditioner``, ``warm_steps`` and
-    ``mixed`` are accepted for signature compatibility: the solve always runs
-    FP32 Krylov vectors against an FP64 true residual.
+    (restart 24, at most ``max_cycles`` cycles, nsrno/dense_wave.py:217-220),
+    ``'gmres_learned'`` (the same with the learned preconditioner) or
+    ``'bicgstab'``, whose unconverged angles fall back to GMRES with the fixed
+    preconditioner as in nsrno/dense_wave.py:205-216.  With a
+    ``preconditioner`` (:class:`~nsrno_b200.learned.LearnedPreconditioner`),
+    as in nsrno/dense_wave.py:197-208: a forward solve without ``initial``
+    starts from one ``warm_steps``-step GMRES cycle with the learned
+    preconditioner, and BiCGSTAB uses the learned preconditioner throughout.
+    The angle batch shares one frequency like the reference; every angle is
+    its own Krylov system here and ``max_angle_residual`` is the largest of
+    them.  ``residual`` is the combined ``||R|| / ||B||`` over all angles, as
+    the reference measures it (nsrno/dense_wave.py:221-225).  ``mixed`` is
+    accepted for signature compatibility: the solve always runs FP32 Krylov
+    vectors against an FP64 true residual.
     """
-    if method not in ("gmres", "bicgstab"):
-        raise ValueError("method must be 'gmres' or 'bicgstab'")
+    if method not in ("gmres", "bicgstab", "gmres_learned"):
+        raise ValueError("method must be 'gmres', 'gmres_learned' or 'bicgstab'")
     started = time.perf_counter()
     med = system.medium
     g = med.geometry
@@ -139,9 +144,16 @@ def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=Fals
     if max_iterations is None:
         max_iterations = max_cycles * 24
     freqs = [system.frequency] * A
+    setup = preconditioner.setup(med, [system.frequency]) if preconditioner is not None else None
+    used_warm = 0
+    if setup is not None and warm_steps and not adjoint and x0 is None:
+        from .learned import warm_start
+        x0, _ = warm_start(med, setup, freqs, rhs=b, steps=int(warm_steps), n_slots=A)
+        used_warm = int(warm_steps)
     if method == "bicgstab":
         res = solve_batched(med, freqs, rhs=b, x0=x0, tolerance=tolerance, max_iterations=max_iterations,
-                            adjoint=adjoint, return_fields=True, fields_dtype=torch.complex128, n_slots=A)
+                            adjoint=adjoint, return_fields=True, fields_dtype=torch.complex128, n_slots=A,
+                            learned=setup)
         bad = [k for k, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
         if bad:
             # Fall back to GMRES for the angles BiCGSTAB did not converge.
@@ -155,7 +167,7 @@ def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=Fals
     else:
         res = gmres_batched(med, freqs, rhs=b, x0=x0, tolerance=tolerance, max_iterations=max_iterations,
                             restart=24, adjoint=adjoint, return_fields=True, fields_dtype=torch.complex128,
-                            n_slots=A)
+                            n_slots=A, learned=setup if method == "gmres_learned" else None)
     bn = torch.linalg.vector_norm(rhs.reshape(A, -1).to(torch.complex128), dim=1).to(res.residual.device)
     combined = float(torch.sqrt((res.residual.square() * bn.square()).sum() / bn.square().sum().clamp_min(1e-300)))
     statuses = [int(s) for s in res.status.cpu()]
@@ -163,7 +175,7 @@ def solve_system(system: HelmholtzSystem, rhs, preconditioner=None, adjoint=Fals
     x = res.fields.to(torch.complex128)
     if squeeze:
         x = x[0]
-    steps = int(res.iterations.sum()) * (2 if method == "bicgstab" else 1)
+    steps = int(res.iterations.sum()) * (2 if method == "bicgstab" else 1) + used_warm * A
     return x, {"reason": reason, "steps": steps, "residual": combined,
                "max_angle_residual": float(res.residual.max()), "seconds": time.perf_counter() - started,
                "dtype": "complex64 Krylov / FP64 residual", "method": method,
@@ -186,12 +198,13 @@ class ImplicitChannels(torch.autograd.Function):
     """Converged channels with an implicit adjoint (nsrno/dense_wave.py:227-256)."""
 
     @staticmethod
-    def forward(ctx, medium, alpha, data, frequency_hz, angles, tolerance, max_iterations):
+    def forward(ctx, medium, alpha, data, frequency_hz, angles, tolerance, max_iterations, preconditioner=None):
         g = data.geometry
         med = Medium(g, medium[0].detach(), medium[1].detach(), alpha.detach(), device=medium.device)
         th = [data.angles[a] for a in angles]
+        setup = preconditioner.setup(med, [frequency_hz]) if preconditioner is not None else None
         res = solve_batched(med, [frequency_hz] * len(th), th, tolerance=tolerance, max_iterations=max_iterations,
-                            return_fields=True, fields_dtype=torch.complex128, n_slots=len(th))
+                            return_fields=True, fields_dtype=torch.complex128, n_slots=len(th), learned=setup)
         bad = [i for i, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
         if bad:
             raise RuntimeError("Forward failed to converge: " + str({"reasons": res.reasons(),
@@ -199,6 +212,7 @@ class ImplicitChannels(torch.autograd.Function):
         resp = data.channel_response(frequency_hz)
         ctx.data, ctx.frequency, ctx.angles, ctx.tolerance, ctx.max_iterations = data, frequency_hz, th, tolerance, max_iterations
         ctx.med = med
+        ctx.setup = setup
         ctx.resp = resp
         ctx.save_for_backward(medium, res.fields)
         out = res.iq * resp
@@ -216,35 +230,52 @@ class ImplicitChannels(torch.autograd.Function):
             rhs[:, g.face, rx] = (gradient * ctx.resp).to(torch.complex64)
             res = solve_batched(med, [ctx.frequency] * A, rhs=rhs, tolerance=ctx.tolerance,
                                 max_iterations=ctx.max_iterations, adjoint=True, return_fields=True,
-                                fields_dtype=torch.complex128, n_slots=A)
+                                fields_dtype=torch.complex128, n_slots=A, learned=ctx.setup)
             bad = [i for i, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
             if bad:
                 raise RuntimeError("Adjoint failed to converge: " + str({"reasons": res.reasons(),
                                                                           "residual": res.residual.tolist()}))
             g_logc, g_logrho = grad_accum(med, [ctx.frequency] * A, u, res.fields)
             grad = torch.stack((g_logc / med.c.double(), g_logrho / med.rho.double())).to(medium.dtype)
-        return grad, None, None, None, None, None, None
+        return grad, None, None, None, None, None, None, None
 
 
-def implicit_channels(medium, alpha, data, frequency_hz, angles, tolerance=1e-5, max_iterations=4000):
-    """Differentiable converged receiver channels ``[A, n_rx]`` (complex128)."""
-    return ImplicitChannels.apply(medium, alpha, data, frequency_hz, list(angles), tolerance, max_iterations)
+def implicit_channels(medium, alpha, data, frequency_hz, angles, tolerance=1e-5, max_iterations=4000,
+                      preconditioner=None):
+    """Differentiable converged receiver channels ``[A, n_rx]`` (complex128).
+
+    With a ``preconditioner`` (:class:`~nsrno_b200.learned.LearnedPreconditioner`)
+    the forward and adjoint solves use the learned preconditioner (its adjoint
+    for the adjoint solve), as ``ImplicitChannels`` passes its network to
+    ``solve_system`` (nsrno/dense_wave.py:232-249)."""
+    return ImplicitChannels.apply(medium, alpha, data, frequency_hz, list(angles), tolerance, max_iterations,
+                                  preconditioner)
 
 
 class HelmholtzSurrogate(torch.nn.Module):
     """Drop-in for ``DenseSurrogate`` (nsrno/dense_surrogate.py:9-36) on a synthetic record."""
 
-    def __init__(self, geometry: Geometry, angles_deg, bins=None, response=True, device="cuda"):
+    def __init__(self, geometry: Geometry, angles_deg, bins=None, response=True, device="cuda",
+                 preconditioner="trained"):
+        """``preconditioner``: ``"trained"`` loads the committed learned
+        preconditioner (the reference surrogate loads its trained network,
+        nsrno/dense_surrogate.py:11-17), ``None`` uses the fixed one, or pass a
+        :class:`~nsrno_b200.learned.LearnedPreconditioner`."""
         super().__init__()
         self.data = AcquisitionData(geometry, angles_deg, response=response)
         self.bins = list(range(241, 535)) if bins is None else list(bins)
         self.device = torch.device(device)
+        if isinstance(preconditioner, str):
+            from .learned import LearnedPreconditioner
+            preconditioner = LearnedPreconditioner.load(device=self.device)
+        self.preconditioner = preconditioner
 
     def forward(self, medium, alpha, frequency_bin, angles=None, tolerance=1e-5):
         if frequency_bin not in self.bins:
             raise ValueError("Frequency outside cached dense band")
         angles = list(range(len(self.data.angles))) if angles is None else list(angles)
-        return implicit_channels(medium, alpha, self.data, bin_frequency(frequency_bin), angles, tolerance)
+        return implicit_channels(medium, alpha, self.data, bin_frequency(frequency_bin), angles, tolerance,
+                                 preconditioner=self.preconditioner)
 
     @torch.no_grad()
     def truncated(self, medium, alpha, frequency_bin, angles=None, iterations=32):
@@ -256,7 +287,9 @@ class HelmholtzSurrogate(torch.nn.Module):
         med = Medium(g, medium[0], medium[1], alpha, device=medium.device)
         f = bin_frequency(frequency_bin)
         th = [self.data.angles[a] for a in angles]
-        res = solve_batched(med, [f] * len(th), th, tolerance=1e-30, max_iterations=iterations, n_slots=len(th))
+        setup = self.preconditioner.setup(med, [f]) if self.preconditioner is not None else None
+        res = solve_batched(med, [f] * len(th), th, tolerance=1e-30, max_iterations=iterations, n_slots=len(th),
+                            learned=setup)
         resp = self.data.channel_response(f)
         rel = float(res.residual.max())
         return (res.iq * resp).to(torch.complex128), rel

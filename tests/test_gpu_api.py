@@ -72,3 +72,51 @@ def test_surrogate_forward_backward_and_truncated(cuda):
         from nsrno_b200 import AcquisitionData, implicit_channels
         implicit_channels(medium, alpha, AcquisitionData(geo, np.rad2deg(rec.angles), response=False),
                           bin_frequency(60), [0], tolerance=1e-12, max_iterations=2)
+
+
+def small_breast(dev):
+    from nsrno_b200 import Geometry, Medium
+    from nsrno_b200.media import breast_record
+    rec = breast_record(seed=31, nz=128, nx=192, n_pml=16, n_rx=40, rx_pitch=4, n_angles=3)
+    return rec, Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=dev)
+
+
+@pytest.mark.parametrize("method", ["bicgstab", "gmres_learned"])
+def test_solve_system_with_learned_preconditioner(cuda, method):
+    """The learned preconditioner with the reference's 8-step warm start
+    (nsrno/dense_wave.py:197-208): same solution as SuperLU, warm steps counted."""
+    from nsrno_b200 import HelmholtzSystem, LearnedPreconditioner, plane_wave_rhs, solve_system
+    rec, med = small_breast(cuda)
+    f = float(rec.frequencies[200])
+    rhs = plane_wave_rhs(med, [f] * 3, rec.angles)
+    net = LearnedPreconditioner.load(device=cuda)
+    x, info = solve_system(HelmholtzSystem(med, f), rhs, preconditioner=net, tolerance=1e-7, method=method,
+                           warm_steps=8)
+    assert info["reason"] == "converged" and info["max_angle_residual"] < 1e-7
+    assert info["steps"] >= 3 * 8
+    spec = spec_of(rec)
+    a, b, t = med.coef64.cpu().numpy()
+    A = H.operator_planes(spec, a, b, t, f)
+    for k in range(3):
+        u = H.solve_lu(A, H.plane_wave_rhs(spec, f, rec.angles[k]))
+        assert rel(x[k].cpu().numpy().ravel(), u) < 1e-5
+
+
+def test_learned_and_fixed_gradients_agree(cuda):
+    """The implicit gradient does not depend on the preconditioner (forward and
+    adjoint both converged): learned vs fixed on a breast-like record."""
+    from nsrno_b200 import AcquisitionData, Geometry, LearnedPreconditioner, implicit_channels
+    rec, med = small_breast(cuda)
+    geo = Geometry.from_record(rec)
+    data = AcquisitionData(geo, np.rad2deg(rec.angles), response=False)
+    f = float(rec.frequencies[120])
+    alpha = torch.as_tensor(rec.alpha.astype(np.float64), device=cuda)
+    grads, outs = [], []
+    for pre in (None, LearnedPreconditioner.load(device=cuda)):
+        medium = torch.as_tensor(np.stack((rec.c, rec.rho)).astype(np.float64), device=cuda).requires_grad_(True)
+        out = implicit_channels(medium, alpha, data, f, [0, 1, 2], tolerance=1e-9, preconditioner=pre)
+        (out.abs().square().sum()).backward()
+        grads.append(medium.grad.cpu().numpy())
+        outs.append(out.detach().cpu().numpy())
+    assert rel(outs[1], outs[0]) < 1e-6
+    assert rel(grads[1], grads[0]) < 1e-5
