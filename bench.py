@@ -157,11 +157,12 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per launch and resident system of the dominant kernel from the committed ncu summary."""
+def profiled_traffic(arm="learned"):
+    """DRAM bytes per node and resident system of the dominant kernel of one arm, from the committed ncu summaries."""
     for path in sorted((ROOT / "profiles").glob("*.md")):
-        m = re.search(r"traffic_bytes_per_node_per_system:\s*([0-9.eE+-]+)\s*kernel:\s*(\w+)", path.read_text())
-        if m:
+        m = re.search(r"traffic_bytes_per_node_per_system:\s*([0-9.eE+-]+)\s*kernel:\s*(\w+)\s*arm:\s*(\w+)",
+                      path.read_text())
+        if m and m.group(3) == arm:
             return float(m.group(1)), m.group(2)
     return None, None
 
@@ -322,10 +323,15 @@ def run_ours(args):
     dominant = L["dominant"]
     achieved = L["achieved"]
     launches = L["launches"] + LEARNED_SETUP_LAUNCHES * args.steps
-    traffic_per_node, traffic_kernel = profiled_traffic()
+    traffic_per_node, traffic_kernel = profiled_traffic("learned")
     traffic = None
     if traffic_per_node is not None and traffic_kernel == dominant:
         traffic = traffic_per_node * n * slots
+    plain_traffic = None
+    if P is not None:
+        tp, tk = profiled_traffic("plain")
+        if tp is not None and tk == P["dominant"]:
+            plain_traffic = tp * n * slots
 
     # end to end through the public API with host buffers (learned arm)
     e2e_value = None
@@ -385,7 +391,8 @@ def run_ours(args):
                 "value": P["value"], "unit": UNIT, "ms_per_step": P["ms_per_step"], "solves": P["solves"],
                 "learned_speedup": value / P["value"],
                 "roofline": {"kernel": P["dominant"], "achieved": P["achieved"], "frac": P["achieved"] / peak,
-                             "iteration_frac": P["iteration_achieved"] / peak, "kernel_ms": P["kms"]}},
+                             "iteration_frac": P["iteration_achieved"] / peak, "kernel_ms": P["kms"],
+                             "traffic": plain_traffic}},
         }
         print(json.dumps(line), flush=True)
     if world > 1:
