@@ -281,6 +281,16 @@ int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, double scal_re
                     int32_t n_fields, int32_t adjoint, int32_t precision, const void* x, void* y,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* Tangent (Born) right-hand side rhs = -dA[dm] u of n_systems background
+ * fields u for the material direction dm = (dlogc, dlogrho) (double [nz][nx],
+ * shared by all systems), in SI units like the solver's rhs: solving
+ * A du = rhs gives the tangent field of the Gauss-Newton Hessian-vector
+ * product.  precision 0: u, rhs c64; 1: c128.  Replaces the perturbation
+ * assembly of Solver.born_data (theranostic/wave.py:280-329). */
+int nsr_tangent_rhs(const NsrGrid* grid, const void* coef, const double* freq_hz, int32_t n_systems,
+                    int32_t precision, const void* u, const double* dlogc, const double* dlogrho,
+                    void* rhs, void* stream);
+
 /* ---- Learned preconditioner: inference -------------------------------- */
 
 /* Bytes of the low-resolution network state of n_freq frequencies. */

@@ -21,7 +21,8 @@ EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_m
            "nsr_grad_accum", "nsr_dense_coef_bytes", "nsr_dense_workspace_size", "nsr_dense_apply",
            "nsr_learned_state_bytes", "nsr_learned_setup", "nsr_learned_precondition",
            "nsr_learned_backward_workspace_size", "nsr_learned_map_backward", "nsr_learned_network_backward",
-           "nsr_learned_spectral_workspace_size", "nsr_learned_spectral_backward", "nsr_learned_adam")
+           "nsr_learned_spectral_workspace_size", "nsr_learned_spectral_backward", "nsr_learned_adam",
+           "nsr_tangent_rhs")
 
 LEARNED_PARAMS = 3645
 
@@ -105,6 +106,7 @@ def load():
     lib.nsr_solve_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrSolveParams),
                                       P, S, P, P, P, P, P, ctypes.POINTER(NsrSolveStats), P]
     lib.nsr_grad_accum.argtypes = [G, P, P, I, I, P, P, P, P, P]
+    lib.nsr_tangent_rhs.argtypes = [G, P, P, I, I, P, P, P, P, P]
     lib.nsr_gmres_workspace_size.restype = S
     lib.nsr_gmres_workspace_size.argtypes = [G, I, I]
     lib.nsr_gmres_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrGmresParams),

@@ -433,3 +433,72 @@ extern "C" int nsr_grad_accum(const NsrGrid* grid, const void* coef, const doubl
                                          (const double2*)lam, g_logc, g_logrho);
   return last_error();
 }
+
+// ---------------------------------------------------------------------------
+// Tangent right-hand side -dA[dm] u (the Born perturbation of
+// theranostic/wave.py:280-329 for a direction dm = (dlog c, dlog rho)).
+// The flux part is the stencil evaluated with a' = -a dlogrho and zero ghost
+// contrast (the fluxes are linear in a); the mass part is
+// -2 k0^2 sx sz b (1+ie) dlogc - k0^2 sx sz b (1+ie)^2 dlogrho.  Output in SI
+// units, the units of the solver's right-hand side.
+// ---------------------------------------------------------------------------
+template <typename CT>
+__global__ void k_tangent(Geo g, const void* __restrict__ mat, const double* __restrict__ freq,
+                          const CT* __restrict__ u, const double* __restrict__ dlogc,
+                          const double* __restrict__ dlogrho, CT* __restrict__ rhs) {
+  const long long n = (long long)g.nz * g.nx;
+  const int sidx = blockIdx.y;
+  const SysScalars s = sys_scalars(g, freq[sidx]);
+  const MatPlanes mp = nsr_planes(mat, n);
+  const CT* us = u + sidx * n;
+  const double inv_h2 = 1.0 / (g.h * g.h);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.nx), j = (int)(k - (long long)i * g.nx);
+    auto U = [&](int i2, int j2) -> double2 {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return make_double2(0.0, 0.0);
+      const CT q = us[(long long)i2 * g.nx + j2];
+      return make_double2((double)q.x, (double)q.y);
+    };
+    auto DA = [&](int i2, int j2) -> double {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return 0.0;
+      const long long id = (long long)i2 * g.nx + j2;
+      return -mp.a64[id] * dlogrho[id];
+    };
+    const double2 flux = stencil<double, false>(g, s, i, j, 0.0, mp.t64[k], U, DA);
+    const double sig = s.sig;
+    const double2 sx = make_double2(1.0, sig * pml_profile<double>((double)j, g.nx, g.n_pml));
+    const double2 sz = make_double2(1.0, sig * pml_profile<double>((double)i, g.nz, g.n_pml));
+    const double2 onepie = make_double2(1.0, mp.t64[k] * s.fpow);
+    const double2 cell = (s.kh2 * mp.b64[k]) * (sx * sz);
+    const double2 dmass = (-2.0 * dlogc[k]) * (cell * onepie) + (-dlogrho[k]) * (cell * (onepie * onepie));
+    const double2 d = flux + dmass * U(i, j);
+    const double2 r = (-inv_h2) * d;
+    CT o;
+    o.x = r.x;
+    o.y = r.y;
+    rhs[sidx * n + k] = o;
+  }
+}
+
+extern "C" int nsr_tangent_rhs(const NsrGrid* grid, const void* coef, const double* freq_hz, int32_t n_systems,
+                               int32_t precision, const void* u, const double* dlogc, const double* dlogrho,
+                               void* rhs, void* stream) {
+  int err = nsr_check_grid(grid, false);
+  if (err) return err;
+  if (!coef || !freq_hz || !u || !dlogc || !dlogrho || !rhs || n_systems < 0 || n_systems > 65535)
+    return NSR_ERR_ARGUMENT;
+  if (precision != 0 && precision != 1) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;
+  long long n = (long long)grid->nz * grid->nx;
+  int bx = (int)((n + 255) / 256);
+  if (bx > 148 * 8) bx = 148 * 8;
+  dim3 gd(bx, n_systems);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == 0)
+    k_tangent<float2><<<gd, 256, 0, st>>>(make_geo(*grid), coef, freq_hz, (const float2*)u, dlogc, dlogrho,
+                                          (float2*)rhs);
+  else
+    k_tangent<double2><<<gd, 256, 0, st>>>(make_geo(*grid), coef, freq_hz, (const double2*)u, dlogc, dlogrho,
+                                           (double2*)rhs);
+  return last_error();
+}

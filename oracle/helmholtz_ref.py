@@ -377,3 +377,42 @@ def time_lu_frequency(spec: Spec, c, rho, alpha_db, frequency_hz, angles_rad):
     seconds = time.perf_counter() - started
     res = max(relative_residual(matrix, fields[:, k], rhs[:, k]) for k in range(rhs.shape[1]))
     return fields.T, seconds, res
+
+
+def operator_derivative(spec: Spec, c, rho, alpha_db, frequency_hz, dlogc, dlogrho):
+    """``dA = sum_k (dA/dlog c_k) dlogc_k + (dA/dlog rho_k) dlogrho_k`` (CSR, SI).
+
+    The directional derivative of :func:`operator` that ``born_data`` applies
+    as ``delta_A`` (theranostic/wave.py:280-329, ``matrix(m) - matrix(0)`` is
+    this derivative for its linear contrasts): mass ``-2 k0^2 sx sz b (1+ie)``
+    per unit log c (the attenuation term is proportional to c) and ``-mass``
+    per unit log rho; edge fluxes ``stretch (da_i + da_j)/(2 h^2)`` with
+    ``da = -a dlogrho`` and zero ghost contrast.
+    """
+    a, b, t = material(spec, c, rho, alpha_db)
+    dlogc = np.asarray(dlogc, dtype=np.float64)
+    dlogrho = np.asarray(dlogrho, dtype=np.float64)
+    sx, sz, sxh, szh = stretches(spec, frequency_hz)
+    e = t * (frequency_hz / 1e6) ** (spec.alpha_power - 1.0)
+    cell = k0_of(spec, frequency_hz) ** 2 * (sz[:, None] * sx[None, :]) * b
+    dmass = -2.0 * cell * (1.0 + 1j * e) * dlogc - cell * (1.0 + 1j * e) ** 2 * dlogrho
+    da = np.pad(-a * dlogrho, 1)                    # zero ghost contrast: no ghost derivative
+    dax = 0.5 * (da[1:-1, :-1] + da[1:-1, 1:])      # [nz, nx+1]
+    daz = 0.5 * (da[:-1, 1:-1] + da[1:, 1:-1])      # [nz+1, nx]
+    fx = (sz[:, None] / sxh[None, :]) * dax / spec.h ** 2
+    fz = (sx[None, :] / szh[:, None]) * daz / spec.h ** 2
+    diagonal = dmass - fx[:, :-1] - fx[:, 1:] - fz[:-1, :] - fz[1:, :]
+    nz, nx = spec.nz, spec.nx
+    east_full = np.zeros((nz, nx), dtype=np.complex128)
+    east_full[:, :-1] = fx[:, 1:-1]
+    e1 = east_full.ravel()[:-1]
+    south = fz[1:-1, :].ravel()
+    return sparse.diags([diagonal.ravel(), e1, e1, south, south], [0, 1, -1, nx, -nx],
+                        shape=(spec.n, spec.n), format="csr", dtype=np.complex128)
+
+
+def born_fields(spec: Spec, c, rho, alpha_db, frequency_hz, u, dlogc, dlogrho):
+    """Tangent fields ``du = -A^-1 dA u`` (theranostic/wave.py:280-329) by SuperLU; ``u`` is [n] or [n, k]."""
+    A = operator(spec, c, rho, alpha_db, frequency_hz)
+    dA = operator_derivative(spec, c, rho, alpha_db, frequency_hz, dlogc, dlogrho)
+    return solve_lu(A, -(dA @ np.asarray(u, dtype=np.complex128)))

@@ -187,3 +187,27 @@ def test_dense_oracle_matches_reference_operator():
         left = np.vdot(q, s.apply(p))
         right = np.vdot(s.adjoint(q), p)
         assert abs(left - right) / abs(left) < 1e-12
+
+
+def test_operator_derivative_against_central_differences():
+    """The directional derivative of the operator (the tangent / Born perturbation)."""
+    spec = H.Spec(nz=20, nx=24, h=1e-4, n_pml=4, face=5, rx_cols=np.arange(4, 20), aperture_half_width=8e-4)
+    rng = np.random.default_rng(11)
+    c = 1500 + 40 * rng.standard_normal((20, 24))
+    rho = 1000 + 30 * rng.standard_normal((20, 24))
+    alpha = rng.uniform(0.3, 1.5, (20, 24))
+    dc = rng.standard_normal((20, 24))
+    dr = rng.standard_normal((20, 24))
+    f = 2.5e6
+    dA = H.operator_derivative(spec, c, rho, alpha, f, dc, dr)
+    eps = 1e-5
+    fd = (H.operator(spec, c * np.exp(eps * dc), rho * np.exp(eps * dr), alpha, f)
+          - H.operator(spec, c * np.exp(-eps * dc), rho * np.exp(-eps * dr), alpha, f)) / (2 * eps)
+    assert abs(dA - fd).max() <= 1e-7 * abs(fd).max()
+    # tangent fields against central differences of the solve
+    b = H.plane_wave_rhs(spec, f, 0.2)
+    u = H.solve_lu(H.operator(spec, c, rho, alpha, f), b)
+    du = H.born_fields(spec, c, rho, alpha, f, u, dc, dr)
+    up = H.solve_lu(H.operator(spec, c * np.exp(eps * dc), rho * np.exp(eps * dr), alpha, f), b)
+    um = H.solve_lu(H.operator(spec, c * np.exp(-eps * dc), rho * np.exp(-eps * dr), alpha, f), b)
+    assert rel(du, (up - um) / (2 * eps)) < 1e-6
