@@ -48,13 +48,15 @@ FALLBACK_HBM_GBS = 6650.0
 # Algorithmic bytes per node of one BiCGSTAB iteration and per kernel launch,
 # per resident system (complex64 vectors; coefficient planes counted once per
 # launch and listed separately): fwd h0 reads r,v,t,p,y and writes r,p,y,w;
-# cols reads and writes w; inv h0 reads w, rhat and writes v; fwd h1 reads r,v
-# and writes w; inv h1 reads w, rhat, r, v and writes t.  res h1 (the FP64
-# true residual) has no work in the timed iterations of a fresh batch.
-KERNEL_BYTES = {"fwd_h0": 72, "cols_h0": 16, "inv_h0": 24, "fwd_h1": 24, "cols_h1": 16, "res_h1": 0, "inv_h1": 40}
+# cols and rinv read and write w; inv h0 reads z (= w after rinv), rhat and
+# writes v; fwd h1 reads r,v and writes w; inv h1 reads z, rhat, r, v and
+# writes t.  res h1 (the FP64 true residual) has no work in the timed
+# iterations of a fresh batch.
+KERNEL_BYTES = {"fwd_h0": 72, "cols_h0": 16, "rinv_h0": 16, "inv_h0": 24, "fwd_h1": 24, "cols_h1": 16,
+                "rinv_h1": 16, "res_h1": 0, "inv_h1": 40}
 # The learned preconditioner adds one complex64 gain read per node to every
-# fwd launch (inner gain) and to every inv launch (outer gain).
-LEARNED_BYTES = {k: v + (8 if k.startswith(("fwd", "inv")) else 0) for k, v in KERNEL_BYTES.items()}
+# fwd launch (inner gain) and to every rinv launch (outer gain).
+LEARNED_BYTES = {k: v + (8 if k.startswith(("fwd", "rinv")) else 0) for k, v in KERNEL_BYTES.items()}
 COEF_BYTES = {"inv_h0": 12, "inv_h1": 12}
 LEARNED_SETUP_LAUNCHES = 5     # pool, three convolutions, gains
 

@@ -113,10 +113,11 @@ typedef struct NsrSolveParams {
 /* Optional host-side statistics of one nsr_solve_batched call. */
 typedef struct NsrSolveStats {
   double loop_ms;            /* device time of the solve loop                   */
-  double kernel_ms[8];       /* mean duration per launch, in launch order: fwd,
-                                cols, inv of the first half; fwd, cols, res, inv
-                                of the second half; [7] unused                  */
-  int32_t kernel_timed[8];   /* launches averaged in kernel_ms                  */
+  double kernel_ms[16];      /* mean duration per launch, in launch order: fwd,
+                                cols, rinv, inv of the first half; fwd, cols,
+                                rinv, res, inv of the second half; [9..15]
+                                unused                                          */
+  int32_t kernel_timed[16];  /* launches averaged in kernel_ms                  */
   int64_t launches;          /* kernels launched by the call                    */
   int32_t graph_launches;    /* CUDA graph launches                             */
   int32_t warm_accepted;     /* initial fields kept                             */

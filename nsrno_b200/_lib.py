@@ -62,12 +62,12 @@ class NsrGmresParams(ctypes.Structure):
 
 
 class NsrSolveStats(ctypes.Structure):
-    _fields_ = [("loop_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double * 8),
-                ("kernel_timed", ctypes.c_int32 * 8), ("launches", ctypes.c_int64),
+    _fields_ = [("loop_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double * 16),
+                ("kernel_timed", ctypes.c_int32 * 16), ("launches", ctypes.c_int64),
                 ("graph_launches", ctypes.c_int32), ("warm_accepted", ctypes.c_int32),
                 ("warm_rejected", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
-    KERNELS = ("fwd_h0", "cols_h0", "inv_h0", "fwd_h1", "cols_h1", "res_h1", "inv_h1")
+    KERNELS = ("fwd_h0", "cols_h0", "rinv_h0", "inv_h0", "fwd_h1", "cols_h1", "rinv_h1", "res_h1", "inv_h1")
 
     def as_dict(self):
         return dict(loop_ms=self.loop_ms, launches=int(self.launches), graph_launches=int(self.graph_launches),

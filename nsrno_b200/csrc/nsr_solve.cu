@@ -2,11 +2,14 @@
 // record.  Design:
 //   * n_slots systems are resident; a device-side queue refills a slot when
 //     its system finishes (converged, budget, breakdown, divergence).
-//   * One BiCGSTAB iteration = two halves; each half is three launches:
+//   * One BiCGSTAB iteration = two halves; each half is four launches:
 //       fwd  : elementwise Krylov update fused with the forward row FFT,
 //       cols : column FFT, shifted-Laplace multiply, inverse column FFT,
-//       inv  : inverse row FFT fused with the 5-point stencil and the
-//              FP64 inner products of that half.
+//       rinv : inverse row FFT in place (z = M^-1 of the half's vector),
+//       inv  : 5-point stencil on z (register sliding window down a column
+//              strip) fused with the FP64 inner products of that half;
+//     the second half adds `res`, the FP64 true residual of the slots that
+//     replace their residual, start or emit.
 //     The last CTA of a slot (arrival counter, no waiting) sums the per-CTA
 //     partials in a fixed order and advances that slot's scalar recurrence,
 //     so no host synchronisation happens inside the loop.
@@ -28,7 +31,9 @@
 
 enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES = 4, MODE_EMIT = 5 };
 
-#define NSR_LAUNCHES_PER_IT 7
+#define NSR_LAUNCHES_PER_IT 9
+#define NSR_ST_TZ 16      // rows of one stencil CTA
+#define NSR_ST_TX 256     // columns of one stencil CTA (one per thread)
 
 struct __align__(16) SlotState {
   int sys, mode, iters, final_reason;
@@ -208,6 +213,39 @@ __global__ void __launch_bounds__(512) k_cols(SolveArgs A, int half) {
   if (!cols_active(mode, half)) return;
   const long long n = (long long)A.g.nz * A.g.nx;
   cols_pass<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.slots[slot].freq, A.shift, A.adjoint, blockIdx.x * TC, A.lp);
+}
+
+// ---------------------------------------------------------------------------
+// rinv: inverse row FFT in place on w, times the outer gain of the learned
+// preconditioner; afterwards w holds z = M^-1 (input of the half).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
+  extern __shared__ float2 sm[];
+  const int slot = blockIdx.y;
+  const SlotState& S = A.B.slots[slot];
+  if (!cols_active(S.mode, half)) return;
+  const Geo& g = A.g;
+  const long long n = (long long)g.nz * g.nx;
+  const int z0 = blockIdx.x * A.rows;
+  const int nr = min(A.rows, g.nz - z0);
+  const long long goff = (long long)z0 * g.nx;
+  float2* __restrict__ w = A.B.w + slot * n + goff;
+  const int nx = g.nx, rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
+  for (int l = 0; l < nr; ++l)
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nx; c += blockDim.x) sm[l * rs + (pad ? c + (c >> 4) : c)] = w[l * nx + c];
+  __syncthreads();
+  fft_rows<true>(sm, nr, A.tab.px);
+  __syncthreads();
+  const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
+  for (int l = 0; l < nr; ++l)
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nx; c += blockDim.x) {
+      const int k = l * nx + c;
+      const float2 v = sm[l * rs + (pad ? c + (c >> 4) : c)];
+      w[k] = G.post ? gain_mul(G.post, goff + k, G.conj, v) : v;
+    }
 }
 
 __device__ void pop_next(const SolveArgs& A, SlotState& S) {
@@ -430,82 +468,73 @@ __device__ __forceinline__ void reduce_and_finalize(const SolveArgs& A, SlotStat
 }
 
 // ---------------------------------------------------------------------------
-// inv: inverse row FFT + stencil + inner products of the Krylov halves.
+// inv: stencil on z = M^-1 (input) + inner products of the Krylov halves.
+// One thread per column of a NSR_ST_TZ x NSR_ST_TX tile walks down its rows
+// with the north/centre/south values of z and a in registers; east/west
+// neighbours are the adjacent threads' loads (L1 hits).
 // ---------------------------------------------------------------------------
 template <bool ADJ>
-__global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
-  extern __shared__ float2 sm[];
+__global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
   const int slot = blockIdx.y;
   SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
   if (mode != (half == 0 ? MODE_ITER_A : MODE_ITER_B)) return;
   const Geo& g = A.g;
   const long long n = (long long)g.nz * g.nx;
-  const int z0 = blockIdx.x * A.tz;
-  const int nb = min(A.tz, g.nz - z0);
   const int nx = g.nx;
+  const int nbx = (nx + NSR_ST_TX - 1) / NSR_ST_TX;
+  const int rb = blockIdx.x / nbx, cb = blockIdx.x - rb * nbx;
+  const int z0 = rb * NSR_ST_TZ;
+  const int z1 = min(z0 + NSR_ST_TZ, g.nz);
+  const int j = cb * NSR_ST_TX + threadIdx.x;
   const long long soff = slot * n;
-  const int rs = nsr_row_stride(nx);
-  const bool pad = nsr_row_padded(nx);
-  auto at = [pad](int j) { return pad ? j + (j >> 4) : j; };
-  {
-    const float2* __restrict__ w = A.B.w + soff;
-    const int nl = nb + 2;
-    for (int rr = 0; rr < nl; ++rr) {
-      const int z = z0 - 1 + rr;
-      const bool in = z >= 0 && z < g.nz;
-#pragma unroll 4
-      for (int j = threadIdx.x; j < nx; j += blockDim.x)
-        sm[rr * rs + at(j)] = in ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
-    fft_rows<true>(sm, nl, A.tab.px);
-    band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
-  }
-  const SysScalars sc = sys_scalars(g, S.freq);
-  const float* __restrict__ ca = A.mat.a32;
-  const float* __restrict__ cb = A.mat.b32;
-  const float* __restrict__ ct = A.mat.t32;
-  const float2* __restrict__ rh = A.B.rh + soff;
   double acc[NSR_NPART];
 #pragma unroll
   for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
-  const float2 sv = f2(S.c_sv);
-  float2* __restrict__ out = (half == 0 ? A.B.v : A.B.t) + soff;
-  const float2* __restrict__ r = A.B.r + soff;
-  const float2* __restrict__ v = A.B.v + soff;
-  for (int rr = 0; rr < nb; ++rr) {
-    const int i = z0 + rr;
-    const float2* row = sm + (rr + 1) * rs;
-    const float2* up = sm + rr * rs;
-    const float2* dn = sm + (rr + 2) * rs;
-#pragma unroll 2
-    for (int j = threadIdx.x; j < nx; j += blockDim.x) {
-      const long long idx = (long long)i * nx + j;
-      const float2 z = make_float2(0.f, 0.f);
-      const int aj = at(j);
-      const float2 pc = row[aj];
-      const float2 pe = j + 1 < nx ? row[at(j + 1)] : z;
-      const float2 pw = j > 0 ? row[at(j - 1)] : z;
-      const float a_c = __ldg(&ca[idx]);
-      const float a_e = j + 1 < nx ? __ldg(&ca[idx + 1]) : 1.0f;
-      const float a_w = j > 0 ? __ldg(&ca[idx - 1]) : 1.0f;
-      const float a_s = i + 1 < g.nz ? __ldg(&ca[idx + nx]) : 1.0f;
-      const float a_n = i > 0 ? __ldg(&ca[idx - nx]) : 1.0f;
-      const float2 av = stencil_pts<ADJ>(g, sc, i, j, a_c, a_e, a_w, a_s, a_n, __ldg(&cb[idx]), __ldg(&ct[idx]),
-                                         pc, pe, pw, dn[aj], up[aj]);
+  if (j < nx) {
+    const SysScalars sc = sys_scalars(g, S.freq);
+    const float* __restrict__ ca = A.mat.a32;
+    const float* __restrict__ cb_ = A.mat.b32;
+    const float* __restrict__ ct = A.mat.t32;
+    const float2* __restrict__ z = A.B.w + soff;
+    const float2* __restrict__ rh = A.B.rh + soff;
+    const float2* __restrict__ r = A.B.r + soff;
+    const float2* __restrict__ v = A.B.v + soff;
+    float2* __restrict__ out = (half == 0 ? A.B.v : A.B.t) + soff;
+    const float2 sv = f2(S.c_sv);
+    const float2 zero = make_float2(0.f, 0.f);
+    const bool has_e = j + 1 < nx, has_w = j > 0;
+    long long idx = (long long)z0 * nx + j;
+    float2 zu = z0 > 0 ? z[idx - nx] : zero;
+    float2 zc = z[idx];
+    float a_n = z0 > 0 ? __ldg(&ca[idx - nx]) : 1.0f;
+    float a_c = __ldg(&ca[idx]);
+    for (int i = z0; i < z1; ++i, idx += nx) {
+      const bool has_s = i + 1 < g.nz;
+      const float2 zd = has_s ? z[idx + nx] : zero;
+      const float a_s = has_s ? __ldg(&ca[idx + nx]) : 1.0f;
+      const float2 ze = has_e ? z[idx + 1] : zero;
+      const float2 zw = has_w ? z[idx - 1] : zero;
+      const float a_e = has_e ? __ldg(&ca[idx + 1]) : 1.0f;
+      const float a_w = has_w ? __ldg(&ca[idx - 1]) : 1.0f;
+      const float2 av = stencil_pts<ADJ>(g, sc, i, j, a_c, a_e, a_w, a_s, a_n, __ldg(&cb_[idx]), __ldg(&ct[idx]),
+                                         zc, ze, zw, zd, zu);
       out[idx] = av;
       const float2 rk = rh[idx];
       if (half == 0) {
         dot_acc(acc[0], acc[1], rk, av);       // <rhat, v>
       } else {
-        const float2 s = r[idx] + sv * v[idx];
-        dot_acc(acc[0], acc[1], av, s);        // <t, s>
+        const float2 s1 = r[idx] + sv * v[idx];
+        dot_acc(acc[0], acc[1], av, s1);       // <t, s>
         acc[2] += (double)av.x * av.x + (double)av.y * av.y;
-        acc[3] += (double)s.x * s.x + (double)s.y * s.y;
+        acc[3] += (double)s1.x * s1.x + (double)s1.y * s1.y;
         dot_acc(acc[4], acc[5], rk, av);       // <rhat, t>
-        dot_acc(acc[6], acc[7], rk, s);        // <rhat, s>
+        dot_acc(acc[6], acc[7], rk, s1);       // <rhat, s>
       }
+      zu = zc;
+      zc = zd;
+      a_n = a_c;
+      a_c = a_s;
     }
   }
   reduce_and_finalize(A, S, slot, mode, acc);
@@ -517,7 +546,6 @@ __global__ void __launch_bounds__(256) k_inv(SolveArgs A, int half) {
 // ---------------------------------------------------------------------------
 template <bool ADJ>
 __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
-  extern __shared__ float2 sm[];
   const int slot = blockIdx.y;
   SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
@@ -540,21 +568,8 @@ __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
 #pragma unroll
   for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
   const long long soff = slot * n;
-  const int rs = nsr_row_stride(nx);
-  const bool pad = nsr_row_padded(nx);
-  if (mode == MODE_RES) {
-    const float2* w = A.B.w + soff;
-    const int nl = nb + 2;
-    for (int k = threadIdx.x; k < nl * nx; k += blockDim.x) {
-      const int zr = k / nx, j = k - zr * nx;
-      const int z = z0 - 1 + zr;
-      sm[zr * rs + (pad ? j + (j >> 4) : j)] = (z >= 0 && z < g.nz) ? w[(long long)z * nx + j] : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
-    fft_rows<true>(sm, nl, A.tab.px);
-    band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
-  }
   if (mode == MODE_RES || mode == MODE_INIT) {
+    const float2* zw = A.B.w + soff;   // z = M^-1 y after the rinv pass
     const double2* xo = A.B.x + (2LL * slot + S.xpar) * n;
     double2* xn = A.B.x + (2LL * slot + (S.xpar ^ 1)) * n;
     const float2* x0 = (A.x0 && S.sys >= 0 && !S.x0_off) ? A.x0 + (long long)S.sys * n : nullptr;
@@ -562,7 +577,7 @@ __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
       if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return make_double2(0.0, 0.0);
       const long long id = (long long)i2 * nx + j2;
       if (mode == MODE_INIT) return x0 ? to_d(x0[id]) : make_double2(0.0, 0.0);
-      return xo[id] + to_d(sm[(i2 - z0 + 1) * rs + (pad ? j2 + (j2 >> 4) : j2)]);
+      return xo[id] + to_d(zw[id]);
     };
     const double h2 = g.h * g.h;
     const float2* rhs = A.rhs ? A.rhs + (long long)S.sys * n : nullptr;
@@ -652,7 +667,9 @@ static Layout layout(const NsrGrid* g, int n_slots) {
   Layout L;
   const size_t n = (size_t)g->nz * g->nx;
   const int tz = band_rows(g);
-  L.nb_inv = (g->nz + tz - 1) / tz;
+  const int nb_res = (g->nz + tz - 1) / tz;
+  const int nb_st = ((g->nz + NSR_ST_TZ - 1) / NSR_ST_TZ) * ((g->nx + NSR_ST_TX - 1) / NSR_ST_TX);
+  L.nb_inv = nb_res > nb_st ? nb_res : nb_st;
   size_t off = 0;
   L.tables = off; off += nsr_align(nsr_prec_table_bytes(g));
   L.slots = off; off += nsr_align(sizeof(SlotState) * n_slots);
@@ -777,14 +794,12 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
 
     const size_t fwd_smem = sizeof(float2) * A.rows * nsr_row_stride(grid->nx);
     const size_t col_smem = nsr_cols_smem(grid);
-    const size_t inv_smem = sizeof(float2) * (A.tz + 2) * nsr_row_stride(grid->nx);
+    const int nb_res = (grid->nz + A.tz - 1) / A.tz;
+    const int nb_st = ((grid->nz + NSR_ST_TZ - 1) / NSR_ST_TZ) * ((grid->nx + NSR_ST_TX - 1) / NSR_ST_TX);
     NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_inv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_inv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_res<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_res<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_rinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
 
     k_solve_init<<<64, 256, 0, st>>>(A, n_slots);
     NSR_TRY(cudaGetLastError());
@@ -792,12 +807,13 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
 
     const dim3 g_fwd((grid->nz + A.rows - 1) / A.rows, n_slots);
     const dim3 g_col((grid->nx + A.tc - 1) / A.tc, n_slots);
-    const dim3 g_inv(L.nb_inv, n_slots);
+    const dim3 g_inv(nb_st, n_slots);
+    const dim3 g_res(nb_res, n_slots);
     const int K = params->graph_iterations > 0 ? params->graph_iterations : 16;
-    // One iteration = 7 launches: fwd, cols, inv of the first half, then fwd,
-    // cols, res, inv of the second half.
-    const int seq_half[NSR_LAUNCHES_PER_IT] = {0, 0, 0, 1, 1, 1, 1};
-    const int seq_kind[NSR_LAUNCHES_PER_IT] = {0, 1, 3, 0, 1, 2, 3};
+    // One iteration = 9 launches: fwd, cols, rinv, inv of the first half, then
+    // fwd, cols, rinv, res, inv of the second half.
+    const int seq_half[NSR_LAUNCHES_PER_IT] = {0, 0, 0, 0, 1, 1, 1, 1, 1};
+    const int seq_kind[NSR_LAUNCHES_PER_IT] = {0, 1, 4, 3, 0, 1, 4, 2, 3};
     auto launch = [&](int q) {
       const int half = seq_half[q], which = seq_kind[q];
       if (which == 0) {
@@ -806,11 +822,13 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
         if (A.tc == 16) k_cols<16><<<g_col, 512, col_smem, st>>>(A, half);
         else k_cols<8><<<g_col, 512, col_smem, st>>>(A, half);
       } else if (which == 2) {
-        if (A.adjoint) k_res<true><<<g_inv, 256, inv_smem, st>>>(A);
-        else k_res<false><<<g_inv, 256, inv_smem, st>>>(A);
+        if (A.adjoint) k_res<true><<<g_res, 256, 0, st>>>(A);
+        else k_res<false><<<g_res, 256, 0, st>>>(A);
+      } else if (which == 3) {
+        if (A.adjoint) k_inv<true><<<g_inv, 256, 0, st>>>(A, half);
+        else k_inv<false><<<g_inv, 256, 0, st>>>(A, half);
       } else {
-        if (A.adjoint) k_inv<true><<<g_inv, 256, inv_smem, st>>>(A, half);
-        else k_inv<false><<<g_inv, 256, inv_smem, st>>>(A, half);
+        k_rinv<<<g_fwd, 256, fwd_smem, st>>>(A, half);
       }
     };
 
