@@ -292,6 +292,17 @@ int nsr_tangent_rhs(const NsrGrid* grid, const void* coef, const double* freq_hz
                     int32_t precision, const void* u, const double* dlogc, const double* dlogrho,
                     void* rhs, void* stream);
 
+/* Fixed preconditioner of the dense path, y = mask * IFFT(m * FFT(x)) with
+ * m = 1/(1 + lap/k0^2 - i shift) and the 8th-order staggered symbols in lap
+ * (nsrno/conditioned_wave.py:90-92, nsrno/dense_wave.py:194-196); adjoint = 1
+ * conjugates m as the reference's adjoint solve does.  k0dx2 = (k0 dx)^2 with
+ * the system's k0 = 2 sin(pi f dt)/(dt c0).  H and W must be 2^a 3^b in
+ * [8, 2048].  x, y: c64 [n_fields][H][W]. */
+size_t nsr_dense_precondition_workspace_size(const NsrDenseGrid* grid, int32_t n_fields);
+int nsr_dense_precondition(const NsrDenseGrid* grid, double k0dx2, double shift, int32_t n_fields,
+                           int32_t adjoint, const float* x, float* y, void* workspace, size_t workspace_bytes,
+                           void* stream);
+
 /* ---- Learned preconditioner: inference -------------------------------- */
 
 /* Bytes of the low-resolution network state of n_freq frequencies. */

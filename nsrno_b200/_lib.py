@@ -22,7 +22,7 @@ EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_m
            "nsr_learned_state_bytes", "nsr_learned_setup", "nsr_learned_precondition",
            "nsr_learned_backward_workspace_size", "nsr_learned_map_backward", "nsr_learned_network_backward",
            "nsr_learned_spectral_workspace_size", "nsr_learned_spectral_backward", "nsr_learned_adam",
-           "nsr_tangent_rhs")
+           "nsr_tangent_rhs", "nsr_dense_precondition_workspace_size", "nsr_dense_precondition")
 
 LEARNED_PARAMS = 3645
 
@@ -117,6 +117,9 @@ def load():
     lib.nsr_dense_workspace_size.restype = S
     lib.nsr_dense_workspace_size.argtypes = [DG, I, I]
     lib.nsr_dense_apply.argtypes = [DG, P, D, D, I, I, I, P, P, P, S, P]
+    lib.nsr_dense_precondition_workspace_size.restype = S
+    lib.nsr_dense_precondition_workspace_size.argtypes = [DG, I]
+    lib.nsr_dense_precondition.argtypes = [DG, D, D, I, I, P, P, P, S, P]
     L = ctypes.POINTER(NsrLearned)
     lib.nsr_learned_state_bytes.restype = S
     lib.nsr_learned_state_bytes.argtypes = [G, I]

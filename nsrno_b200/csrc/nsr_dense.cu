@@ -13,6 +13,8 @@
 // Pass 1 writes the staggered fluxes, pass 2 takes their divergence.
 #include "nsr_internal.cuh"
 
+#include <string.h>
+
 __constant__ double c_dense_a[4] = {1225.0 / 1024.0, -245.0 / 3072.0, 49.0 / 5120.0, -5.0 / 7168.0};
 
 struct DenseCoef {
@@ -216,6 +218,146 @@ extern "C" int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, dou
       k_dense_div<double, false><<<gr, 256, 0, st>>>(g, coef, (const double2*)x, t, (double2*)y, n_fields);
     }
   }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
+// ---------------------------------------------------------------------------
+// Fixed preconditioner of the dense path (nsrno/conditioned_wave.py:90-92,
+// nsrno/dense_wave.py:194-196):
+//   M r = mask * IFFT((1 + lap/k0^2 - i shift)^-1 FFT(r)),
+// lap = -(|Dx|^2 + |Dz|^2) with the 8th-order staggered symbols
+// |D(q)|^2 = (2 sum_k a_k sin((k + 1/2) q))^2 / dx^2 (conditioned_wave.py:24-27).
+// The transforms are the solver's row and column FFTs (grids of 2^a 3^b).
+// ---------------------------------------------------------------------------
+__global__ void k_dense_symbol(int n, FftPlan plan, float* d2) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int f = nsr_digit_reverse(k, n, plan.radix, plan.nst);
+    const double q = 2.0 * NSR_PI * f / n;
+    double s = 0.0;
+    for (int j = 0; j < 4; ++j) s += c_dense_a[j] * sin((j + 0.5) * q);
+    d2[k] = (float)(4.0 * s * s);   // |D|^2 dx^2
+  }
+}
+
+template <int TC>
+__global__ void __launch_bounds__(512) k_dense_cols(int nz, int nx, PrecTables t, const float* __restrict__ d2z,
+                                                    const float* __restrict__ d2x, float2* __restrict__ w,
+                                                    float inv_k0dx2, float shift, int adjoint) {
+  extern __shared__ float2 sm[];
+  const long long n = (long long)nz * nx;
+  float2* ws = w + blockIdx.y * n;
+  const int c0 = blockIdx.x * TC;
+  const int ncol = min(TC, nx - c0);
+  for (int k = threadIdx.x; k < nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
+    sm[k] = c < ncol ? ws[(long long)z * nx + c0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_cols<false, TC>(sm, t.pz);
+  const float inv_n = 1.0f / (float)n;
+  for (int k = threadIdx.x; k < nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
+    if (c < ncol) {
+      const float re = 1.0f - (d2z[z] + d2x[c0 + c]) * inv_k0dx2;
+      float2 mul = divc(make_float2(inv_n, 0.f), make_float2(re, -shift));
+      if (adjoint) mul = conjc(mul);
+      sm[k] = sm[k] * mul;
+    }
+  }
+  __syncthreads();
+  fft_cols<true, TC>(sm, t.pz);
+  for (int k = threadIdx.x; k < nz * TC; k += blockDim.x) {
+    const int z = k / TC, c = k - z * TC;
+    if (c < ncol) ws[(long long)z * nx + c0 + c] = sm[k];
+  }
+}
+
+__global__ void k_dense_rows(int nz, int nx, int pz, int px, int h, int w, PrecTables t,
+                             const float2* __restrict__ x, float2* __restrict__ y, int rows, int inverse) {
+  extern __shared__ float2 sm[];
+  const long long n = (long long)nz * nx;
+  const int z0 = blockIdx.x * rows;
+  const int nr = min(rows, nz - z0);
+  const float2* xs = x + blockIdx.y * n + (long long)z0 * nx;
+  const int rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
+  for (int k = threadIdx.x; k < nr * nx; k += blockDim.x) {
+    const int l = k / nx, c = k - l * nx;
+    sm[l * rs + (pad ? c + (c >> 4) : c)] = xs[k];
+  }
+  __syncthreads();
+  if (inverse) fft_rows<true>(sm, nr, t.px);
+  else fft_rows<false>(sm, nr, t.px);
+  __syncthreads();
+  float2* ys = y + blockIdx.y * n + (long long)z0 * nx;
+  for (int k = threadIdx.x; k < nr * nx; k += blockDim.x) {
+    const int l = k / nx, c = k - l * nx;
+    const int i = z0 + l;
+    const bool in = !inverse || (i >= pz && i < pz + h && c >= px && c < px + w);
+    ys[k] = in ? sm[l * rs + (pad ? c + (c >> 4) : c)] : make_float2(0.f, 0.f);
+  }
+}
+
+static NsrGrid dense_fft_grid(const NsrDenseGrid* g) {
+  NsrGrid q;
+  memset(&q, 0, sizeof(q));
+  q.nz = g->H;
+  q.nx = g->W;
+  q.h = g->dx;
+  q.c0 = 1540.0;      // only the transform sizes of this grid are used
+  q.rho0 = 1000.0;
+  return q;
+}
+
+extern "C" size_t nsr_dense_precondition_workspace_size(const NsrDenseGrid* g, int32_t n_fields) {
+  if (!g || n_fields <= 0 || n_fields > 65535) return 0;
+  NsrGrid q = dense_fft_grid(g);
+  if (nsr_check_grid(&q, true)) return 0;
+  return nsr_align(nsr_prec_table_bytes(&q)) + nsr_align(sizeof(float) * (g->H + g->W)) +
+         nsr_align(sizeof(float2) * (size_t)g->H * g->W * n_fields);
+}
+
+extern "C" int nsr_dense_precondition(const NsrDenseGrid* grid, double k0dx2, double shift, int32_t n_fields,
+                                      int32_t adjoint, const float* x, float* y, void* workspace,
+                                      size_t workspace_bytes, void* stream) {
+  if (!grid || !x || !y || !workspace || n_fields < 0 || n_fields > 65535 || !(k0dx2 > 0) || !(shift >= 0))
+    return NSR_ERR_ARGUMENT;
+  if (grid->pz < 0 || grid->px < 0 || grid->pz + grid->h > grid->H || grid->px + grid->w > grid->W)
+    return NSR_ERR_ARGUMENT;
+  if (n_fields == 0) return 0;
+  const size_t need = nsr_dense_precondition_workspace_size(grid, n_fields);
+  if (need == 0) return NSR_ERR_UNSUPPORTED_SIZE;
+  if (workspace_bytes < need) return NSR_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  NsrGrid q = dense_fft_grid(grid);
+  char* ws = (char*)workspace;
+  PrecTables t;
+  int err = nsr_prec_setup(&q, &t, ws, st);
+  if (err) return err;
+  float* d2x = (float*)(ws + nsr_align(nsr_prec_table_bytes(&q)));
+  float* d2z = d2x + grid->W;
+  float2* w = (float2*)(ws + nsr_align(nsr_prec_table_bytes(&q)) + nsr_align(sizeof(float) * (grid->H + grid->W)));
+  k_dense_symbol<<<(grid->W + 255) / 256, 256, 0, st>>>(grid->W, t.px, d2x);
+  k_dense_symbol<<<(grid->H + 255) / 256, 256, 0, st>>>(grid->H, t.pz, d2z);
+  const int rows = nsr_rows_per_cta(&q);
+  const size_t row_smem = sizeof(float2) * (size_t)rows * nsr_row_stride(grid->W);
+  const dim3 gr((grid->H + rows - 1) / rows, n_fields);
+  k_dense_rows<<<gr, 256, row_smem, st>>>(grid->H, grid->W, grid->pz, grid->px, grid->h, grid->w, t,
+                                          (const float2*)x, w, rows, 0);
+  const int tc = nsr_cols_tc(&q);
+  const dim3 gc((grid->W + tc - 1) / tc, n_fields);
+  const size_t csm = nsr_cols_smem(&q);
+  const float inv = (float)(1.0 / k0dx2);
+  if (tc == 16) {
+    cudaFuncSetAttribute(k_dense_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+    k_dense_cols<16><<<gc, 512, csm, st>>>(grid->H, grid->W, t, d2z, d2x, w, inv, (float)shift, adjoint);
+  } else {
+    cudaFuncSetAttribute(k_dense_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+    k_dense_cols<8><<<gc, 512, csm, st>>>(grid->H, grid->W, t, d2z, d2x, w, inv, (float)shift, adjoint);
+  }
+  k_dense_rows<<<gr, 256, row_smem, st>>>(grid->H, grid->W, grid->pz, grid->px, grid->h, grid->w, t, w,
+                                          (float2*)y, rows, 1);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? 0 : (int)e;
 }

@@ -407,8 +407,12 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
     if (S.iters >= A.max_it) { finish_system(A, S, NSR_ITERATION_BUDGET, rel); return; }
     const double2 z = make_double2(0.0, 0.0);
     S.c_sv = S.c_rt = S.c_yp = S.c_ys = z;
-    if (S.force_restart || (A.restart2 > 0.0 && rr < A.restart2 * S.r0norm2)) {
-      // Restart: fresh shadow vector rhat = r (written by the next fwd pass), p = r.
+    // Restart (fresh shadow vector rhat = r, written by the next fwd pass; p = r)
+    // after a forced restart, after the true residual fell by restart_factor
+    // since the last restart, or when it grew since then: the FP32 recurrence
+    // has lost its bi-orthogonality and would otherwise run away (one system
+    // in 24,000 of the training media diverged without this).
+    if (S.force_restart || rr > S.r0norm2 || (A.restart2 > 0.0 && rr < A.restart2 * S.r0norm2)) {
       S.restart = 1;
       S.force_restart = 0;
       S.r0norm2 = rr;

@@ -158,3 +158,160 @@ class DenseSystem:
     def adjoint(self, p):
         """Its exact adjoint (nsrno/dense_wave.py:70-82)."""
         return self._run(p, True)
+
+    # ------------------------------------------------------------------
+    # Preconditioner, source and assembly (nsrno/conditioned_wave.py:82-92,
+    # nsrno/dense_wave.py:46-62)
+    # ------------------------------------------------------------------
+    def fixed_preconditioner(self, shift=0.15, adjoint=False):
+        """``r -> mask IFFT(FFT(r) / (1 + lap/k0^2 - i shift))`` (conditioned_wave.py:90-92) on the
+        device (``nsr_dense_precondition``); ``adjoint`` conjugates the multiplier as
+        nsrno/dense_wave.py:195 does for the adjoint solve.  Complex64 arithmetic."""
+        g = self.g
+        k0dx2 = (self.k0 * g.dx) ** 2
+
+        def apply(r):
+            r = torch.as_tensor(r)
+            squeeze = r.dim() == 2
+            x = (r[None] if squeeze else r).to(torch.complex64).contiguous()
+            if not x.is_cuda or tuple(x.shape[1:]) != (g.H, g.W):
+                raise ValueError(f"fields must be CUDA [n, {g.H}, {g.W}]")
+            lib = _lib.load()
+            nbytes = lib.nsr_dense_precondition_workspace_size(ctypes.byref(g.struct), x.shape[0])
+            if nbytes == 0:
+                raise ValueError("the dense preconditioner needs H and W of the form 2^a 3^b in [8, 2048]")
+            ws = torch.empty(nbytes, dtype=torch.uint8, device=x.device)
+            y = torch.empty_like(x)
+            _lib.check(lib.nsr_dense_precondition(ctypes.byref(g.struct), float(k0dx2), float(shift), x.shape[0],
+                                                  int(bool(adjoint)), ctypes.c_void_p(x.data_ptr()),
+                                                  ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
+                                                  nbytes, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+            y = y.to(r.dtype)
+            return y[0] if squeeze else y
+        return apply
+
+    def source(self, line):
+        """Pressure source of a line on the array row (conditioned_wave.py:82-88):
+        ``line [n, w]`` padded into row ``face``, times ``a c0^2 2 dt / (c_src dx (D - 1))``."""
+        g = self.g
+        line = torch.as_tensor(line)
+        squeeze = line.dim() == 1
+        if squeeze:
+            line = line[None]
+        dev = line.device
+        zi, xi = g.spec["source_c_lookup_zx"]
+        source_c = float(self.c[zi + g.pz, xi + g.px])
+        a = torch.as_tensor(RHO0 / self.rho, device=dev)
+        dtype = torch.complex128 if line.dtype in (torch.complex128, torch.float64) else torch.complex64
+        profile = torch.zeros((line.shape[0], g.H, g.W), dtype=dtype, device=dev)
+        profile[:, g.face, g.px:g.px + line.shape[-1]] = line.to(dtype)
+        scale = C0 ** 2 * 2 * g.dt / (source_c * g.dx * (self.D - 1.0))
+        out = profile * (a.to(dtype) * scale)
+        return out[0] if squeeze else out
+
+
+def homogeneous_system(geometry: DenseGeometry, frequency, device="cuda"):
+    """The uniform reference medium (1540 m/s, 1000 kg/m^3, alpha 0.002) of the
+    dense acquisition (nsrno/dense_wave.py:53-55)."""
+    medium = np.stack((np.full((geometry.h, geometry.w), C0), np.full((geometry.h, geometry.w), RHO0)))
+    return DenseSystem(geometry, medium, np.full((geometry.h, geometry.w), 0.002), frequency, device=device)
+
+
+def assemble(system: DenseSystem, reference: DenseSystem, line, pref):
+    """Scattered-field right-hand side with homogeneous-reference subtraction
+    (nsrno/dense_wave.py:46-57): ``S(src) - S0(src) - A p_ref + A0 p_ref``."""
+    return system.source(line) - reference.source(line) - system.apply(pref) + reference.apply(pref)
+
+
+def gmres(operator, precondition, rhs, x, callback=None, restart=32, max_cycles=80, tolerance=1e-4):
+    """Restarted right-preconditioned GMRES with two classical Gram-Schmidt passes
+    over the whole field batch as one vector (nsrno/wave_solver.py:9-36): happy
+    breakdown below 1e-12, preconditioned directions kept, the small least
+    squares in complex128 on the host.  Returns ``(x, reason, steps)``."""
+    shape = rhs.shape
+    n = rhs.numel()
+    scale = rhs.norm().clamp_min(1e-30)
+    basis = torch.empty((restart + 1, n), dtype=rhs.dtype, device=rhs.device)
+    directions = torch.empty((restart, n), dtype=rhs.dtype, device=rhs.device)
+    steps = 0
+    for _ in range(max_cycles):
+        residual = rhs - operator(x)
+        beta = residual.norm()
+        relative = float(beta / scale)
+        if callback is not None:
+            callback(steps, x, relative)
+        if relative < tolerance:
+            return x, "converged", steps
+        basis[0] = residual.flatten() / beta
+        h = torch.zeros((restart + 1, restart), dtype=rhs.dtype, device=rhs.device)
+        used = restart
+        for j in range(restart):
+            z = precondition(basis[j].reshape(shape))
+            directions[j] = z.flatten()
+            w = operator(z).flatten()
+            steps += 1
+            for _ in range(2):
+                coefficients = basis[: j + 1].conj() @ w
+                w = w - basis[: j + 1].T @ coefficients
+                h[: j + 1, j] += coefficients
+            h[j + 1, j] = w.norm()
+            if float(h[j + 1, j].abs()) < 1e-12:
+                used = j + 1
+                break
+            basis[j + 1] = w / h[j + 1, j]
+        q = torch.zeros(used + 1, dtype=torch.complex128)
+        q[0] = complex(beta)
+        y = torch.linalg.lstsq(h[: used + 1, :used].cpu().to(torch.complex128), q).solution
+        x = x + (directions[:used].T @ y.to(rhs.device, rhs.dtype)).reshape(shape)
+    final = float((rhs - operator(x)).norm() / scale)
+    if callback is not None:
+        callback(steps, x, final)
+    return x, ("converged" if final < tolerance else "iteration_budget"), steps
+
+
+def solve(system: DenseSystem, rhs, adjoint=False, tolerance=1e-5, restart=32, max_cycles=100, shift=0.15,
+          initial=None):
+    """Converged dense-path solve of ``A x = rhs`` (or ``A^H x = rhs``) with the
+    fixed preconditioner: the GMRES branch of ``solve_system``
+    (nsrno/dense_wave.py:217-220).  Returns ``(x, info)``."""
+    import time
+    started = time.perf_counter()
+    rhs = torch.as_tensor(rhs)
+    op = system.adjoint if adjoint else system.apply
+    pre = system.fixed_preconditioner(shift, adjoint=adjoint)
+    trace = []
+    x0 = torch.zeros_like(rhs) if initial is None else torch.as_tensor(initial).to(rhs.dtype)
+    x, reason, steps = gmres(op, pre, rhs, x0, lambda k, u, r: trace.append({"steps": k, "residual": r}),
+                             restart=restart, max_cycles=max_cycles, tolerance=tolerance)
+    return x, {"reason": reason, "steps": steps, "residual": trace[-1]["residual"],
+               "seconds": time.perf_counter() - started, "dtype": str(rhs.dtype), "method": "gmres",
+               "trace": trace}
+
+
+def homogeneous_reference(geometry: DenseGeometry, frequencies, lines, tolerance=1e-4, device="cuda"):
+    """Reference pressure fields of the uniform medium (scripts/prepare_wave_teachers.py:22-35):
+    for every frequency and source line ``lines [n_freq, n_angles, w]``, GMRES(32)
+    on the uniform system with its own source.  Returns native fields
+    complex64 ``[n_angles, n_freq, h, w]``, the layout of the on-disk
+    ``reference/a{angle:02d}.npy`` arrays (nsrno/dense_wave.py:39-41)."""
+    g = geometry
+    lines = torch.as_tensor(lines, device=device)
+    n_freq, n_angles = lines.shape[:2]
+    out = torch.empty((n_angles, n_freq, g.h, g.w), dtype=torch.complex64, device=device)
+    for k, f in enumerate(frequencies):
+        s0 = homogeneous_system(g, f, device=device)
+        src = s0.source(lines[k].to(torch.complex128))
+        p, info = solve(s0, src, tolerance=tolerance, restart=32, max_cycles=80)
+        if info["reason"] != "converged":
+            raise RuntimeError(f"Homogeneous reference failed at {f} Hz: {info['trace'][-1]}")
+        out[:, k] = p[:, g.pz:g.pz + g.h, g.px:g.px + g.w].to(torch.complex64)
+    return out
+
+
+def save_reference(directory, fields):
+    """Write ``reference/a{angle:02d}.npy`` ([n_freq, h, w] complex64 each)."""
+    from pathlib import Path
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    for a in range(fields.shape[0]):
+        np.save(d / f"a{a:02d}.npy", fields[a].cpu().numpy())

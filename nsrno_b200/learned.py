@@ -211,8 +211,16 @@ def make_batch(medium: Medium, freqs, angles, with_target=True, tolerance=1e-6):
     if with_target:
         res = solve_batched(medium, freqs, angles, tolerance=tolerance, max_iterations=6000,
                             n_slots=int(freqs.numel()))
-        if res.reasons() != ["converged"] * int(freqs.numel()):
-            raise RuntimeError(f"target solve did not converge: {res.reasons()}")
+        bad = [k for k, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
+        if bad:
+            # GMRES for the systems BiCGSTAB did not converge (the fallback of solve_system)
+            from .solver import gmres_batched
+            idx = torch.as_tensor(bad, device=dev)
+            fb = gmres_batched(medium, freqs[idx], angles[idx], tolerance=tolerance, max_iterations=20000,
+                               restart=32, n_slots=len(bad))
+            if fb.reasons() != ["converged"] * len(bad):
+                raise RuntimeError(f"target solve did not converge: {fb.reasons()}")
+            res.iq[idx] = fb.iq
         target = res.iq
     return Batch(medium, freqs, angles, rhs, rx, target)
 
@@ -322,7 +330,7 @@ def training_media(n_media, nz, nx, seed0=100, device=None):
     return out
 
 
-def train(steps=1500, nz=256, nx=384, batch=4, krylov_steps=32, lr=3e-3, n_media=8, channel_weight=1.0, seed=0,
+def train(steps=2000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media=8, channel_weight=1.0, seed=0,
           device=None, log=print, params=None):
     """Train the learned preconditioner on seeded breast-like media (GPU).
 
@@ -363,11 +371,11 @@ def train(steps=1500, nz=256, nx=384, batch=4, krylov_steps=32, lr=3e-3, n_media
 
 def main():
     ap = argparse.ArgumentParser(description="Train the learned preconditioner on the GPU")
-    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--nz", type=int, default=256)
     ap.add_argument("--nx", type=int, default=384)
     ap.add_argument("--batch", type=int, default=4)
-    ap.add_argument("--krylov-steps", type=int, default=32)
+    ap.add_argument("--krylov-steps", type=int, default=48)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--media", type=int, default=8)
     ap.add_argument("--channel-weight", type=float, default=1.0)

@@ -139,3 +139,38 @@ class DenseSystem:
         value = (axis(self.ax, self.svx, self.gvx, self.mx, g.arx, g.Dx) +
                  axis(self.az, self.svz, self.gvz, self.mz, g.arz, g.Dz) + np.conj(self.mass) * y)
         return g.mask * value + (1 - g.mask) * p
+
+    def fixed_preconditioner(self, p, shift=0.15, adjoint=False):
+        """``mask IFFT(FFT(p) / (1 + lap/k0^2 - i shift))`` (conditioned_wave.py:90-92);
+        the adjoint solve conjugates the multiplier (dense_wave.py:195)."""
+        g = self.g
+        lap = -(np.abs(g.Dx) ** 2 + np.abs(g.Dz) ** 2)
+        m = 1.0 / (1.0 + lap / self.k0 ** 2 - 1j * shift)
+        if adjoint:
+            m = np.conj(m)
+        return g.mask * np.fft.ifft2(m * np.fft.fft2(p))
+
+    def source(self, line):
+        """Pressure source of a line on the array row (conditioned_wave.py:82-88)."""
+        g = self.g
+        zi, xi = g.spec["source_c_lookup_zx"]
+        source_c = self.c[zi + g.pz, xi + g.px]
+        line = np.atleast_2d(line)
+        profile = np.zeros((line.shape[0], g.H, g.W), dtype=np.complex128)
+        face = round(-g.spec["z0_m"] / g.dx) + g.pz
+        profile[:, face, g.px:g.px + line.shape[-1]] = line
+        return profile * self.a * C0 ** 2 * 2 * g.dt / (source_c * g.dx * (self.D - 1))
+
+
+def homogeneous(g: DenseGeometry, frequency):
+    """The uniform reference medium of the dense acquisition (dense_wave.py:53-55)."""
+    medium = np.stack((np.full((g.h, g.w), C0), np.full((g.h, g.w), RHO0)))
+    return DenseSystem(g, medium, np.full((g.h, g.w), 0.002), frequency)
+
+
+def assemble(system: DenseSystem, reference: DenseSystem, line, pref):
+    """``S(src) - S0(src) - A p_ref + A0 p_ref`` (dense_wave.py:46-57), pref [n, H, W]."""
+    out = system.source(line) - reference.source(line)
+    for k in range(pref.shape[0]):
+        out[k] += -system.apply(pref[k]) + reference.apply(pref[k])
+    return out

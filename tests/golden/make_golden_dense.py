@@ -10,6 +10,10 @@ grid, ``projected_operator(system, p)`` and ``adjoint_operator(system, p)``
 (nsrno/dense_wave.py:66-82, nsrno/conditioned_wave.py:52-80) restricted to the
 native (masked) region -- outside it both operators are the identity.
 The probe is ``default_rng(PROBE_SEED)`` normal real + 1j normal imag, [H, W].
+Also stored, at the first frequency: the fixed preconditioner of the probe,
+the acquisition right-hand side ``S(line) - S0(line) - A p_ref + A0 p_ref`` of
+seeded lines and masked reference fields, the source term alone, and a
+GMRES solve converged to 1e-10.
 """
 from __future__ import annotations
 
@@ -20,6 +24,7 @@ from pathlib import Path
 import numpy as np
 
 PROBE_SEED = 20261203
+ASSEMBLY_SEED = 77
 SPEC = {"medium_shape": [32, 40], "dx_m": 5e-5, "x0_m": -0.001, "z0_m": -0.0002, "native_dt_s": 2.5e-9,
         "pml": 6, "eta_per_unit_alpha": [0.012, 0.021], "taus_s": [2.0e-8, 1.5e-7],
         "source_c_lookup_zx": [10, 20]}
@@ -56,6 +61,31 @@ def main(reference_root):
         mask = np.zeros((g.H, g.W), bool)
         mask[inner] = True
         assert np.allclose(y[~mask], p[~mask]) and np.allclose(yh[~mask], p[~mask])
+    # Fixed preconditioner, acquisition assembly and a converged GMRES solve
+    # (nsrno/conditioned_wave.py:82-92, nsrno/dense_wave.py:46-62,
+    # nsrno/wave_solver.py:9-36) at the first frequency, complex128.
+    from nsrno.dense_wave import source_rhs
+    from nsrno.wave_solver import gmres
+    s = ConditionedFrequencySystem(g, medium, torch.tensor(alpha), FREQS[0])
+    out["precondition"] = s.fixed_preconditioner()(pt)[0].numpy()
+    uniform = torch.empty_like(medium)
+    uniform[0] = 1540.0
+    uniform[1] = 1000.0
+    s0 = ConditionedFrequencySystem(g, uniform, torch.full_like(torch.tensor(alpha), 0.002), FREQS[0])
+    arng = np.random.default_rng(ASSEMBLY_SEED)
+    line = torch.tensor(arng.standard_normal((2, w)) + 1j * arng.standard_normal((2, w)))
+    pref = torch.tensor(arng.standard_normal((2, g.H, g.W)) + 1j * arng.standard_normal((2, g.H, g.W)))
+    pref = pref * g.mask
+    rhs = source_rhs(s, line) - source_rhs(s0, line) - projected_operator(s, pref) + projected_operator(s0, pref)
+    out.update(assembly_line=line.numpy(), assembly_pref=pref.numpy(), assembly_rhs=rhs.numpy(),
+               source=source_rhs(s, line).numpy())
+    trace = []
+    b = rhs[:1]
+    x, reason = gmres(lambda v: projected_operator(s, v), s.fixed_preconditioner(), b, torch.zeros_like(b),
+                      lambda n, u, r: trace.append(r), restart=32, max_cycles=200, tolerance=1e-10)
+    assert reason == "converged", trace[-1]
+    out["solve_rhs"] = b.numpy()
+    out["solve_x"] = x.numpy()
     path = Path(__file__).resolve().parent / "reference_dense.npz"
     np.savez_compressed(path, **out)
     print(path, {k: np.shape(v) for k, v in out.items()})

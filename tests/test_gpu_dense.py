@@ -62,3 +62,78 @@ def test_dense_operator_matches_oracle_on_a_larger_grid(cuda):
         qy = np.vdot(q, y)
         aq = np.vdot(s.adjoint(torch.as_tensor(q, device=cuda)).cpu().numpy(), p)
         assert abs(qy - aq) / abs(qy) < 1e-12
+
+
+def dense_case(gold, cuda):
+    from nsrno_b200.dense import DenseGeometry, DenseSystem
+    g = DenseGeometry(json.loads(str(gold["spec"])))
+    return g, DenseSystem(g, gold["medium"], gold["alpha"], float(gold["freqs"][0]), device=cuda)
+
+
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_dense_preconditioner_matches_reference(cuda, gold, adjoint):
+    g, s = dense_case(gold, cuda)
+    prng = np.random.default_rng(int(gold["probe_seed"]))
+    p = prng.standard_normal((g.H, g.W)) + 1j * prng.standard_normal((g.H, g.W))
+    y = s.fixed_preconditioner(adjoint=adjoint)(torch.as_tensor(p, device=cuda)).cpu().numpy()
+    if adjoint:
+        o = D.DenseSystem(D.DenseGeometry(json.loads(str(gold["spec"]))), gold["medium"], gold["alpha"],
+                          float(gold["freqs"][0]))
+        assert rel(y, o.fixed_preconditioner(p, adjoint=True)) < 2e-5
+    else:
+        assert rel(y, gold["precondition"]) < 2e-5
+
+
+def test_dense_assembly_matches_reference(cuda, gold):
+    """S(src) - S0(src) - A p_ref + A0 p_ref (nsrno/dense_wave.py:46-57) on the device."""
+    from nsrno_b200.dense import assemble, homogeneous_system
+    g, s = dense_case(gold, cuda)
+    s0 = homogeneous_system(g, float(gold["freqs"][0]), device=cuda)
+    line = torch.as_tensor(gold["assembly_line"], device=cuda)
+    pref = torch.as_tensor(gold["assembly_pref"], device=cuda)
+    rhs = assemble(s, s0, line, pref).cpu().numpy()
+    assert rel(rhs, gold["assembly_rhs"]) < 1e-12
+    assert rel(s.source(line).cpu().numpy(), gold["source"]) < 1e-12
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-7), (torch.complex64, 1e-4)])
+def test_dense_gmres_solve_matches_reference(cuda, gold, dtype, tol):
+    """GMRES(32) with the fixed preconditioner on the dense operator against the
+    reference's own converged solve (nsrno/wave_solver.py:9-36)."""
+    from nsrno_b200.dense import solve
+    g, s = dense_case(gold, cuda)
+    b = torch.as_tensor(gold["solve_rhs"], device=cuda).to(dtype)
+    x, info = solve(s, b, tolerance=1e-9 if dtype == torch.complex128 else 1e-5, max_cycles=200)
+    assert info["reason"] == "converged"
+    assert rel(x.cpu().numpy(), gold["solve_x"]) < tol
+
+
+def test_dense_adjoint_solve(cuda, gold):
+    from nsrno_b200.dense import solve
+    g, s = dense_case(gold, cuda)
+    b = torch.as_tensor(gold["solve_rhs"], device=cuda)
+    x, info = solve(s, b, adjoint=True, tolerance=1e-9, max_cycles=200)
+    assert info["reason"] == "converged"
+    r = s.adjoint(x) - b
+    assert float(r.norm() / b.norm()) < 1e-9
+
+
+def test_homogeneous_reference_fields(cuda, gold, tmp_path):
+    """Uniform-medium reference fields in the on-disk layout reference/a{angle:02d}.npy
+    [bins, h, w] (nsrno/dense_wave.py:39-41, scripts/prepare_wave_teachers.py:22-35)."""
+    from nsrno_b200.dense import DenseGeometry, homogeneous_reference, save_reference
+    g = DenseGeometry(json.loads(str(gold["spec"])))
+    freqs = [float(f) for f in gold["freqs"]]
+    lines = np.broadcast_to(gold["assembly_line"], (2,) + gold["assembly_line"].shape).copy()
+    fields = homogeneous_reference(g, freqs, lines, tolerance=1e-6, device=cuda)
+    assert fields.shape == (2, 2, g.h, g.w) and fields.dtype == torch.complex64
+    og = D.DenseGeometry(json.loads(str(gold["spec"])))
+    for k, f in enumerate(freqs):
+        s0 = D.homogeneous(og, f)
+        src = s0.source(lines[k])
+        for a in range(2):
+            p = np.zeros((og.H, og.W), complex)
+            p[og.pz:og.pz + og.h, og.px:og.px + og.w] = fields[a, k].cpu().numpy()
+            assert rel(s0.apply(p), src[a]) < 1e-5
+    save_reference(tmp_path, fields)
+    assert np.load(tmp_path / "a01.npy").shape == (2, g.h, g.w)

@@ -174,3 +174,18 @@ def test_warm_start_gate_discards_bad_initial_fields(cuda):
     assert torch.equal(bad.iq, cold.iq)
     ok = solve_batched(med, f[:3], th[:3], tolerance=1e-6, x0=noise, warm_gate=0.0)
     assert ok.extra["stats"]["warm_accepted"] == 3 and ok.reasons() == ["converged"] * 3
+
+
+def test_growing_residual_restarts(cuda):
+    """The one system of 24,000 training-media solves whose FP32 recurrence ran
+    away (relative residual 1.3e5 at iteration 320) converges once a growing
+    true residual restarts the recurrence."""
+    from nsrno_b200 import Geometry, Medium, solve_batched
+    from nsrno_b200.media import breast_record
+    rec = breast_record(seed=106, nz=256, nx=384, n_rx=88, rx_pitch=4)
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=cuda)
+    f = [8796334.860474803] * 2
+    th = [0.17115545431964527, -0.2]
+    res = solve_batched(med, f, th, tolerance=1e-6, max_iterations=6000, n_slots=2)
+    assert res.reasons() == ["converged"] * 2
+    assert float(res.residual.max()) < 1e-6

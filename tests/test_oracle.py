@@ -211,3 +211,24 @@ def test_operator_derivative_against_central_differences():
     up = H.solve_lu(H.operator(spec, c * np.exp(eps * dc), rho * np.exp(eps * dr), alpha, f), b)
     um = H.solve_lu(H.operator(spec, c * np.exp(-eps * dc), rho * np.exp(-eps * dr), alpha, f), b)
     assert rel(du, (up - um) / (2 * eps)) < 1e-6
+
+
+def test_dense_oracle_preconditioner_and_assembly_match_reference():
+    """Fixed preconditioner, source and assembled right-hand side of the dense
+    oracle against the reference's own output (complex128)."""
+    import json
+    from conftest import GOLDEN
+    from oracle import dense_ref as D
+    with np.load(GOLDEN / "reference_dense.npz") as z:
+        gold = {k: z[k] for k in z.files}
+    g = D.DenseGeometry(json.loads(str(gold["spec"])))
+    prng = np.random.default_rng(int(gold["probe_seed"]))
+    p = prng.standard_normal((g.H, g.W)) + 1j * prng.standard_normal((g.H, g.W))
+    s = D.DenseSystem(g, gold["medium"], gold["alpha"], float(gold["freqs"][0]))
+    assert rel(s.fixed_preconditioner(p), gold["precondition"]) < 1e-12
+    assert rel(s.source(gold["assembly_line"]), gold["source"]) < 1e-12
+    s0 = D.homogeneous(g, float(gold["freqs"][0]))
+    rhs = D.assemble(s, s0, gold["assembly_line"], gold["assembly_pref"])
+    assert rel(rhs, gold["assembly_rhs"]) < 1e-12
+    x = gold["solve_x"][0]
+    assert rel(s.apply(x), gold["solve_rhs"][0]) < 1e-9
