@@ -303,6 +303,14 @@ int nsr_dense_precondition(const NsrDenseGrid* grid, double k0dx2, double shift,
                            int32_t adjoint, const float* x, float* y, void* workspace, size_t workspace_bytes,
                            void* stream);
 
+/* Band-limited RF traces rf[ch][t] (double) from receiver spectra
+ * spectrum[ch][b] (c128) on positive bins 0 < bins[b] < n_samples/2:
+ * the irfft with 'forward' normalisation of predict_band_rf
+ * (nsrno/wave_operator.py:169-180).  Bins must be valid (checked by the
+ * host wrapper); a spectrum with no bins gives zero traces. */
+int nsr_band_rf(int32_t n_channels, int32_t n_bins, int32_t n_samples, const double* spectrum,
+                const int32_t* bins, double* rf, void* stream);
+
 /* ---- Learned preconditioner: inference -------------------------------- */
 
 /* Bytes of the low-resolution network state of n_freq frequencies. */

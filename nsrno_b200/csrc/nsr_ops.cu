@@ -502,3 +502,43 @@ extern "C" int nsr_tangent_rhs(const NsrGrid* grid, const void* coef, const doub
                                            (double2*)rhs);
   return last_error();
 }
+
+// ---------------------------------------------------------------------------
+// Band-limited RF traces from receiver spectra (predict_band_rf,
+// nsrno/wave_operator.py:169-180): the inverse real DFT with 'forward'
+// normalisation of a spectrum that is zero except on the given positive bins,
+//   x[t] = sum_b 2 Re(S[b] exp(2 pi i k_b t / n)),   0 < k_b < n/2.
+// The phase k_b t is reduced modulo n in integers, so every term is exact to
+// double rounding whatever the trace length.
+// ---------------------------------------------------------------------------
+__global__ void k_band_rf(int n_ch, int n_bins, int n, const double2* __restrict__ spec,
+                          const int* __restrict__ bins, double* __restrict__ out) {
+  const int ch = blockIdx.y;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int b = 0; b < n_bins; ++b) {
+      const long long m = ((long long)bins[b] * t) % n;
+      double sn, cs;
+      sincospi(2.0 * (double)m / (double)n, &sn, &cs);
+      const double2 s = spec[(long long)ch * n_bins + b];
+      acc += 2.0 * (s.x * cs - s.y * sn);
+    }
+    out[(long long)ch * n + t] = acc;
+  }
+}
+
+extern "C" int nsr_band_rf(int32_t n_channels, int32_t n_bins, int32_t n_samples, const double* spectrum,
+                           const int32_t* bins, double* rf, void* stream) {
+  if (n_channels < 0 || n_bins < 0 || n_samples <= 0 || n_channels > 65535 || !rf ||
+      (n_bins > 0 && (!spectrum || !bins)))
+    return NSR_ERR_ARGUMENT;
+  if (n_channels == 0) return 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_bins == 0) {
+    cudaError_t e = cudaMemsetAsync(rf, 0, sizeof(double) * (size_t)n_channels * n_samples, st);
+    return e == cudaSuccess ? 0 : (int)e;
+  }
+  const int bx = (n_samples + 255) / 256;
+  k_band_rf<<<dim3(bx, n_channels), 256, 0, st>>>(n_channels, n_bins, n_samples, (const double2*)spectrum, bins, rf);
+  return last_error();
+}

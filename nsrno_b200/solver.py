@@ -375,3 +375,37 @@ def receiver_response(frequency, dt=2.5e-9):
     omega = 2 * np.pi * frequency * dt
     _, fir = freqz(taps, worN=[omega])
     return float(abs(h[0]) ** 2 * (fir[0] * np.exp(1j * omega * half_len)).real)
+
+
+def band_rf(spectrum, bins, n_samples=2401):
+    """Band-limited RF traces ``[n_channels, n_samples]`` (float64) from receiver
+    spectra ``[n_channels, n_bins]`` on positive bins (predict_band_rf,
+    nsrno/wave_operator.py:169-180: ``irfft`` with 'forward' normalisation of a
+    spectrum that is zero elsewhere).  Raises ``ValueError('Positive RF bin out
+    of range')`` like the reference."""
+    spectrum = torch.as_tensor(spectrum)
+    _require_cuda(spectrum, "spectrum")
+    bins_np = np.asarray(bins, dtype=np.int64).reshape(-1)
+    if spectrum.dim() != 2 or spectrum.shape[1] != bins_np.size:
+        raise ValueError("spectrum must be [n_channels, n_bins]")
+    if ((bins_np <= 0) | (2 * bins_np >= n_samples)).any():
+        raise ValueError("Positive RF bin out of range")
+    spec = spectrum.to(torch.complex128).contiguous()
+    b = torch.as_tensor(bins_np.astype(np.int32), device=spec.device)
+    out = torch.empty((spec.shape[0], int(n_samples)), dtype=torch.float64, device=spec.device)
+    _lib.check(_lib.load().nsr_band_rf(spec.shape[0], int(bins_np.size), int(n_samples), _ptr(spec), _ptr(b),
+                                       _ptr(out), _stream()))
+    return out
+
+
+def receiver_rf(iq, frequency_bins, response=True, n_samples=2401, clock_hz=40e6):
+    """RF traces of the receiver IQ of a record's bins: ``iq [n_bins, n_channels]``
+    times the receive response of each bin (nsrno/conditioned_data.py:10-24),
+    then :func:`band_rf`."""
+    iq = torch.as_tensor(iq)
+    bins = np.asarray(frequency_bins, dtype=np.int64).reshape(-1)
+    if response:
+        r = torch.as_tensor([receiver_response(float(k) * clock_hz / n_samples) for k in bins],
+                            dtype=torch.float64, device=iq.device)
+        iq = iq.to(torch.complex128) * r[:, None]
+    return band_rf(iq.transpose(0, 1), bins, n_samples)

@@ -143,3 +143,19 @@ def test_grad_accum_matches_oracle(cuda, dtype):
         ref_r += r_
     assert rel(gc.cpu().numpy(), ref_c) < 1e-12
     assert rel(gr.cpu().numpy(), ref_r) < 1e-12
+
+
+def test_band_rf_matches_irfft(cuda):
+    """predict_band_rf (nsrno/wave_operator.py:169-180): irfft(n=2401, norm='forward')
+    of a spectrum that is zero except on the given bins."""
+    from nsrno_b200 import band_rf
+    rng = np.random.default_rng(4)
+    bins = np.array([241, 300, 377, 534, 1000])
+    spec = rng.standard_normal((6, bins.size)) + 1j * rng.standard_normal((6, bins.size))
+    full = np.zeros((6, 1201), complex)
+    full[:, bins] = spec
+    want = np.fft.irfft(full, n=2401, axis=-1, norm="forward")
+    got = band_rf(torch.as_tensor(spec, device=cuda), bins).cpu().numpy()
+    assert rel(got, want) < 1e-12
+    with pytest.raises(ValueError, match="Positive RF bin out of range"):
+        band_rf(torch.as_tensor(spec, device=cuda), np.array([0, 300, 377, 534, 1000]))
