@@ -375,13 +375,18 @@ __device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __rest
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
+      // The stage with m == 1 (the last forward, first inverse) has unit twiddles.
       if (!INV) {
         small_dft<R, false>(v[u]);
+        if constexpr (m > 1) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * __ldg(&tw[jj[u] * k * tstep]);
+          for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * __ldg(&tw[jj[u] * k * tstep]);
+        }
       } else {
+        if constexpr (m > 1) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * conjc(__ldg(&tw[jj[u] * k * tstep]));
+          for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * conjc(__ldg(&tw[jj[u] * k * tstep]));
+        }
         small_dft<R, true>(v[u]);
       }
     }
@@ -404,6 +409,19 @@ __device__ __forceinline__ void ct_forward(float2* s, int nl, const float2* __re
     ct_stage<N, R, L, false, LF, LS, ES, PAD>(s, nl, tw);
     __syncthreads();
     ct_forward<N, S + 1, LF, LS, ES, PAD>(s, nl, tw);
+  }
+}
+
+// Forward stages S .. STOP-1.
+template <int N, int S, int STOP, bool LF, int LS, int ES, bool PAD>
+__device__ __forceinline__ void ct_forward_upto(float2* s, int nl, const float2* __restrict__ tw) {
+  if constexpr (S < STOP) {
+    constexpr RadixList RL = nsr_radix_list(N);
+    constexpr int R = RL.r[S];
+    constexpr int L = nsr_stage_len(N, S);
+    ct_stage<N, R, L, false, LF, LS, ES, PAD>(s, nl, tw);
+    __syncthreads();
+    ct_forward_upto<N, S + 1, STOP, LF, LS, ES, PAD>(s, nl, tw);
   }
 }
 
@@ -465,6 +483,53 @@ __device__ void fft_cols(float2* s, const FftPlan& P) {
     case 1536: ct_fft<1536, INV, true, 1, TC, false>(s, TC, P.tw); return;
     case 2048: ct_fft<2048, INV, true, 1, TC, false>(s, TC, P.tw); return;
     default: fft_lines<INV>(s, TC, 1, TC, true, P); return;
+  }
+}
+
+// Forward column FFT, a pointwise multiply in the digit-reversed domain and the
+// inverse column FFT, with the last forward stage, the multiply and the first
+// inverse stage done in registers in one shared-memory pass (that stage has
+// m == 1: contiguous groups of R elements and unit twiddles).  `mul(l, k)`
+// returns the factor of line l (column of the tile) at digit-reversed position k.
+template <int N, int TC, typename MUL>
+__device__ __forceinline__ void ct_cols_fused(float2* s, const float2* __restrict__ tw, MUL mul) {
+  constexpr RadixList RL = nsr_radix_list(N);
+  constexpr int LAST = RL.nst - 1;
+  constexpr int R = RL.r[LAST];
+  if constexpr (LAST > 0) ct_forward_upto<N, 0, LAST, true, 1, TC, false>(s, TC, tw);
+  constexpr int per_line = N / R;
+  const int nb = TC * per_line;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    const int l = b % TC, o = b / TC;
+    float2* base = s + l + o * R * TC;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = base[q * TC];
+    small_dft<R, false>(v);
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = v[q] * mul(l, o * R + q);
+    small_dft<R, true>(v);
+#pragma unroll
+    for (int q = 0; q < R; ++q) base[q * TC] = v[q];
+  }
+  __syncthreads();
+  if constexpr (LAST > 0) ct_inverse<N, LAST - 1, true, 1, TC, false>(s, TC, tw);
+}
+
+// Column pass with the fused middle stage for the specialised sizes; other
+// sizes run the separate transforms and multiply.  Returns false for those
+// other sizes, which the caller then handles itself.
+template <int TC, typename MUL>
+__device__ __forceinline__ bool fft_cols_fused(float2* s, const FftPlan& P, MUL mul) {
+  switch (P.n) {
+    case 256: ct_cols_fused<256, TC>(s, P.tw, mul); return true;
+    case 384: ct_cols_fused<384, TC>(s, P.tw, mul); return true;
+    case 512: ct_cols_fused<512, TC>(s, P.tw, mul); return true;
+    case 768: ct_cols_fused<768, TC>(s, P.tw, mul); return true;
+    case 1024: ct_cols_fused<1024, TC>(s, P.tw, mul); return true;
+    case 1536: ct_cols_fused<1536, TC>(s, P.tw, mul); return true;
+    case 2048: ct_cols_fused<2048, TC>(s, P.tw, mul); return true;
+    default: return false;
   }
 }
 

@@ -126,35 +126,59 @@ __device__ __forceinline__ void cols_pass(float2* sm, const Geo& g, const PrecTa
     sm[k] = c < ncol ? ws[(long long)z * g.nx + c0 + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_cols<false, TC>(sm, tab.pz);
   const SysScalars s = sys_scalars(g, freq);
   const float kh2 = (float)s.kh2;
   const float inv_n = 1.0f / (float)n;
   const float2 shiftc = make_float2(kh2, (float)(s.kh2 * shift));
+  bool fused;
   if (lp) {
-    const LearnedSpec L = load_learned_spec(lp);
+    // The spectral parameters go through shared memory so that the fused
+    // radix stage keeps its registers for the butterfly.
+    __shared__ LearnedSpec Ls;
+    if (threadIdx.x == 0) Ls = load_learned_spec(lp);
+    __syncthreads();
     const float h2 = (float)(g.h * g.h);
-    for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-      const int z = k / TC, c = k - z * TC;
-      if (c < ncol) {
-        float2 mul = inv_n * learned_symbol(L, tab.s2z[z], tab.s2x[c0 + c], kh2, h2);
-        if (adjoint) mul = conjc(mul);
-        sm[k] = sm[k] * mul;
-      }
-    }
+    fused = fft_cols_fused<TC>(sm, tab.pz, [&](int c, int z) -> float2 {
+      if (c >= ncol) return make_float2(0.f, 0.f);
+      const float2 mul = inv_n * learned_symbol(Ls, tab.s2z[z], tab.s2x[c0 + c], kh2, h2);
+      return adjoint ? conjc(mul) : mul;
+    });
   } else {
-    for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-      const int z = k / TC, c = k - z * TC;
-      if (c < ncol) {
-        const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
-        float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
-        if (adjoint) mul = conjc(mul);
-        sm[k] = sm[k] * mul;
+    fused = fft_cols_fused<TC>(sm, tab.pz, [&](int c, int z) -> float2 {
+      if (c >= ncol) return make_float2(0.f, 0.f);
+      const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
+      const float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
+      return adjoint ? conjc(mul) : mul;
+    });
+  }
+  if (!fused) {
+    // Sizes without a specialised transform: separate passes.
+    fft_cols<false, TC>(sm, tab.pz);
+    if (lp) {
+      const LearnedSpec L = load_learned_spec(lp);
+      const float h2 = (float)(g.h * g.h);
+      for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+        const int z = k / TC, c = k - z * TC;
+        if (c < ncol) {
+          float2 mul = inv_n * learned_symbol(L, tab.s2z[z], tab.s2x[c0 + c], kh2, h2);
+          if (adjoint) mul = conjc(mul);
+          sm[k] = sm[k] * mul;
+        }
+      }
+    } else {
+      for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+        const int z = k / TC, c = k - z * TC;
+        if (c < ncol) {
+          const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
+          float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
+          if (adjoint) mul = conjc(mul);
+          sm[k] = sm[k] * mul;
+        }
       }
     }
+    __syncthreads();
+    fft_cols<true, TC>(sm, tab.pz);
   }
-  __syncthreads();
-  fft_cols<true, TC>(sm, tab.pz);
   for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
     const int z = k / TC, c = k - z * TC;
     if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];

@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
 // cols: column FFT, preconditioner multiply, inverse column FFT (in place).
 // ---------------------------------------------------------------------------
 template <int TC>
-__global__ void __launch_bounds__(512) k_cols(SolveArgs A, int half) {
+__global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
   const int slot = blockIdx.y;
   const int mode = A.B.slots[slot].mode;
