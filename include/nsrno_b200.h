@@ -311,6 +311,16 @@ int nsr_dense_precondition(const NsrDenseGrid* grid, double k0dx2, double shift,
 int nsr_band_rf(int32_t n_channels, int32_t n_bins, int32_t n_samples, const double* spectrum,
                 const int32_t* bins, double* rf, void* stream);
 
+/* FP64 true relative residual ||b - A x|| / ||b|| (or A^H) of n_systems c128
+ * fields x; b is rhs (c128, SI) or, when rhs is NULL, the plane-wave source of
+ * (freq, angle).  Deterministic order of summation.  Replaces the acceptance
+ * residual of nsrno/dense_wave.py:146-147,221-225 and the diagnostics of
+ * theranostic/wave.py:320-323. */
+size_t nsr_true_residual_workspace_size(const NsrGrid* grid, int32_t n_systems);
+int nsr_true_residual(const NsrGrid* grid, const void* coef, const double* freq_hz, const double* angle_rad,
+                      int32_t n_systems, int32_t adjoint, const double* x, const double* rhs, double* residual,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- Learned preconditioner: inference -------------------------------- */
 
 /* Bytes of the low-resolution network state of n_freq frequencies. */

@@ -8,7 +8,7 @@ compute runs in hand-written sm_100a CUDA kernels behind the C ABI of
 """
 from . import _lib
 from .solver import (BatchResult, Geometry, Medium, Workspace, apply, gmres_batched, grad_accum, plane_wave_rhs,
-                     precondition, receiver_response, solve_batched, band_rf, receiver_rf)
+                     precondition, receiver_response, solve_batched, band_rf, receiver_rf, true_residual)
 from .learned import LearnedPreconditioner, LearnedSetup, learned_precondition, warm_start
 from .api import (AcquisitionData, HelmholtzSurrogate, HelmholtzSystem, ImplicitChannels, PlaneWaveModel,
                   bin_frequency, implicit_channels, solve_frequency, solve_system)
@@ -17,4 +17,4 @@ __all__ = ["BatchResult", "Geometry", "Medium", "Workspace", "apply", "gmres_bat
            "precondition", "receiver_response", "solve_batched", "AcquisitionData", "HelmholtzSurrogate",
            "HelmholtzSystem", "ImplicitChannels", "PlaneWaveModel", "bin_frequency", "implicit_channels",
            "solve_frequency", "solve_system", "LearnedPreconditioner", "LearnedSetup", "learned_precondition",
-           "warm_start", "band_rf", "receiver_rf"]
+           "warm_start", "band_rf", "receiver_rf", "true_residual"]

@@ -22,7 +22,8 @@ EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_m
            "nsr_learned_state_bytes", "nsr_learned_setup", "nsr_learned_precondition",
            "nsr_learned_backward_workspace_size", "nsr_learned_map_backward", "nsr_learned_network_backward",
            "nsr_learned_spectral_workspace_size", "nsr_learned_spectral_backward", "nsr_learned_adam",
-           "nsr_tangent_rhs", "nsr_dense_precondition_workspace_size", "nsr_dense_precondition", "nsr_band_rf")
+           "nsr_tangent_rhs", "nsr_dense_precondition_workspace_size", "nsr_dense_precondition", "nsr_band_rf",
+           "nsr_true_residual_workspace_size", "nsr_true_residual")
 
 LEARNED_PARAMS = 3645
 
@@ -108,6 +109,9 @@ def load():
     lib.nsr_grad_accum.argtypes = [G, P, P, I, I, P, P, P, P, P]
     lib.nsr_tangent_rhs.argtypes = [G, P, P, I, I, P, P, P, P, P]
     lib.nsr_band_rf.argtypes = [I, I, I, P, P, P, P]
+    lib.nsr_true_residual_workspace_size.restype = S
+    lib.nsr_true_residual_workspace_size.argtypes = [G, I]
+    lib.nsr_true_residual.argtypes = [G, P, P, P, I, I, P, P, P, P, S, P]
     lib.nsr_gmres_workspace_size.restype = S
     lib.nsr_gmres_workspace_size.argtypes = [G, I, I]
     lib.nsr_gmres_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrGmresParams),

@@ -542,3 +542,100 @@ extern "C" int nsr_band_rf(int32_t n_channels, int32_t n_bins, int32_t n_samples
   k_band_rf<<<dim3(bx, n_channels), 256, 0, st>>>(n_channels, n_bins, n_samples, (const double2*)spectrum, bins, rf);
   return last_error();
 }
+
+// ---------------------------------------------------------------------------
+// FP64 true relative residual ||b - A x|| / ||b|| of n_systems fields
+// (the acceptance check of nsrno/dense_wave.py:146-147,221-225 and
+// theranostic/wave.py:320-323).  b is the given SI right-hand side or, when
+// rhs is null, the plane-wave source of (freq, angle).  Per-CTA partials are
+// summed in CTA order by a second kernel, so the result is deterministic.
+// ---------------------------------------------------------------------------
+#define NSR_TR_BLOCKS 256
+__global__ void __launch_bounds__(256) k_true_residual(Geo g, const void* __restrict__ mat,
+                                                       const double* __restrict__ freq,
+                                                       const double* __restrict__ angle,
+                                                       const double2* __restrict__ x, const double2* __restrict__ rhs,
+                                                       int adjoint, double* __restrict__ partials) {
+  const long long n = (long long)g.nz * g.nx;
+  const int sidx = blockIdx.y;
+  const SysScalars s = sys_scalars(g, freq[sidx]);
+  const MatPlanes mp = nsr_planes(mat, n);
+  const double2* xs = x + sidx * n;
+  const double st = angle ? sin(angle[sidx]) : 0.0;
+  const double h2 = g.h * g.h;
+  double rr = 0.0, bb = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.nx), j = (int)(k - (long long)i * g.nx);
+    auto P = [&](int i2, int j2) -> double2 {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return make_double2(0.0, 0.0);
+      return xs[(long long)i2 * g.nx + j2];
+    };
+    auto Aa = [&](int i2, int j2) -> double {
+      if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= g.nx) return 1.0;
+      return mp.a64[(long long)i2 * g.nx + j2];
+    };
+    double2 b;
+    if (rhs) {
+      b = h2 * rhs[sidx * n + k];
+    } else if (i == g.face) {
+      const double2 l = source_line(g, s.k0, st, j);
+      b = make_double2(-l.x, -l.y);
+    } else {
+      b = make_double2(0.0, 0.0);
+    }
+    const double2 ax = adjoint ? stencil<double, true>(g, s, i, j, mp.b64[k], mp.t64[k], P, Aa)
+                               : stencil<double, false>(g, s, i, j, mp.b64[k], mp.t64[k], P, Aa);
+    const double2 r = b - ax;
+    rr += r.x * r.x + r.y * r.y;
+    bb += b.x * b.x + b.y * b.y;
+  }
+  __shared__ double wr[8], wb[8];
+  for (int o = 16; o > 0; o >>= 1) {
+    rr += __shfl_xor_sync(0xffffffffu, rr, o);
+    bb += __shfl_xor_sync(0xffffffffu, bb, o);
+  }
+  if ((threadIdx.x & 31) == 0) { wr[threadIdx.x >> 5] = rr; wb[threadIdx.x >> 5] = bb; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tr = 0.0, tb = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tr += wr[w]; tb += wb[w]; }
+    partials[((long long)sidx * gridDim.x + blockIdx.x) * 2] = tr;
+    partials[((long long)sidx * gridDim.x + blockIdx.x) * 2 + 1] = tb;
+  }
+}
+
+__global__ void k_true_residual_sum(int n_systems, int nb, const double* __restrict__ partials,
+                                    double* __restrict__ residual) {
+  const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sidx >= n_systems) return;
+  double rr = 0.0, bb = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    rr += partials[((long long)sidx * nb + b) * 2];
+    bb += partials[((long long)sidx * nb + b) * 2 + 1];
+  }
+  residual[sidx] = bb > 0.0 ? sqrt(rr / bb) : sqrt(rr);
+}
+
+extern "C" size_t nsr_true_residual_workspace_size(const NsrGrid* grid, int32_t n_systems) {
+  if (nsr_check_grid(grid, false) || n_systems <= 0 || n_systems > 65535) return 0;
+  return nsr_align(sizeof(double) * 2 * NSR_TR_BLOCKS * (size_t)n_systems);
+}
+
+extern "C" int nsr_true_residual(const NsrGrid* grid, const void* coef, const double* freq_hz,
+                                 const double* angle_rad, int32_t n_systems, int32_t adjoint, const double* x,
+                                 const double* rhs, double* residual, void* workspace, size_t workspace_bytes,
+                                 void* stream) {
+  int err = nsr_check_grid(grid, false);
+  if (err) return err;
+  if (!coef || !freq_hz || !x || !residual || !workspace || n_systems < 0 || n_systems > 65535) return NSR_ERR_ARGUMENT;
+  if (!rhs && !angle_rad) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;
+  if (workspace_bytes < nsr_true_residual_workspace_size(grid, n_systems)) return NSR_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  double* partials = (double*)workspace;
+  k_true_residual<<<dim3(NSR_TR_BLOCKS, n_systems), 256, 0, st>>>(make_geo(*grid), coef, freq_hz,
+                                                                   rhs ? nullptr : angle_rad, (const double2*)x,
+                                                                   (const double2*)rhs, adjoint ? 1 : 0, partials);
+  k_true_residual_sum<<<(n_systems + 127) / 128, 128, 0, st>>>(n_systems, NSR_TR_BLOCKS, partials, residual);
+  return last_error();
+}

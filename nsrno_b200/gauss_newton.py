@@ -186,6 +186,15 @@ def main():
     out = gn.step()
     out.pop("update")
     fw = gn.forward_result
+    # FP64 spot checks: 8 systems spread over the band re-solved to a 1e-10 FP64
+    # true residual; the receiver IQ of the 1e-6 forward solves against them.
+    spot = np.unique(np.linspace(0, len(f) - 1, 8).round().astype(int))
+    ref = solve_batched(med, f[spot], th[spot], tolerance=1e-10, max_iterations=20000, n_slots=len(spot),
+                        learned=gn.setup)
+    _require_converged(ref, "FP64 spot check")
+    diff = (fw.iq[torch.as_tensor(spot, device=dev)] - ref.iq).norm(dim=1) / ref.iq.norm(dim=1)
+    out.update(spot_systems=spot.tolist(), spot_iq_rel_error_max=float(diff.max()),
+               spot_iq_rel_error_mean=float(diff.mean()), spot_residual_max=float(ref.residual.max()))
     out.update(grid_zx=[a.nz, a.nx], h=a.h, systems=len(f), bins=len(pick), angles=a.angles,
                preconditioner="fixed" if a.fixed else "learned", observed_data_seconds=t_obs,
                solves_per_step=4 * len(f), solves_per_second=4 * len(f) / out["seconds"],

@@ -242,7 +242,6 @@ def loss_and_grad(params: torch.Tensor, batch: Batch, steps: int, channel_weight
     pre.params = params
     setup = pre.setup(med, batch.freqs)
     inner, outer = setup.gains[:, 0], setup.gains[:, 1]
-    gidx = torch.arange(S, dtype=torch.int32, device=params.device)
     core = lambda v, adj=False: learned_precondition(med, None, v, batch.freqs, adjoint=adj, params=params)
     b = batch.rhs
     r = b.clone()
@@ -297,7 +296,6 @@ def loss_and_grad(params: torch.Tensor, batch: Batch, steps: int, channel_weight
                                             _ptr(g_out.contiguous()), _ptr(d_maps), _ptr(bw), bw_bytes, _stream()))
     _lib.check(lib.nsr_learned_network_backward(grid, _ptr(params), _ptr(setup.state), S, _ptr(d_maps), _ptr(grad),
                                                 _ptr(bw), bw_bytes, _stream()))
-    del gidx
     return float(loss_sys.mean()), grad, [float(v) for v in loss_sys]
 
 

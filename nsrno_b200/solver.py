@@ -409,3 +409,27 @@ def receiver_rf(iq, frequency_bins, response=True, n_samples=2401, clock_hz=40e6
                             dtype=torch.float64, device=iq.device)
         iq = iq.to(torch.complex128) * r[:, None]
     return band_rf(iq.transpose(0, 1), bins, n_samples)
+
+
+def true_residual(medium: Medium, x: torch.Tensor, freqs, angles=None, rhs=None, adjoint=False):
+    """FP64 true relative residuals ``||b - A x|| / ||b||`` [S] of fields x [S, nz, nx]
+    (``nsr_true_residual``); ``b`` is ``rhs`` (SI) or the plane-wave source of (freqs, angles)."""
+    g = medium.geometry
+    _require_cuda(x, "x")
+    if x.dim() != 3 or tuple(x.shape[1:]) != (g.nz, g.nx) or not x.is_complex():
+        raise ValueError("x must be complex [S, nz, nx]")
+    dev = x.device
+    x = x.to(torch.complex128).contiguous()
+    S = x.shape[0]
+    freqs = torch.as_tensor(freqs, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+    if rhs is None and angles is None:
+        raise ValueError("either angles or rhs must be given")
+    ang = None if angles is None else torch.as_tensor(angles, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+    b = None if rhs is None else torch.as_tensor(rhs).to(dev, torch.complex128).contiguous()
+    lib = _lib.load()
+    nbytes = lib.nsr_true_residual_workspace_size(ctypes.byref(medium._grid), S)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = torch.empty(S, dtype=torch.float64, device=dev)
+    _lib.check(lib.nsr_true_residual(ctypes.byref(medium._grid), _ptr(medium.material), _ptr(freqs), _ptr(ang), S,
+                                     int(bool(adjoint)), _ptr(x), _ptr(b), _ptr(out), _ptr(ws), nbytes, _stream()))
+    return out

@@ -159,3 +159,29 @@ def test_band_rf_matches_irfft(cuda):
     assert rel(got, want) < 1e-12
     with pytest.raises(ValueError, match="Positive RF bin out of range"):
         band_rf(torch.as_tensor(spec, device=cuda), np.array([0, 300, 377, 534, 1000]))
+
+
+def test_true_residual_matches_oracle(cuda):
+    """nsr_true_residual against the oracle's relative residual, plane-wave and given rhs, forward and adjoint."""
+    from nsrno_b200 import Geometry, Medium, true_residual
+    from nsrno_b200.media import blob_record
+    rec = blob_record(nz=48, nx=64, n_pml=6, h=2e-4, n_blobs=2, frequencies=(0.8e6,), n_rx=16)
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=cuda)
+    spec = spec_of(rec)
+    a, b, t = med.coef64.cpu().numpy()
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((2, rec.nz, rec.nx)) + 1j * rng.standard_normal((2, rec.nz, rec.nx))
+    f = [0.8e6, 0.8e6]
+    th = [0.1, -0.2]
+    got = true_residual(med, torch.as_tensor(x, device=cuda), f, th).cpu().numpy()
+    A = H.operator_planes(spec, a, b, t, 0.8e6)
+    for s in range(2):
+        want = H.relative_residual(A, x[s].ravel(), H.plane_wave_rhs(spec, f[s], th[s]))
+        assert abs(got[s] - want) < 1e-12 * want
+    rhs = rng.standard_normal((2, rec.nz, rec.nx)) + 1j * rng.standard_normal((2, rec.nz, rec.nx))
+    got = true_residual(med, torch.as_tensor(x, device=cuda), f, rhs=torch.as_tensor(rhs, device=cuda),
+                        adjoint=True).cpu().numpy()
+    AH = A.conj().T.tocsr()
+    for s in range(2):
+        want = H.relative_residual(AH, x[s].ravel(), rhs[s].ravel())
+        assert abs(got[s] - want) < 1e-12 * want
