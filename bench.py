@@ -70,6 +70,8 @@ def parse():
     p.add_argument("--cpu-sample-bins", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-Krylov comparison arm")
+    p.add_argument("--plain-only", action="store_true",
+                   help="run only the plain-Krylov arm (for profiling it); prints a short line, not the bench line")
     return p.parse_args()
 
 
@@ -315,6 +317,16 @@ def run_ours(args):
                             "iterations_mean": float(iters.mean()), "iterations_max": int(iters.max()),
                             "residual_max": float(resid.max())})
 
+    if args.plain_only:
+        ms_p, res_p, _ = timed(False)
+        P = summarise(ms_p, res_p, KERNEL_BYTES)
+        if rank == 0:
+            print(json.dumps({"arm": "plain", "value": P["value"], "unit": UNIT, "kernel_ms": P["kms"],
+                              "solves": P["solves"]}), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     ms_l, res_l, clock_info = timed(True, sample_clocks=True)
     L = summarise(ms_l, res_l, LEARNED_BYTES)
     P = None

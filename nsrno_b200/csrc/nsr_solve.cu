@@ -32,7 +32,7 @@
 enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES = 4, MODE_EMIT = 5 };
 
 #define NSR_LAUNCHES_PER_IT 9
-#define NSR_ST_TZ 16      // rows of one stencil CTA
+#define NSR_ST_TZ 32      // rows of one stencil CTA
 #define NSR_ST_TX 256     // columns of one stencil CTA (one per thread)
 
 struct __align__(16) SlotState {
@@ -93,6 +93,7 @@ struct SolveArgs {
   const float* lp;        // parameters (spectral multiplier)
   const float2* gains;    // [n_gain][2][n]
   const int* gain_index;  // [n_systems] (null: system s uses pair s)
+  int slot0;              // first slot of the launch's slot group
 };
 
 // Which slots a launch serves.  The first half of an iteration runs only the
@@ -116,7 +117,7 @@ __device__ __forceinline__ double abs2(double2 a) { return a.x * a.x + a.y * a.y
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
-  const int slot = blockIdx.y;
+  const int slot = A.slot0 + blockIdx.y;
   const SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
   if (!fwd_active(mode, half)) return;
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
 template <int TC>
 __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
-  const int slot = blockIdx.y;
+  const int slot = A.slot0 + blockIdx.y;
   const int mode = A.B.slots[slot].mode;
   if (!cols_active(mode, half)) return;
   const long long n = (long long)A.g.nz * A.g.nx;
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
-  const int slot = blockIdx.y;
+  const int slot = A.slot0 + blockIdx.y;
   const SlotState& S = A.B.slots[slot];
   if (!cols_active(S.mode, half)) return;
   const Geo& g = A.g;
@@ -479,7 +480,7 @@ __device__ __forceinline__ void reduce_and_finalize(const SolveArgs& A, SlotStat
 // ---------------------------------------------------------------------------
 template <bool ADJ>
 __global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
-  const int slot = blockIdx.y;
+  const int slot = A.slot0 + blockIdx.y;
   SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
   if (mode != (half == 0 ? MODE_ITER_A : MODE_ITER_B)) return;
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
 // ---------------------------------------------------------------------------
 template <bool ADJ>
 __global__ void __launch_bounds__(256) k_res(SolveArgs A) {
-  const int slot = blockIdx.y;
+  const int slot = A.slot0 + blockIdx.y;
   SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
   if (!(mode == MODE_RES || mode == MODE_INIT || mode == MODE_EMIT)) return;
@@ -724,7 +725,8 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
   const size_t n = (size_t)grid->nz * grid->nx;
   cudaStream_t caller = (cudaStream_t)stream;
 
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr, st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_poll[2] = {nullptr, nullptr};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -740,6 +742,9 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
 #define NSR_TRY(x) do { ce = (x); if (ce != cudaSuccess) { err = (int)ce; goto cleanup; } } while (0)
   {
     NSR_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    NSR_TRY(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    NSR_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    NSR_TRY(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     NSR_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
     NSR_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
     NSR_TRY(cudaEventCreateWithFlags(&ev_poll[0], cudaEventDisableTiming));
@@ -809,30 +814,42 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     NSR_TRY(cudaGetLastError());
     launches = 3;  // two table kernels and the slot initialisation
 
-    const dim3 g_fwd((grid->nz + A.rows - 1) / A.rows, n_slots);
-    const dim3 g_col((grid->nx + A.tc - 1) / A.tc, n_slots);
-    const dim3 g_inv(nb_st, n_slots);
-    const dim3 g_res(nb_res, n_slots);
+    // The slots run as two independent groups on two branches of the captured
+    // graph, so that one group's kernels fill the tail waves of the other's.
+    const int n_groups = n_slots >= 8 ? 2 : 1;
+    int g_first[2] = {0, 0}, g_count[2] = {n_slots, 0};
+    if (n_groups == 2) {
+      g_count[0] = (n_slots + 1) / 2;
+      g_first[1] = g_count[0];
+      g_count[1] = n_slots - g_count[0];
+    }
     const int K = params->graph_iterations > 0 ? params->graph_iterations : 16;
     // One iteration = 9 launches: fwd, cols, rinv, inv of the first half, then
     // fwd, cols, rinv, res, inv of the second half.
     const int seq_half[NSR_LAUNCHES_PER_IT] = {0, 0, 0, 0, 1, 1, 1, 1, 1};
     const int seq_kind[NSR_LAUNCHES_PER_IT] = {0, 1, 4, 3, 0, 1, 4, 2, 3};
-    auto launch = [&](int q) {
+    auto launch = [&](int q, int grp, cudaStream_t sq) {
       const int half = seq_half[q], which = seq_kind[q];
+      SolveArgs Ag = A;
+      Ag.slot0 = g_first[grp];
+      const int ns = g_count[grp];
+      const dim3 g_fwd((grid->nz + A.rows - 1) / A.rows, ns);
+      const dim3 g_col((grid->nx + A.tc - 1) / A.tc, ns);
+      const dim3 g_inv(nb_st, ns);
+      const dim3 g_res(nb_res, ns);
       if (which == 0) {
-        k_fwd<<<g_fwd, 256, fwd_smem, st>>>(A, half);
+        k_fwd<<<g_fwd, 256, fwd_smem, sq>>>(Ag, half);
       } else if (which == 1) {
-        if (A.tc == 16) k_cols<16><<<g_col, 512, col_smem, st>>>(A, half);
-        else k_cols<8><<<g_col, 512, col_smem, st>>>(A, half);
+        if (A.tc == 16) k_cols<16><<<g_col, 512, col_smem, sq>>>(Ag, half);
+        else k_cols<8><<<g_col, 512, col_smem, sq>>>(Ag, half);
       } else if (which == 2) {
-        if (A.adjoint) k_res<true><<<g_res, 256, 0, st>>>(A);
-        else k_res<false><<<g_res, 256, 0, st>>>(A);
+        if (A.adjoint) k_res<true><<<g_res, 256, 0, sq>>>(Ag);
+        else k_res<false><<<g_res, 256, 0, sq>>>(Ag);
       } else if (which == 3) {
-        if (A.adjoint) k_inv<true><<<g_inv, 256, 0, st>>>(A, half);
-        else k_inv<false><<<g_inv, 256, 0, st>>>(A, half);
+        if (A.adjoint) k_inv<true><<<g_inv, 256, 0, sq>>>(Ag, half);
+        else k_inv<false><<<g_inv, 256, 0, sq>>>(Ag, half);
       } else {
-        k_rinv<<<g_fwd, 256, fwd_smem, st>>>(A, half);
+        k_rinv<<<g_fwd, 256, fwd_smem, sq>>>(Ag, half);
       }
     };
 
@@ -849,18 +866,38 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
       if (!ev_prof) { err = (int)cudaErrorMemoryAllocation; goto cleanup; }
       for (int e = 0; e < n_prof_events; ++e) NSR_TRY(cudaEventCreate(&ev_prof[e]));
       NSR_TRY(cudaEventRecord(ev_prof[0], st));
+      // Both slot groups of a kernel between two events, running side by side
+      // as in the captured iterations: the durations cover every resident system.
       for (int it = 0; it < P; ++it)
         for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) {
-          launch(q);
+          const int e = it * NSR_LAUNCHES_PER_IT + q;
+          if (n_groups == 2) NSR_TRY(cudaStreamWaitEvent(st2, ev_prof[e], 0));
+          launch(q, 0, st);
+          if (n_groups == 2) {
+            launch(q, 1, st2);
+            NSR_TRY(cudaEventRecord(ev_join, st2));
+            NSR_TRY(cudaStreamWaitEvent(st, ev_join, 0));
+          }
           NSR_TRY(cudaGetLastError());
-          NSR_TRY(cudaEventRecord(ev_prof[1 + it * NSR_LAUNCHES_PER_IT + q], st));
+          NSR_TRY(cudaEventRecord(ev_prof[e + 1], st));
         }
-      launches += (long long)NSR_LAUNCHES_PER_IT * P;
+      launches += (long long)NSR_LAUNCHES_PER_IT * P * n_groups;
     }
 
     NSR_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    if (n_groups == 2) {
+      NSR_TRY(cudaEventRecord(ev_fork, st));
+      NSR_TRY(cudaStreamWaitEvent(st2, ev_fork, 0));
+    }
     for (int it = 0; it < K; ++it)
-      for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) launch(q);
+      for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) {
+        launch(q, 0, st);
+        if (n_groups == 2) launch(q, 1, st2);
+      }
+    if (n_groups == 2) {
+      NSR_TRY(cudaEventRecord(ev_join, st2));
+      NSR_TRY(cudaStreamWaitEvent(st, ev_join, 0));
+    }
     ce = cudaStreamEndCapture(st, &graph);
     if (ce != cudaSuccess) { err = (int)ce; goto cleanup; }
     NSR_TRY(cudaGraphInstantiate(&exec, graph, 0));
@@ -876,7 +913,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     while (launched < max_launch) {
       NSR_TRY(cudaGraphLaunch(exec, st));
       ++graph_launches;
-      launches += (long long)NSR_LAUNCHES_PER_IT * K;
+      launches += (long long)NSR_LAUNCHES_PER_IT * K * n_groups;
       const int slot_i = (int)(launched & 1);
       NSR_TRY(cudaMemcpyAsync(&host[slot_i], A.B.done, sizeof(int), cudaMemcpyDeviceToHost, st));
       NSR_TRY(cudaEventRecord(ev_poll[slot_i], st));
@@ -922,6 +959,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
   }
 cleanup:
   if (st) cudaStreamSynchronize(st);
+  if (st2) cudaStreamSynchronize(st2);
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   if (ev_in) cudaEventDestroy(ev_in);
@@ -936,6 +974,9 @@ cleanup:
     free(ev_prof);
   }
   if (st) cudaStreamDestroy(st);
+  if (st2) cudaStreamDestroy(st2);
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
 #undef NSR_TRY
   return err;
 }
