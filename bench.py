@@ -161,14 +161,14 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(arm="learned"):
-    """DRAM bytes per node and resident system of the dominant kernel of one arm, from the committed ncu summaries."""
+def profiled_traffic(arm, kernel):
+    """DRAM bytes per node and resident system of one kernel of one arm, from the committed ncu summaries."""
+    pat = r"traffic_bytes_per_node_per_system:\s*([0-9.eE+-]+)\s*kernel:\s*(\w+)\s*arm:\s*(\w+)"
     for path in sorted((ROOT / "profiles").glob("*.md")):
-        m = re.search(r"traffic_bytes_per_node_per_system:\s*([0-9.eE+-]+)\s*kernel:\s*(\w+)\s*arm:\s*(\w+)",
-                      path.read_text())
-        if m and m.group(3) == arm:
-            return float(m.group(1)), m.group(2)
-    return None, None
+        for m in re.finditer(pat, path.read_text()):
+            if m.group(3) == arm and m.group(2) == kernel:
+                return float(m.group(1))
+    return None
 
 
 # ---------------------------------------------------------------------------
@@ -337,15 +337,12 @@ def run_ours(args):
     dominant = L["dominant"]
     achieved = L["achieved"]
     launches = L["launches"] + LEARNED_SETUP_LAUNCHES * args.steps
-    traffic_per_node, traffic_kernel = profiled_traffic("learned")
-    traffic = None
-    if traffic_per_node is not None and traffic_kernel == dominant:
-        traffic = traffic_per_node * n * slots
+    traffic_per_node = profiled_traffic("learned", dominant)
+    traffic = None if traffic_per_node is None else traffic_per_node * n * slots
     plain_traffic = None
     if P is not None:
-        tp, tk = profiled_traffic("plain")
-        if tp is not None and tk == P["dominant"]:
-            plain_traffic = tp * n * slots
+        tp = profiled_traffic("plain", P["dominant"])
+        plain_traffic = None if tp is None else tp * n * slots
 
     # end to end through the public API with host buffers (learned arm)
     e2e_value = None

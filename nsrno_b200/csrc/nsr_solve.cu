@@ -33,7 +33,8 @@ enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES
 
 #define NSR_LAUNCHES_PER_IT 9
 #define NSR_ST_TZ 32      // rows of one stencil CTA
-#define NSR_ST_TX 256     // columns of one stencil CTA (one per thread)
+#define NSR_ST_TX 512     // columns of one stencil CTA (two per thread; even nx)
+#define NSR_ST_TX1 256    // columns of one stencil CTA of k_inv1 (one per thread; odd nx)
 
 struct __align__(16) SlotState {
   int sys, mode, iters, final_reason;
@@ -474,10 +475,16 @@ __device__ __forceinline__ void reduce_and_finalize(const SolveArgs& A, SlotStat
 
 // ---------------------------------------------------------------------------
 // inv: stencil on z = M^-1 (input) + inner products of the Krylov halves.
-// One thread per column of a NSR_ST_TZ x NSR_ST_TX tile walks down its rows
-// with the north/centre/south values of z and a in registers; east/west
-// neighbours are the adjacent threads' loads (L1 hits).
+// One thread owns two adjacent columns of a NSR_ST_TZ x NSR_ST_TX tile and
+// walks down its rows with the north/centre/south values of z and a in
+// registers; every field is read as 16-byte pairs.  The east/west
+// neighbours come from the adjacent threads by warp shuffles (global loads
+// at the warp edges).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float4 pack2(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
+
 template <bool ADJ>
 __global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
   const int slot = A.slot0 + blockIdx.y;
@@ -491,7 +498,109 @@ __global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
   const int rb = blockIdx.x / nbx, cb = blockIdx.x - rb * nbx;
   const int z0 = rb * NSR_ST_TZ;
   const int z1 = min(z0 + NSR_ST_TZ, g.nz);
-  const int j = cb * NSR_ST_TX + threadIdx.x;
+  const int j = cb * NSR_ST_TX + 2 * threadIdx.x;   // first of the thread's two columns
+  const bool own = j < nx;                          // nx is even here: both columns exist
+  const int lane = threadIdx.x & 31;
+  const long long soff = slot * n;
+  double acc[NSR_NPART];
+#pragma unroll
+  for (int q = 0; q < NSR_NPART; ++q) acc[q] = 0.0;
+  // Every thread of a warp takes part in the shuffles; threads past the last
+  // column carry zeros and store nothing.
+  {
+    const SysScalars sc = sys_scalars(g, S.freq);
+    const float* __restrict__ ca = A.mat.a32;
+    const float* __restrict__ cb_ = A.mat.b32;
+    const float* __restrict__ ct = A.mat.t32;
+    const float2* __restrict__ z = A.B.w + soff;
+    const float2* __restrict__ rh = A.B.rh + soff;
+    const float2* __restrict__ r = A.B.r + soff;
+    const float2* __restrict__ v = A.B.v + soff;
+    float2* __restrict__ out = (half == 0 ? A.B.v : A.B.t) + soff;
+    const float2 sv = f2(S.c_sv);
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float2 zero = make_float2(0.f, 0.f);
+    const int jc = own ? j : 0;
+    const bool edge_w = lane == 0, edge_e = lane == 31 || j + 2 >= nx;
+    long long idx = (long long)z0 * nx + jc;
+    float4 zu = (own && z0 > 0) ? *reinterpret_cast<const float4*>(z + idx - nx) : zero4;
+    float4 zc = own ? *reinterpret_cast<const float4*>(z + idx) : zero4;
+    float2 an = (own && z0 > 0) ? __ldg(reinterpret_cast<const float2*>(ca + idx - nx)) : make_float2(1.f, 1.f);
+    float2 ac = own ? __ldg(reinterpret_cast<const float2*>(ca + idx)) : make_float2(1.f, 1.f);
+    for (int i = z0; i < z1; ++i, idx += nx) {
+      const bool has_s = i + 1 < g.nz;
+      const float4 zd = (own && has_s) ? *reinterpret_cast<const float4*>(z + idx + nx) : zero4;
+      const float2 as = (own && has_s) ? __ldg(reinterpret_cast<const float2*>(ca + idx + nx)) : make_float2(1.f, 1.f);
+      // west neighbour of column j, east neighbour of column j+1
+      float2 zw = make_float2(__shfl_up_sync(0xffffffffu, zc.z, 1), __shfl_up_sync(0xffffffffu, zc.w, 1));
+      float aw = __shfl_up_sync(0xffffffffu, ac.y, 1);
+      float2 ze = make_float2(__shfl_down_sync(0xffffffffu, zc.x, 1), __shfl_down_sync(0xffffffffu, zc.y, 1));
+      float ae = __shfl_down_sync(0xffffffffu, ac.x, 1);
+      if (own && edge_w) {
+        zw = j > 0 ? z[idx - 1] : zero;
+        aw = j > 0 ? __ldg(&ca[idx - 1]) : 1.0f;
+      }
+      if (own && edge_e) {
+        ze = j + 2 < nx ? z[idx + 2] : zero;
+        ae = j + 2 < nx ? __ldg(&ca[idx + 2]) : 1.0f;
+      }
+      if (own) {
+        const float2 bb = __ldg(reinterpret_cast<const float2*>(cb_ + idx));
+        const float2 tt = __ldg(reinterpret_cast<const float2*>(ct + idx));
+        const float2 c0 = lo2(zc), c1 = hi2(zc);
+        const float2 av0 = stencil_pts<ADJ>(g, sc, i, j, ac.x, ac.y, aw, as.x, an.x, bb.x, tt.x, c0, c1, zw, lo2(zd),
+                                            lo2(zu));
+        const float2 av1 = stencil_pts<ADJ>(g, sc, i, j + 1, ac.y, ae, ac.x, as.y, an.y, bb.y, tt.y, c1, ze, c0,
+                                            hi2(zd), hi2(zu));
+        *reinterpret_cast<float4*>(out + idx) = pack2(av0, av1);
+        const float4 rk = *reinterpret_cast<const float4*>(rh + idx);
+        if (half == 0) {
+          dot_acc(acc[0], acc[1], lo2(rk), av0);       // <rhat, v>
+          dot_acc(acc[0], acc[1], hi2(rk), av1);
+        } else {
+          const float4 rr = *reinterpret_cast<const float4*>(r + idx);
+          const float4 vv = *reinterpret_cast<const float4*>(v + idx);
+          const float2 s0 = lo2(rr) + sv * lo2(vv), s1 = hi2(rr) + sv * hi2(vv);
+          dot_acc(acc[0], acc[1], av0, s0);            // <t, s>
+          dot_acc(acc[0], acc[1], av1, s1);
+          acc[2] += (double)av0.x * av0.x + (double)av0.y * av0.y + (double)av1.x * av1.x + (double)av1.y * av1.y;
+          acc[3] += (double)s0.x * s0.x + (double)s0.y * s0.y + (double)s1.x * s1.x + (double)s1.y * s1.y;
+          dot_acc(acc[4], acc[5], lo2(rk), av0);       // <rhat, t>
+          dot_acc(acc[4], acc[5], hi2(rk), av1);
+          dot_acc(acc[6], acc[7], lo2(rk), s0);        // <rhat, s>
+          dot_acc(acc[6], acc[7], hi2(rk), s1);
+        }
+      }
+      zu = zc;
+      zc = zd;
+      an = ac;
+      ac = as;
+    }
+  }
+  reduce_and_finalize(A, S, slot, mode, acc);
+}
+
+// ---------------------------------------------------------------------------
+// inv: stencil on z = M^-1 (input) + inner products of the Krylov halves.
+// k_inv1 (grids of odd width, whose rows are not 16-byte aligned): one thread
+// per column of a NSR_ST_TZ x NSR_ST_TX1 tile walks down its rows
+// with the north/centre/south values of z and a in registers; east/west
+// neighbours are the adjacent threads' loads (L1 hits).
+// ---------------------------------------------------------------------------
+template <bool ADJ>
+__global__ void __launch_bounds__(256, 4) k_inv1(SolveArgs A, int half) {
+  const int slot = A.slot0 + blockIdx.y;
+  SlotState& S = A.B.slots[slot];
+  const int mode = S.mode;
+  if (mode != (half == 0 ? MODE_ITER_A : MODE_ITER_B)) return;
+  const Geo& g = A.g;
+  const long long n = (long long)g.nz * g.nx;
+  const int nx = g.nx;
+  const int nbx = (nx + NSR_ST_TX1 - 1) / NSR_ST_TX1;
+  const int rb = blockIdx.x / nbx, cb = blockIdx.x - rb * nbx;
+  const int z0 = rb * NSR_ST_TZ;
+  const int z1 = min(z0 + NSR_ST_TZ, g.nz);
+  const int j = cb * NSR_ST_TX1 + threadIdx.x;
   const long long soff = slot * n;
   double acc[NSR_NPART];
 #pragma unroll
@@ -655,6 +764,13 @@ __global__ void k_solve_init(SolveArgs A, int n_slots) {
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
+// Stencil CTAs per slot: two columns per thread on even widths (16-byte
+// aligned rows), one column per thread otherwise.
+static int stencil_ctas(const NsrGrid* g) {
+  const int tx = (g->nx % 2 == 0) ? NSR_ST_TX : NSR_ST_TX1;
+  return ((g->nz + NSR_ST_TZ - 1) / NSR_ST_TZ) * ((g->nx + tx - 1) / tx);
+}
+
 static int band_rows(const NsrGrid* g) {
   int budget = g->nx <= 1024 ? 8192 : 16384;
   int tz = budget / g->nx - 2;
@@ -673,7 +789,7 @@ static Layout layout(const NsrGrid* g, int n_slots) {
   const size_t n = (size_t)g->nz * g->nx;
   const int tz = band_rows(g);
   const int nb_res = (g->nz + tz - 1) / tz;
-  const int nb_st = ((g->nz + NSR_ST_TZ - 1) / NSR_ST_TZ) * ((g->nx + NSR_ST_TX - 1) / NSR_ST_TX);
+  const int nb_st = stencil_ctas(g);
   L.nb_inv = nb_res > nb_st ? nb_res : nb_st;
   size_t off = 0;
   L.tables = off; off += nsr_align(nsr_prec_table_bytes(g));
@@ -804,7 +920,8 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     const size_t fwd_smem = sizeof(float2) * A.rows * nsr_row_stride(grid->nx);
     const size_t col_smem = nsr_cols_smem(grid);
     const int nb_res = (grid->nz + A.tz - 1) / A.tz;
-    const int nb_st = ((grid->nz + NSR_ST_TZ - 1) / NSR_ST_TZ) * ((grid->nx + NSR_ST_TX - 1) / NSR_ST_TX);
+    const int nb_st = stencil_ctas(grid);
+    const bool pairs = grid->nx % 2 == 0;
     NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
@@ -846,8 +963,13 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
         if (A.adjoint) k_res<true><<<g_res, 256, 0, sq>>>(Ag);
         else k_res<false><<<g_res, 256, 0, sq>>>(Ag);
       } else if (which == 3) {
-        if (A.adjoint) k_inv<true><<<g_inv, 256, 0, sq>>>(Ag, half);
-        else k_inv<false><<<g_inv, 256, 0, sq>>>(Ag, half);
+        if (pairs) {
+          if (A.adjoint) k_inv<true><<<g_inv, 256, 0, sq>>>(Ag, half);
+          else k_inv<false><<<g_inv, 256, 0, sq>>>(Ag, half);
+        } else {
+          if (A.adjoint) k_inv1<true><<<g_inv, 256, 0, sq>>>(Ag, half);
+          else k_inv1<false><<<g_inv, 256, 0, sq>>>(Ag, half);
+        }
       } else {
         k_rinv<<<g_fwd, 256, fwd_smem, sq>>>(Ag, half);
       }
