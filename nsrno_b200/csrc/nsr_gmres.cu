@@ -5,10 +5,11 @@
 //
 // The systems of a batch share the Arnoldi index j, so j is a launch argument
 // and one restart cycle is a fixed sequence of launches captured once in a
-// CUDA graph.  Per Arnoldi step (7 launches):
+// CUDA graph.  Per Arnoldi step (8 launches):
 //   fwd   v_j = (j ? w / h_{j,j-1} : r / beta), forward row FFT of v_j
 //   cols  column FFT, shifted-Laplace multiply, inverse column FFT
-//   inv   inverse row FFT + 5-point stencil: w = A M^-1 v_j
+//   rinv  inverse row FFT in place: W = M^-1 v_j
+//   inv   5-point stencil: w = A W
 //   dot   h_i = <v_i, w> (i <= j), FP64 partials, last-CTA sum
 //   axpy  w -= sum_i h_i v_i                (classical Gram-Schmidt, pass 1)
 //   dot   h'_i = <v_i, w>                   (pass 2)
@@ -16,8 +17,8 @@
 //         Givens rotations to column j, forms the new one and the residual
 //         estimate, all in FP64 on the device (no host least squares).
 // At the end of a cycle: back substitution for y (FP64), u = V y fused with
-// the forward row FFT, the column pass, and an FP64 pass that applies
-// x += M^-1 u and recomputes the true residual b - A x.
+// the forward row FFT, the column and inverse row passes, and an FP64 pass
+// that applies x += M^-1 u and recomputes the true residual b - A x.
 #include "nsr_internal.cuh"
 #include "nsr_device.cuh"
 
@@ -168,43 +169,79 @@ __global__ void __launch_bounds__(512) gk_cols(GArgs A, int j) {
   cols_pass<TC>(sm, A.g, A.tab, A.W + slot * n, S.freq, A.shift, A.adjoint, blockIdx.x * TC, A.lp);
 }
 
-// inv: w = A M^-1 v_j (FP32 stencil on the inverse row FFT of W)
-template <bool ADJ>
-__global__ void __launch_bounds__(256) gk_inv(GArgs A, int j) {
+// rinv: inverse row FFT of W in place, times the outer gain (W becomes M^-1 v_j,
+// or M^-1 u at the end of a cycle when j < 0).
+__global__ void __launch_bounds__(256, 4) gk_rinv(GArgs A, int j) {
   extern __shared__ float2 sm[];
+  const int slot = blockIdx.y;
+  const GSlot& S = A.slots[slot];
+  const bool on = j >= 0 ? g_active(S, j) : (S.sys >= 0 && !S.done && S.used > 0);
+  if (!on) return;
+  const Geo& g = A.g;
+  const long long n = (long long)g.nz * g.nx;
+  const int z0 = blockIdx.x * A.rows;
+  const int nr = min(A.rows, g.nz - z0);
+  const long long off = (long long)z0 * g.nx;
+  float2* __restrict__ Wp = A.W + slot * n + off;
+  const int nx = g.nx, rs = nsr_row_stride(nx);
+  const bool pad = nsr_row_padded(nx);
+  for (int l = 0; l < nr; ++l)
+    for (int c = threadIdx.x; c < nx; c += blockDim.x) sm[row_slot(l, c, rs, pad)] = Wp[l * nx + c];
+  __syncthreads();
+  fft_rows<true>(sm, nr, A.tab.px);
+  __syncthreads();
+  const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
+  for (int l = 0; l < nr; ++l)
+    for (int c = threadIdx.x; c < nx; c += blockDim.x) {
+      const float2 v = sm[row_slot(l, c, rs, pad)];
+      Wp[l * nx + c] = G.post ? gain_mul(G.post, off + l * nx + c, G.conj, v) : v;
+    }
+}
+
+// inv: w = A z with z = M^-1 v_j in W.  One thread per column of a
+// NSR_GST_TZ x NSR_GST_TX tile walks down its rows with the north/centre/south
+// values of z and a in registers.
+#define NSR_GST_TZ 32
+#define NSR_GST_TX 256
+template <bool ADJ>
+__global__ void __launch_bounds__(256, 4) gk_inv(GArgs A, int j) {
   const int slot = blockIdx.y;
   const GSlot& S = A.slots[slot];
   if (!g_active(S, j)) return;
   const Geo& g = A.g;
   const long long n = (long long)g.nz * g.nx;
-  const int z0 = blockIdx.x * A.tz;
-  const int nb = min(A.tz, g.nz - z0);
-  const int nx = g.nx, rs = nsr_row_stride(nx);
-  const bool pad = nsr_row_padded(nx);
-  band_inverse_rows(sm, g, A.tab, A.W + slot * n, z0, nb);
-  band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
+  const int nx = g.nx;
+  const int nbx = (nx + NSR_GST_TX - 1) / NSR_GST_TX;
+  const int rb = blockIdx.x / nbx, cb = blockIdx.x - rb * nbx;
+  const int z0 = rb * NSR_GST_TZ;
+  const int z1 = min(z0 + NSR_GST_TZ, g.nz);
+  const int jj = cb * NSR_GST_TX + threadIdx.x;
+  if (jj >= nx) return;
   const SysScalars sc = sys_scalars(g, S.freq);
+  const float* __restrict__ ca = A.mat.a32;
+  const float2* __restrict__ z = A.W + slot * n;
   float2* __restrict__ w = A.w + slot * n;
-  const float* ca = A.mat.a32;
-  for (int rr = 0; rr < nb; ++rr) {
-    const int i = z0 + rr;
-    const float2* row = sm + (rr + 1) * rs;
-    const float2* up = sm + rr * rs;
-    const float2* dn = sm + (rr + 2) * rs;
-    for (int jj = threadIdx.x; jj < nx; jj += blockDim.x) {
-      const long long idx = (long long)i * nx + jj;
-      const float2 z = make_float2(0.f, 0.f);
-      const int aj = pad ? jj + (jj >> 4) : jj;
-      const float2 pe = jj + 1 < nx ? row[pad ? (jj + 1) + ((jj + 1) >> 4) : jj + 1] : z;
-      const float2 pw = jj > 0 ? row[pad ? (jj - 1) + ((jj - 1) >> 4) : jj - 1] : z;
-      const float a_c = __ldg(&ca[idx]);
-      const float a_e = jj + 1 < nx ? __ldg(&ca[idx + 1]) : 1.0f;
-      const float a_w = jj > 0 ? __ldg(&ca[idx - 1]) : 1.0f;
-      const float a_s = i + 1 < g.nz ? __ldg(&ca[idx + nx]) : 1.0f;
-      const float a_n = i > 0 ? __ldg(&ca[idx - nx]) : 1.0f;
-      w[idx] = stencil_pts<ADJ>(g, sc, i, jj, a_c, a_e, a_w, a_s, a_n, __ldg(&A.mat.b32[idx]),
-                                __ldg(&A.mat.t32[idx]), row[aj], pe, pw, dn[aj], up[aj]);
-    }
+  const float2 zero = make_float2(0.f, 0.f);
+  const bool has_e = jj + 1 < nx, has_w = jj > 0;
+  long long idx = (long long)z0 * nx + jj;
+  float2 zu = z0 > 0 ? z[idx - nx] : zero;
+  float2 zc = z[idx];
+  float a_n = z0 > 0 ? __ldg(&ca[idx - nx]) : 1.0f;
+  float a_c = __ldg(&ca[idx]);
+  for (int i = z0; i < z1; ++i, idx += nx) {
+    const bool has_s = i + 1 < g.nz;
+    const float2 zd = has_s ? z[idx + nx] : zero;
+    const float a_s = has_s ? __ldg(&ca[idx + nx]) : 1.0f;
+    const float2 ze = has_e ? z[idx + 1] : zero;
+    const float2 zw = has_w ? z[idx - 1] : zero;
+    const float a_e = has_e ? __ldg(&ca[idx + 1]) : 1.0f;
+    const float a_w = has_w ? __ldg(&ca[idx - 1]) : 1.0f;
+    w[idx] = stencil_pts<ADJ>(g, sc, i, jj, a_c, a_e, a_w, a_s, a_n, __ldg(&A.mat.b32[idx]), __ldg(&A.mat.t32[idx]),
+                              zc, ze, zw, zd, zu);
+    zu = zc;
+    zc = zd;
+    a_n = a_c;
+    a_c = a_s;
   }
 }
 
@@ -373,7 +410,6 @@ __global__ void __launch_bounds__(256) gk_comb(GArgs A) {
 // FP64 true residual.  init = 1: x = x0 (or 0); init = 0: x += M^-1 V y.
 template <bool ADJ>
 __global__ void __launch_bounds__(256) gk_res(GArgs A, int init) {
-  extern __shared__ float2 sm[];
   const int slot = blockIdx.y;
   GSlot& S = A.slots[slot];
   if (S.sys < 0 || S.done) return;
@@ -382,12 +418,8 @@ __global__ void __launch_bounds__(256) gk_res(GArgs A, int init) {
   const long long n = (long long)g.nz * g.nx;
   const int z0 = blockIdx.x * A.tz;
   const int nb = min(A.tz, g.nz - z0);
-  const int nx = g.nx, rs = nsr_row_stride(nx);
-  const bool pad = nsr_row_padded(nx);
-  if (!init) {
-    band_inverse_rows(sm, g, A.tab, A.W + slot * n, z0, nb);
-    band_post_gain(sm, g, gain_pair(A.gains, S.gidx, n, A.adjoint).post, A.adjoint != 0, z0, nb);
-  }
+  const int nx = g.nx;
+  const float2* zW = A.W + slot * n;   // M^-1 u after the rinv pass
   const SysScalars sc = sys_scalars(g, S.freq);
   const double2* xo = A.x + (2LL * slot + S.xpar) * n;
   double2* xn = A.x + (2LL * slot + (S.xpar ^ 1)) * n;
@@ -396,7 +428,7 @@ __global__ void __launch_bounds__(256) gk_res(GArgs A, int init) {
     if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return make_double2(0.0, 0.0);
     const long long id = (long long)i2 * nx + j2;
     if (init) return x0 ? to_d(x0[id]) : make_double2(0.0, 0.0);
-    return xo[id] + to_d(sm[(i2 - z0 + 1) * rs + (pad ? j2 + (j2 >> 4) : j2)]);
+    return xo[id] + to_d(zW[id]);
   };
   auto Aa = [&](int i2, int j2) -> double {
     if (i2 < 0 || i2 >= g.nz || j2 < 0 || j2 >= nx) return 1.0;
@@ -667,27 +699,25 @@ extern "C" int nsr_gmres_batched(const NsrGrid* grid, const void* material, cons
     const int rs = nsr_row_stride(grid->nx);
     const size_t fwd_smem = sizeof(float2) * A.rows * rs;
     const size_t col_smem = nsr_cols_smem(grid);
-    const size_t inv_smem = sizeof(float2) * (A.tz + 2) * rs;
+    const int nb_st = ((grid->nz + NSR_GST_TZ - 1) / NSR_GST_TZ) * ((grid->nx + NSR_GST_TX - 1) / NSR_GST_TX);
     NSR_TRY(cudaFuncSetAttribute(gk_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     NSR_TRY(cudaFuncSetAttribute(gk_comb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     NSR_TRY(cudaFuncSetAttribute(gk_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(gk_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-    NSR_TRY(cudaFuncSetAttribute(gk_inv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
-    NSR_TRY(cudaFuncSetAttribute(gk_inv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
-    NSR_TRY(cudaFuncSetAttribute(gk_res<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
-    NSR_TRY(cudaFuncSetAttribute(gk_res<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+    NSR_TRY(cudaFuncSetAttribute(gk_rinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
 
     const dim3 g_rows((grid->nz + A.rows - 1) / A.rows, n_slots);
     const dim3 g_col((grid->nx + A.tc - 1) / A.tc, n_slots);
     const dim3 g_band(L.nb_band, n_slots);
+    const dim3 g_st(nb_st, n_slots);
     const dim3 g_dot(L.nb_dot, n_slots);
     auto cols = [&](int j) {
       if (A.tc == 16) gk_cols<16><<<g_col, 512, col_smem, st>>>(A, j);
       else gk_cols<8><<<g_col, 512, col_smem, st>>>(A, j);
     };
     auto res = [&](int init) {
-      if (A.adjoint) gk_res<true><<<g_band, 256, inv_smem, st>>>(A, init);
-      else gk_res<false><<<g_band, 256, inv_smem, st>>>(A, init);
+      if (A.adjoint) gk_res<true><<<g_band, 256, 0, st>>>(A, init);
+      else gk_res<false><<<g_band, 256, 0, st>>>(A, init);
     };
 
     // One restart cycle.
@@ -695,8 +725,9 @@ extern "C" int nsr_gmres_batched(const NsrGrid* grid, const void* material, cons
     for (int j = 0; j < m; ++j) {
       gk_fwd<<<g_rows, 256, fwd_smem, st>>>(A, j);
       cols(j);
-      if (A.adjoint) gk_inv<true><<<g_band, 256, inv_smem, st>>>(A, j);
-      else gk_inv<false><<<g_band, 256, inv_smem, st>>>(A, j);
+      gk_rinv<<<g_rows, 256, fwd_smem, st>>>(A, j);
+      if (A.adjoint) gk_inv<true><<<g_st, 256, 0, st>>>(A, j);
+      else gk_inv<false><<<g_st, 256, 0, st>>>(A, j);
       gk_dot<<<g_dot, 256, 0, st>>>(A, j);
       gk_axpy<<<g_dot, 256, 0, st>>>(A, j, 1);
       gk_dot<<<g_dot, 256, 0, st>>>(A, j);
@@ -705,6 +736,7 @@ extern "C" int nsr_gmres_batched(const NsrGrid* grid, const void* material, cons
     gk_solve<<<(n_slots + 127) / 128, 128, 0, st>>>(A);
     gk_comb<<<g_rows, 256, fwd_smem, st>>>(A);
     cols(-1);
+    gk_rinv<<<g_rows, 256, fwd_smem, st>>>(A, -1);
     res(0);
     gk_count<<<1, 256, 0, st>>>(A, remaining);
     ce = cudaStreamEndCapture(st, &graph);
