@@ -75,3 +75,17 @@ def test_workspace_queries(lib):
     assert lib.nsr_solve_workspace_size(ctypes.byref(g), 0) == 0
     assert lib.nsr_precondition_workspace_size(ctypes.byref(g), 2) >= 2 * n * 8
     assert lib.nsr_precondition_workspace_size(ctypes.byref(grid(nx=4096)), 1) == 0
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/nsrno_b200.h is a C99 header (no C++ or torch types at the boundary)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "probe.c"
+    src.write_text('#include "nsrno_b200.h"\nint main(void) { NsrSolveParams p; NsrLearned l; NsrGrid g;'
+                   ' (void)p; (void)l; (void)g; return 0; }\n')
+    subprocess.run([cc, "-std=c99", "-Wall", "-Werror", f"-I{ROOT / 'include'}", "-fsyntax-only", str(src)],
+                   check=True)
