@@ -328,7 +328,7 @@ def training_media(n_media, nz, nx, seed0=100, device=None):
     return out
 
 
-def train(steps=2000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media=8, channel_weight=1.0, seed=0,
+def train(steps=4000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media=16, channel_weight=1.0, seed=0,
           device=None, log=print, params=None):
     """Train the learned preconditioner on seeded breast-like media (GPU).
 
@@ -369,13 +369,13 @@ def train(steps=2000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media
 
 def main():
     ap = argparse.ArgumentParser(description="Train the learned preconditioner on the GPU")
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--nz", type=int, default=256)
     ap.add_argument("--nx", type=int, default=384)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--krylov-steps", type=int, default=48)
     ap.add_argument("--lr", type=float, default=3e-3)
-    ap.add_argument("--media", type=int, default=8)
+    ap.add_argument("--media", type=int, default=16)
     ap.add_argument("--channel-weight", type=float, default=1.0)
     ap.add_argument("--out", type=Path, default=WEIGHTS)
     a = ap.parse_args()
