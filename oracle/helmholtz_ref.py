@@ -1,7 +1,7 @@
 """CPU oracle for the 5-point viscoacoustic Helmholtz solve -- TEST INFRASTRUCTURE ONLY.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import this module, and only as the checker or as the timed
+``bench.py`` may import this module, and only to check results or as the timed
 CPU baseline.  The product path (``nsrno_b200``) never imports it.
 
 It restates, in complex128 NumPy/SciPy, the discretisation of the reference
@@ -20,7 +20,8 @@ and the Krylov drivers of the dense path:
 * ``bicgstab``   nsrno/dense_wave.py:118-148  -> :func:`bicgstab`
 * ``gmres``      nsrno/wave_solver.py:9-36    -> :func:`gmres`
 
-Two extensions follow the north-star contract and are stated here because the
+Two extensions follow the solve contract (c, rho, alpha, freq, angle, source)
+and are stated here because the
 5-point reference has no counterpart for them:
 
 * power-law attenuation folded into the mass term, ``k^2 -> k^2 (1 + i e)^2``

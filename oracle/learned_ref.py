@@ -1,7 +1,7 @@
 """CPU oracle of the learned preconditioner -- TEST INFRASTRUCTURE ONLY.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU leg of ``bench.py`` may
-import this module, and only as the checker.  The product path
+import this module, and only to check results.  The product path
 (``nsrno_b200``) never imports it.
 
 It restates, in float64 / complex128 PyTorch on the CPU (autograd supplies the

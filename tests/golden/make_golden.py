@@ -1,5 +1,5 @@
 """Generate golden vectors from the reference implementation (run in a container
-that has the reference checked out; the GPU box does not need this script).
+that has the reference checked out; machines that only run the tests do not need this script).
 
     python tests/golden/make_golden.py /root/reference
 

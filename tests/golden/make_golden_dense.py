@@ -1,5 +1,5 @@
 """Generate golden vectors of the reference's 8th-order dense operator
-(run in a container that has the reference checked out; not needed on the GPU box).
+(run in a container that has the reference checked out; not needed where the tests only run).
 
     python tests/golden/make_golden_dense.py /root/reference
 
