@@ -808,8 +808,10 @@ extern "C" size_t nsr_solve_workspace_size(const NsrGrid* grid, int32_t n_slots)
   return layout(grid, n_slots).total;
 }
 
+// Pinned host word the solve loop polls; one per host thread, so that solves
+// issued from different threads (e.g. one per device) do not share it.
 static int* pinned_counter() {
-  static int* p = nullptr;
+  static thread_local int* p = nullptr;
   if (!p) {
     if (cudaHostAlloc((void**)&p, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) p = nullptr;
   }
