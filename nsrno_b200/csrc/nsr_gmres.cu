@@ -624,8 +624,9 @@ extern "C" int nsr_gmres_batched(const NsrGrid* grid, const void* material, cons
                                  int32_t* iterations, int32_t* status, void* fields, void* stream) {
   int err = nsr_check_grid(grid, true);
   if (err) return err;
-  if (!params || !material || !freq_hz || n_systems < 0 || n_rx < 0 || (n_rx > 0 && (!rx_index || !iq)))
-    return NSR_ERR_ARGUMENT;
+  if (!params || !material || n_systems < 0 || n_rx < 0) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;   // an empty batch touches no buffer
+  if (!freq_hz || (n_rx > 0 && (!rx_index || !iq))) return NSR_ERR_ARGUMENT;
   if (!rhs && !angle_rad) return NSR_ERR_ARGUMENT;
   if (!residual || !iterations || !status || !workspace) return NSR_ERR_ARGUMENT;
   const int m = params->restart, n_slots = params->n_slots;

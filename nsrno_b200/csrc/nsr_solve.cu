@@ -828,7 +828,9 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
                                  void* fields, NsrSolveStats* stats, void* stream) {
   int err = nsr_check_grid(grid, true);
   if (err) return err;
-  if (!params || !coef || !freq_hz || n_systems < 0 || n_rx < 0 || (n_rx > 0 && !rx_index)) return NSR_ERR_ARGUMENT;
+  if (!params || !coef || n_systems < 0 || n_rx < 0) return NSR_ERR_ARGUMENT;
+  if (n_systems == 0) return 0;   // an empty batch touches no buffer
+  if (!freq_hz || (n_rx > 0 && !rx_index)) return NSR_ERR_ARGUMENT;
   if (!rhs && !angle_rad) return NSR_ERR_ARGUMENT;
   if (!iq && n_rx > 0) return NSR_ERR_ARGUMENT;
   if (!residual || !iterations || !status || !workspace) return NSR_ERR_ARGUMENT;

@@ -189,3 +189,49 @@ def test_growing_residual_restarts(cuda):
     res = solve_batched(med, f, th, tolerance=1e-6, max_iterations=6000, n_slots=2)
     assert res.reasons() == ["converged"] * 2
     assert float(res.residual.max()) < 1e-6
+
+
+def test_empty_batch(cuda):
+    from nsrno_b200 import gmres_batched, solve_batched
+    rec, med = blob_case(cuda)
+    r = solve_batched(med, [], [])
+    assert r.iq.shape[0] == 0 and r.reasons() == []
+    g = gmres_batched(med, [], [])
+    assert g.reasons() == []
+
+
+def test_odd_width_grid_matches_lu(cuda):
+    """243 x 729 (odd widths: the one-column stencil kernel), fixed and learned
+    preconditioners, against SuperLU."""
+    from nsrno_b200 import Geometry, LearnedPreconditioner, Medium, solve_batched
+    from nsrno_b200.media import breast_record
+    rec = breast_record(seed=9, nz=243, nx=729, n_pml=20, n_rx=64, rx_pitch=4, bins=[5.2e6], n_angles=2)
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=cuda)
+    f, th = rec.systems()
+    spec = spec_of(rec)
+    a, b, t = med.coef64.cpu().numpy()
+    A = H.operator_planes(spec, a, b, t, f[0])
+    st = LearnedPreconditioner.load(device=cuda).setup(med, rec.frequencies)
+    for learned in (None, st):
+        res = solve_batched(med, f, th, tolerance=1e-8, max_iterations=4000, return_fields=True, learned=learned)
+        assert res.reasons() == ["converged"] * 2
+        for s in range(2):
+            ref = H.solve_lu(A, H.plane_wave_rhs(spec, f[s], th[s]))
+            assert rel(res.fields[s].cpu().numpy().ravel(), ref) < 1e-5
+
+
+def test_largest_grid_converges(cuda):
+    """2048 x 2048, the largest transform size (8-column tiles in the column
+    pass): converged systems whose FP64 true residual, recomputed by the
+    independent nsr_true_residual kernel, meets the tolerance."""
+    from nsrno_b200 import Geometry, Medium, solve_batched, true_residual
+    from nsrno_b200.media import blob_record
+    rec = blob_record(nz=2048, nx=2048, h=5e-5, n_pml=32, n_blobs=4, frequencies=(1.5e6,), n_rx=192, rx_pitch=4)
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=cuda)
+    f, th = rec.systems()
+    res = solve_batched(med, f[:2], th[:2], tolerance=1e-6, max_iterations=4000, return_fields=True,
+                        fields_dtype=torch.complex128)
+    assert res.reasons() == ["converged"] * 2
+    tr = true_residual(med, res.fields, f[:2], th[:2]).cpu().numpy()
+    assert (tr < 1e-6).all()
+    assert np.allclose(tr, res.residual.cpu().numpy(), rtol=1e-6)
