@@ -115,66 +115,25 @@ __device__ __forceinline__ float2 learned_symbol(const LearnedSpec& L, float s2z
   return make_float2(er * dr + ei * di, ei * dr - er * di);
 }
 
-template <int TC>
-__device__ __forceinline__ void cols_pass(float2* sm, const Geo& g, const PrecTables& tab, float2* __restrict__ ws,
-                                          double freq, double shift, int adjoint, int c0,
-                                          const float* __restrict__ lp = nullptr) {
-  const long long n = (long long)g.nz * g.nx;
+// Column pass with an arbitrary multiplier: `mul(c, z)` is the factor of tile
+// column c at digit-reversed z position, including the 1/n of the transform
+// pair; columns at or beyond the grid edge are never multiplied.
+template <int TC, typename MUL>
+__device__ __forceinline__ void cols_pass_with(float2* sm, const Geo& g, const PrecTables& tab,
+                                               float2* __restrict__ ws, int c0, MUL mul) {
   const int ncol = min(TC, g.nx - c0);
   for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
     const int z = k / TC, c = k - z * TC;
     sm[k] = c < ncol ? ws[(long long)z * g.nx + c0 + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  const SysScalars s = sys_scalars(g, freq);
-  const float kh2 = (float)s.kh2;
-  const float inv_n = 1.0f / (float)n;
-  const float2 shiftc = make_float2(kh2, (float)(s.kh2 * shift));
-  bool fused;
-  if (lp) {
-    // The spectral parameters go through shared memory so that the fused
-    // radix stage keeps its registers for the butterfly.
-    __shared__ LearnedSpec Ls;
-    if (threadIdx.x == 0) Ls = load_learned_spec(lp);
-    __syncthreads();
-    const float h2 = (float)(g.h * g.h);
-    fused = fft_cols_fused<TC>(sm, tab.pz, [&](int c, int z) -> float2 {
-      if (c >= ncol) return make_float2(0.f, 0.f);
-      const float2 mul = inv_n * learned_symbol(Ls, tab.s2z[z], tab.s2x[c0 + c], kh2, h2);
-      return adjoint ? conjc(mul) : mul;
-    });
-  } else {
-    fused = fft_cols_fused<TC>(sm, tab.pz, [&](int c, int z) -> float2 {
-      if (c >= ncol) return make_float2(0.f, 0.f);
-      const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
-      const float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
-      return adjoint ? conjc(mul) : mul;
-    });
-  }
-  if (!fused) {
+  auto m = [&](int c, int z) -> float2 { return c < ncol ? mul(c, z) : make_float2(0.f, 0.f); };
+  if (!fft_cols_fused<TC>(sm, tab.pz, m)) {
     // Sizes without a specialised transform: separate passes.
     fft_cols<false, TC>(sm, tab.pz);
-    if (lp) {
-      const LearnedSpec L = load_learned_spec(lp);
-      const float h2 = (float)(g.h * g.h);
-      for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-        const int z = k / TC, c = k - z * TC;
-        if (c < ncol) {
-          float2 mul = inv_n * learned_symbol(L, tab.s2z[z], tab.s2x[c0 + c], kh2, h2);
-          if (adjoint) mul = conjc(mul);
-          sm[k] = sm[k] * mul;
-        }
-      }
-    } else {
-      for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
-        const int z = k / TC, c = k - z * TC;
-        if (c < ncol) {
-          const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
-          float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
-          if (adjoint) mul = conjc(mul);
-          sm[k] = sm[k] * mul;
-        }
-      }
+    for (int k = threadIdx.x; k < g.nz * TC; k += blockDim.x) {
+      const int z = k / TC, c = k - z * TC;
+      sm[k] = sm[k] * m(c, z);
     }
     __syncthreads();
     fft_cols<true, TC>(sm, tab.pz);
@@ -183,6 +142,64 @@ __device__ __forceinline__ void cols_pass(float2* sm, const Geo& g, const PrecTa
     const int z = k / TC, c = k - z * TC;
     if (c < ncol) ws[(long long)z * g.nx + c0 + c] = sm[k];
   }
+}
+
+// Fixed shifted-Laplace multiplier 1 / (n (-4 (s2z + s2x) + (k0 h)^2 (1 + i shift))).
+template <int TC>
+__device__ __forceinline__ void cols_pass_fixed(float2* sm, const Geo& g, const PrecTables& tab,
+                                                float2* __restrict__ ws, double freq, double shift, int adjoint,
+                                                int c0) {
+  const SysScalars s = sys_scalars(g, freq);
+  const float inv_n = 1.0f / (float)((long long)g.nz * g.nx);
+  const float2 shiftc = make_float2((float)s.kh2, (float)(s.kh2 * shift));
+  cols_pass_with<TC>(sm, g, tab, ws, c0, [&](int c, int z) -> float2 {
+    const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
+    const float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
+    return adjoint ? conjc(mul) : mul;
+  });
+}
+
+// Learned multiplier read from a plane evaluated beforehand for this system:
+// symp[z * nx + x] at digit-reversed (z, x), 1/n included.
+template <int TC>
+__device__ __forceinline__ void cols_pass_plane(float2* sm, const Geo& g, const PrecTables& tab,
+                                                float2* __restrict__ ws, const float2* __restrict__ symp,
+                                                int adjoint, int c0) {
+  cols_pass_with<TC>(sm, g, tab, ws, c0, [&](int c, int z) -> float2 {
+    const float2 mul = symp[(long long)z * g.nx + c0 + c];
+    return adjoint ? conjc(mul) : mul;
+  });
+}
+
+// Learned multiplier times 1/n at digit-reversed position (z, x) of frequency
+// `freq`: the value cols_pass_plane expects in its plane.
+__device__ __forceinline__ float2 learned_plane_value(const LearnedSpec& L, const Geo& g, const PrecTables& tab,
+                                                      float kh2, int z, int x) {
+  const float h2 = (float)(g.h * g.h);
+  const float inv_n = 1.0f / (float)((long long)g.nz * g.nx);
+  return inv_n * learned_symbol(L, tab.s2z[z], tab.s2x[x], kh2, h2);
+}
+
+// Column pass of either preconditioner, chosen at run time: the learned
+// multiplier evaluated on the fly from `lp` (non-null), else the fixed one.
+template <int TC>
+__device__ __forceinline__ void cols_pass(float2* sm, const Geo& g, const PrecTables& tab, float2* __restrict__ ws,
+                                          double freq, double shift, int adjoint, int c0,
+                                          const float* __restrict__ lp = nullptr) {
+  if (!lp) {
+    cols_pass_fixed<TC>(sm, g, tab, ws, freq, shift, adjoint, c0);
+    return;
+  }
+  // The spectral parameters go through shared memory so that the fused radix
+  // stage keeps its registers for the butterfly.
+  __shared__ LearnedSpec Ls;
+  if (threadIdx.x == 0) Ls = load_learned_spec(lp);
+  __syncthreads();
+  const float kh2 = (float)sys_scalars(g, freq).kh2;
+  cols_pass_with<TC>(sm, g, tab, ws, c0, [&](int c, int z) -> float2 {
+    const float2 mul = learned_plane_value(Ls, g, tab, kh2, z, c0 + c);
+    return adjoint ? conjc(mul) : mul;
+  });
 }
 
 // Rows z0-1 .. z0+nb of w (zero outside the grid) into the padded row layout

@@ -58,6 +58,7 @@ struct SolveBufs {
   int* warm;          // [2]: initial fields accepted, rejected
   double* partials;   // [n_slots][nb_inv][NSR_NPART]
   float2 *r, *rh, *p, *v, *t, *y, *w;   // [n_slots][n]
+  float2* sym;        // [n_slots][n] learned multiplier of the slot's system (learned solves only)
   double2* x;         // [n_slots][2][n]
 };
 
@@ -132,6 +133,18 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   if (mode == MODE_INIT) {
     const float2 z = make_float2(0.f, 0.f);
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) { p[k] = z; v[k] = z; t[k] = z; y[k] = z; }
+    if (A.lp) {
+      // The learned Fourier multiplier depends on the system's frequency only:
+      // evaluate it once per system, in the digit-reversed (z, x) order of the
+      // transformed field, for k_cols to read.
+      const LearnedSpec L = load_learned_spec(A.lp);
+      const float kh2 = (float)sys_scalars(g, S.freq).kh2;
+      float2* __restrict__ sym = A.B.sym + off;
+      for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const int l = k / g.nx;
+        sym[k] = learned_plane_value(L, g, A.tab, kh2, z0 + l, k - l * g.nx);
+      }
+    }
     return;
   }
   if (mode == MODE_EMIT) {
@@ -148,11 +161,12 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
     return;
   }
   const float2 sv = f2(S.c_sv), rt = f2(S.c_rt), yp = f2(S.c_yp), ys = f2(S.c_ys), pp = f2(S.c_pp), pv = f2(S.c_pv);
-  const int nx = g.nx;
   const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
   const long long goff = (long long)z0 * g.nx;   // node index of this tile's first element
-  const int rs = nsr_row_stride(nx);
-  const bool pad = nsr_row_padded(nx);
+  // The tile's rows are contiguous in HBM, so one flat index k = l*nx + c runs
+  // over them.  The padded row layout puts (l, c) at l*(nx + nx/16) + c + c/16,
+  // which equals k + k/16 because every padded width is a multiple of 16.
+  const bool pad = nsr_row_padded(g.nx);
   float2* __restrict__ rr_ = r;
   float2* __restrict__ pp_ = p;
   float2* __restrict__ yy_ = y;
@@ -161,60 +175,53 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   if (mode == MODE_ITER_A) {
     const bool restart = S.restart != 0;
     float2* __restrict__ rh = A.B.rh + off;
-    for (int l = 0; l < nr; ++l) {
 #pragma unroll 4
-      for (int c = threadIdx.x; c < nx; c += blockDim.x) {
-        const int k = l * nx + c;
-        const float2 rk = rr_[k], vk = vv_[k], tk = tt_[k], pk = pp_[k], yk = yy_[k];
-        const float2 s1 = rk + sv * vk;
-        const float2 rn = s1 + rt * tk;
-        const float2 yn = yk + yp * pk + ys * s1;
-        const float2 pn = rn + pp * pk + pv * vk;
-        rr_[k] = rn; pp_[k] = pn; yy_[k] = yn;
-        if (restart) rh[k] = rn;
-        sm[l * rs + (pad ? c + (c >> 4) : c)] = G.pre ? gain_mul(G.pre, goff + k, G.conj, pn) : pn;
-      }
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 rk = rr_[k], vk = vv_[k], tk = tt_[k], pk = pp_[k], yk = yy_[k];
+      const float2 s1 = rk + sv * vk;
+      const float2 rn = s1 + rt * tk;
+      const float2 yn = yk + yp * pk + ys * s1;
+      const float2 pn = rn + pp * pk + pv * vk;
+      rr_[k] = rn; pp_[k] = pn; yy_[k] = yn;
+      if (restart) rh[k] = rn;
+      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, pn) : pn;
     }
   } else if (mode == MODE_ITER_B) {
-    for (int l = 0; l < nr; ++l) {
-#pragma unroll 4
-      for (int c = threadIdx.x; c < nx; c += blockDim.x) {
-        const int k = l * nx + c;
-        const float2 s1 = rr_[k] + sv * vv_[k];
-        sm[l * rs + (pad ? c + (c >> 4) : c)] = G.pre ? gain_mul(G.pre, goff + k, G.conj, s1) : s1;
-      }
+#pragma unroll 8
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 s1 = rr_[k] + sv * vv_[k];
+      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, s1) : s1;
     }
   } else {  // MODE_RES: apply the pending update to y, transform y, clear it
-    for (int l = 0; l < nr; ++l) {
-      for (int c = threadIdx.x; c < nx; c += blockDim.x) {
-        const int k = l * nx + c;
-        const float2 s1 = rr_[k] + sv * vv_[k];
-        const float2 yn = yy_[k] + yp * pp_[k] + ys * s1;
-        sm[l * rs + (pad ? c + (c >> 4) : c)] = G.pre ? gain_mul(G.pre, goff + k, G.conj, yn) : yn;
-        yy_[k] = make_float2(0.f, 0.f);
-      }
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 s1 = rr_[k] + sv * vv_[k];
+      const float2 yn = yy_[k] + yp * pp_[k] + ys * s1;
+      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, yn) : yn;
+      yy_[k] = make_float2(0.f, 0.f);
     }
   }
   __syncthreads();
   fft_rows<false>(sm, nr, A.tab.px);
   float2* __restrict__ w = A.B.w + off;
-  for (int l = 0; l < nr; ++l) {
-#pragma unroll 4
-    for (int c = threadIdx.x; c < nx; c += blockDim.x) w[l * nx + c] = sm[l * rs + (pad ? c + (c >> 4) : c)];
-  }
+#pragma unroll 8
+  for (int k = threadIdx.x; k < cnt; k += blockDim.x) w[k] = sm[pad ? k + (k >> 4) : k];
 }
 
 // ---------------------------------------------------------------------------
 // cols: column FFT, preconditioner multiply, inverse column FFT (in place).
 // ---------------------------------------------------------------------------
-template <int TC>
+template <int TC, bool LEARNED>
 __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
   const int slot = A.slot0 + blockIdx.y;
   const int mode = A.B.slots[slot].mode;
   if (!cols_active(mode, half)) return;
   const long long n = (long long)A.g.nz * A.g.nx;
-  cols_pass<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.slots[slot].freq, A.shift, A.adjoint, blockIdx.x * TC, A.lp);
+  if (LEARNED)
+    cols_pass_plane<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.sym + slot * n, A.adjoint, blockIdx.x * TC);
+  else
+    cols_pass_fixed<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.slots[slot].freq, A.shift, A.adjoint,
+                        blockIdx.x * TC);
 }
 
 // ---------------------------------------------------------------------------
@@ -232,22 +239,19 @@ __global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
   const int nr = min(A.rows, g.nz - z0);
   const long long goff = (long long)z0 * g.nx;
   float2* __restrict__ w = A.B.w + slot * n + goff;
-  const int nx = g.nx, rs = nsr_row_stride(nx);
-  const bool pad = nsr_row_padded(nx);
-  for (int l = 0; l < nr; ++l)
-#pragma unroll 4
-    for (int c = threadIdx.x; c < nx; c += blockDim.x) sm[l * rs + (pad ? c + (c >> 4) : c)] = w[l * nx + c];
+  const bool pad = nsr_row_padded(g.nx);   // flat index k + k/16, as in k_fwd
+  const int cnt = nr * g.nx;
+#pragma unroll 8
+  for (int k = threadIdx.x; k < cnt; k += blockDim.x) sm[pad ? k + (k >> 4) : k] = w[k];
   __syncthreads();
   fft_rows<true>(sm, nr, A.tab.px);
   __syncthreads();
   const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
-  for (int l = 0; l < nr; ++l)
-#pragma unroll 4
-    for (int c = threadIdx.x; c < nx; c += blockDim.x) {
-      const int k = l * nx + c;
-      const float2 v = sm[l * rs + (pad ? c + (c >> 4) : c)];
-      w[k] = G.post ? gain_mul(G.post, goff + k, G.conj, v) : v;
-    }
+#pragma unroll 8
+  for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+    const float2 v = sm[pad ? k + (k >> 4) : k];
+    w[k] = G.post ? gain_mul(G.post, goff + k, G.conj, v) : v;
+  }
 }
 
 __device__ void pop_next(const SolveArgs& A, SlotState& S) {
@@ -797,7 +801,7 @@ static Layout layout(const NsrGrid* g, int n_slots) {
   L.arrive = off; off += nsr_align(sizeof(int) * n_slots);
   L.queue = off; off += nsr_align(sizeof(int) * 4);
   L.partials = off; off += nsr_align(sizeof(double) * NSR_NPART * (size_t)L.nb_inv * n_slots);
-  L.vec = off; off += 7 * nsr_align(sizeof(float2) * n * n_slots);
+  L.vec = off; off += 8 * nsr_align(sizeof(float2) * n * n_slots);
   L.x = off; off += nsr_align(sizeof(double2) * n * 2 * n_slots);
   L.total = off;
   return L;
@@ -887,8 +891,8 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     A.B.warm = A.B.queue + 2;
     A.B.partials = (double*)(ws + L.partials);
     const size_t vb = nsr_align(sizeof(float2) * n * n_slots);
-    float2** vecs[7] = {&A.B.r, &A.B.rh, &A.B.p, &A.B.v, &A.B.t, &A.B.y, &A.B.w};
-    for (int q = 0; q < 7; ++q) *vecs[q] = (float2*)(ws + L.vec + q * vb);
+    float2** vecs[8] = {&A.B.r, &A.B.rh, &A.B.p, &A.B.v, &A.B.t, &A.B.y, &A.B.w, &A.B.sym};
+    for (int q = 0; q < 8; ++q) *vecs[q] = (float2*)(ws + L.vec + q * vb);
     A.B.x = (double2*)(ws + L.x);
     A.mat = nsr_planes(coef, (long long)grid->nz * grid->nx);
     A.freq = freq_hz;
@@ -927,8 +931,10 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     const int nb_st = stencil_ctas(grid);
     const bool pairs = grid->nx % 2 == 0;
     NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_cols<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_cols<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_cols<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    NSR_TRY(cudaFuncSetAttribute(k_cols<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(k_rinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
 
     k_solve_init<<<64, 256, 0, st>>>(A, n_slots);
@@ -961,8 +967,13 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
       if (which == 0) {
         k_fwd<<<g_fwd, 256, fwd_smem, sq>>>(Ag, half);
       } else if (which == 1) {
-        if (A.tc == 16) k_cols<16><<<g_col, 512, col_smem, sq>>>(Ag, half);
-        else k_cols<8><<<g_col, 512, col_smem, sq>>>(Ag, half);
+        if (A.lp) {
+          if (A.tc == 16) k_cols<16, true><<<g_col, 512, col_smem, sq>>>(Ag, half);
+          else k_cols<8, true><<<g_col, 512, col_smem, sq>>>(Ag, half);
+        } else {
+          if (A.tc == 16) k_cols<16, false><<<g_col, 512, col_smem, sq>>>(Ag, half);
+          else k_cols<8, false><<<g_col, 512, col_smem, sq>>>(Ag, half);
+        }
       } else if (which == 2) {
         if (A.adjoint) k_res<true><<<g_res, 256, 0, sq>>>(Ag);
         else k_res<false><<<g_res, 256, 0, sq>>>(Ag);

@@ -68,9 +68,10 @@ def test_workspace_queries(lib):
     g = grid()
     n = 768 * 1024
     ws = lib.nsr_solve_workspace_size(ctypes.byref(g), 16)
-    # seven complex64 vectors and two complex128 iterates per slot, plus tables
-    assert ws >= 16 * n * (7 * 8 + 2 * 16)
-    assert ws < 16 * n * (7 * 8 + 2 * 16) + (1 << 22)
+    # seven complex64 vectors, the learned multiplier plane and two complex128
+    # iterates per slot, plus tables
+    assert ws >= 16 * n * (8 * 8 + 2 * 16)
+    assert ws < 16 * n * (8 * 8 + 2 * 16) + (1 << 22)
     assert lib.nsr_solve_workspace_size(ctypes.byref(grid(nz=7 * 16)), 4) == 0   # 112 = 2^4 * 7
     assert lib.nsr_solve_workspace_size(ctypes.byref(g), 0) == 0
     assert lib.nsr_precondition_workspace_size(ctypes.byref(g), 2) >= 2 * n * 8
