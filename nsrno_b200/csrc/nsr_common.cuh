@@ -180,6 +180,11 @@ struct FftPlan {
   int nst;
   int radix[NSR_MAX_RADIX_STAGES];
   const float2* tw;   // tw[k] = exp(-2 pi i k / n), k < n
+  // Twiddles of the specialised transforms, stage by stage: for every stage
+  // with m = L/R > 1 (L its length, R its radix), (R-1) m entries, entry
+  // (k-1) m + j holding tw[j k n/L] for 1 <= k < R, j < m.  Butterflies j of
+  // one warp read consecutive entries for each k.
+  const float2* tws;
 };
 
 template <int R, bool INV>
@@ -346,11 +351,26 @@ __host__ __device__ constexpr int nsr_stage_len(int n, int stage) {
   return len;
 }
 
+// Offset (in float2) of the twiddle rows of the stage of length `len` in
+// FftPlan::tws; with len = 0, the total number of entries.
+__host__ __device__ constexpr int nsr_twiddle_offset(int n, int len) {
+  RadixList L = nsr_radix_list(n);
+  int l = n, off = 0;
+  for (int s = 0; s < L.nst; ++s) {
+    if (l == len) return off;
+    const int m = l / L.r[s];
+    if (m > 1) off += m * (L.r[s] - 1);
+    l = m;
+  }
+  return off;
+}
+
 // One stage, everything but the number of lines known at compile time.
 // Elements: s[l*LS + k*ES].  LF: thread index runs over lines first.
 template <int N, int R, int L, bool INV, bool LF, int LS, int ES, bool PAD>
-__device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __restrict__ tw) {
-  constexpr int m = L / R, per_line = N / R, tstep = N / L;
+__device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __restrict__ tws) {
+  constexpr int m = L / R, per_line = N / R;
+  const float2* __restrict__ tst = tws + nsr_twiddle_offset(N, L);
   constexpr int U = R >= 16 ? 1 : 2;   // butterflies in flight per thread
   const int nb = nl * per_line;
   auto at = [](int k) { return PAD ? k + (k >> 4) : k; };
@@ -375,18 +395,23 @@ __device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __rest
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      // The stage with m == 1 (the last forward, first inverse) has unit twiddles.
+      // The stage with m == 1 (the last forward, first inverse) has unit
+      // twiddles.  Otherwise entry k of butterfly j sits at (k-1) m + j.
+      auto twiddle = [&](float2* x) {
+        if constexpr (m > 1) {
+          const float2* __restrict__ tj = tst + jj[u];
+#pragma unroll
+          for (int k = 1; k < R; ++k) {
+            const float2 w = __ldg(tj + (k - 1) * m);
+            x[k] = x[k] * (INV ? conjc(w) : w);
+          }
+        }
+      };
       if (!INV) {
         small_dft<R, false>(v[u]);
-        if constexpr (m > 1) {
-#pragma unroll
-          for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * __ldg(&tw[jj[u] * k * tstep]);
-        }
+        twiddle(v[u]);
       } else {
-        if constexpr (m > 1) {
-#pragma unroll
-          for (int k = 1; k < R; ++k) v[u][k] = v[u][k] * conjc(__ldg(&tw[jj[u] * k * tstep]));
-        }
+        twiddle(v[u]);
         small_dft<R, true>(v[u]);
       }
     }
@@ -401,47 +426,47 @@ __device__ __forceinline__ void ct_stage(float2* s, int nl, const float2* __rest
 }
 
 template <int N, int S, bool LF, int LS, int ES, bool PAD>
-__device__ __forceinline__ void ct_forward(float2* s, int nl, const float2* __restrict__ tw) {
+__device__ __forceinline__ void ct_forward(float2* s, int nl, const float2* __restrict__ tws) {
   constexpr RadixList RL = nsr_radix_list(N);
   if constexpr (S < RL.nst) {
     constexpr int R = RL.r[S];
     constexpr int L = nsr_stage_len(N, S);
-    ct_stage<N, R, L, false, LF, LS, ES, PAD>(s, nl, tw);
+    ct_stage<N, R, L, false, LF, LS, ES, PAD>(s, nl, tws);
     __syncthreads();
-    ct_forward<N, S + 1, LF, LS, ES, PAD>(s, nl, tw);
+    ct_forward<N, S + 1, LF, LS, ES, PAD>(s, nl, tws);
   }
 }
 
 // Forward stages S .. STOP-1.
 template <int N, int S, int STOP, bool LF, int LS, int ES, bool PAD>
-__device__ __forceinline__ void ct_forward_upto(float2* s, int nl, const float2* __restrict__ tw) {
+__device__ __forceinline__ void ct_forward_upto(float2* s, int nl, const float2* __restrict__ tws) {
   if constexpr (S < STOP) {
     constexpr RadixList RL = nsr_radix_list(N);
     constexpr int R = RL.r[S];
     constexpr int L = nsr_stage_len(N, S);
-    ct_stage<N, R, L, false, LF, LS, ES, PAD>(s, nl, tw);
+    ct_stage<N, R, L, false, LF, LS, ES, PAD>(s, nl, tws);
     __syncthreads();
-    ct_forward_upto<N, S + 1, STOP, LF, LS, ES, PAD>(s, nl, tw);
+    ct_forward_upto<N, S + 1, STOP, LF, LS, ES, PAD>(s, nl, tws);
   }
 }
 
 template <int N, int S, bool LF, int LS, int ES, bool PAD>
-__device__ __forceinline__ void ct_inverse(float2* s, int nl, const float2* __restrict__ tw) {
+__device__ __forceinline__ void ct_inverse(float2* s, int nl, const float2* __restrict__ tws) {
   constexpr RadixList RL = nsr_radix_list(N);
   if constexpr (S >= 0) {
     constexpr int R = RL.r[S];
     constexpr int L = nsr_stage_len(N, S);
-    ct_stage<N, R, L, true, LF, LS, ES, PAD>(s, nl, tw);
+    ct_stage<N, R, L, true, LF, LS, ES, PAD>(s, nl, tws);
     __syncthreads();
-    ct_inverse<N, S - 1, LF, LS, ES, PAD>(s, nl, tw);
+    ct_inverse<N, S - 1, LF, LS, ES, PAD>(s, nl, tws);
   }
 }
 
 template <int N, bool INV, bool LF, int LS, int ES, bool PAD>
-__device__ __forceinline__ void ct_fft(float2* s, int nl, const float2* __restrict__ tw) {
+__device__ __forceinline__ void ct_fft(float2* s, int nl, const float2* __restrict__ tws) {
   constexpr RadixList RL = nsr_radix_list(N);
-  if (!INV) ct_forward<N, 0, LF, LS, ES, PAD>(s, nl, tw);
-  else ct_inverse<N, RL.nst - 1, LF, LS, ES, PAD>(s, nl, tw);
+  if (!INV) ct_forward<N, 0, LF, LS, ES, PAD>(s, nl, tws);
+  else ct_inverse<N, RL.nst - 1, LF, LS, ES, PAD>(s, nl, tws);
 }
 
 // Row layout in shared memory: the specialised sizes insert one pad element
@@ -460,13 +485,13 @@ __host__ __device__ inline int nsr_row_stride(int n) { return nsr_row_padded(n) 
 template <bool INV>
 __device__ void fft_rows(float2* s, int nl, const FftPlan& P) {
   switch (P.n) {
-    case 256: ct_fft<256, INV, false, 256 + 16, 1, true>(s, nl, P.tw); return;
-    case 384: ct_fft<384, INV, false, 384 + 24, 1, true>(s, nl, P.tw); return;
-    case 512: ct_fft<512, INV, false, 512 + 32, 1, true>(s, nl, P.tw); return;
-    case 768: ct_fft<768, INV, false, 768 + 48, 1, true>(s, nl, P.tw); return;
-    case 1024: ct_fft<1024, INV, false, 1024 + 64, 1, true>(s, nl, P.tw); return;
-    case 1536: ct_fft<1536, INV, false, 1536 + 96, 1, true>(s, nl, P.tw); return;
-    case 2048: ct_fft<2048, INV, false, 2048 + 128, 1, true>(s, nl, P.tw); return;
+    case 256: ct_fft<256, INV, false, 256 + 16, 1, true>(s, nl, P.tws); return;
+    case 384: ct_fft<384, INV, false, 384 + 24, 1, true>(s, nl, P.tws); return;
+    case 512: ct_fft<512, INV, false, 512 + 32, 1, true>(s, nl, P.tws); return;
+    case 768: ct_fft<768, INV, false, 768 + 48, 1, true>(s, nl, P.tws); return;
+    case 1024: ct_fft<1024, INV, false, 1024 + 64, 1, true>(s, nl, P.tws); return;
+    case 1536: ct_fft<1536, INV, false, 1536 + 96, 1, true>(s, nl, P.tws); return;
+    case 2048: ct_fft<2048, INV, false, 2048 + 128, 1, true>(s, nl, P.tws); return;
     default: fft_lines<INV>(s, nl, P.n, 1, false, P); return;
   }
 }
@@ -475,13 +500,13 @@ __device__ void fft_rows(float2* s, int nl, const FftPlan& P) {
 template <bool INV, int TC>
 __device__ void fft_cols(float2* s, const FftPlan& P) {
   switch (P.n) {
-    case 256: ct_fft<256, INV, true, 1, TC, false>(s, TC, P.tw); return;
-    case 384: ct_fft<384, INV, true, 1, TC, false>(s, TC, P.tw); return;
-    case 512: ct_fft<512, INV, true, 1, TC, false>(s, TC, P.tw); return;
-    case 768: ct_fft<768, INV, true, 1, TC, false>(s, TC, P.tw); return;
-    case 1024: ct_fft<1024, INV, true, 1, TC, false>(s, TC, P.tw); return;
-    case 1536: ct_fft<1536, INV, true, 1, TC, false>(s, TC, P.tw); return;
-    case 2048: ct_fft<2048, INV, true, 1, TC, false>(s, TC, P.tw); return;
+    case 256: ct_fft<256, INV, true, 1, TC, false>(s, TC, P.tws); return;
+    case 384: ct_fft<384, INV, true, 1, TC, false>(s, TC, P.tws); return;
+    case 512: ct_fft<512, INV, true, 1, TC, false>(s, TC, P.tws); return;
+    case 768: ct_fft<768, INV, true, 1, TC, false>(s, TC, P.tws); return;
+    case 1024: ct_fft<1024, INV, true, 1, TC, false>(s, TC, P.tws); return;
+    case 1536: ct_fft<1536, INV, true, 1, TC, false>(s, TC, P.tws); return;
+    case 2048: ct_fft<2048, INV, true, 1, TC, false>(s, TC, P.tws); return;
     default: fft_lines<INV>(s, TC, 1, TC, true, P); return;
   }
 }
@@ -492,11 +517,11 @@ __device__ void fft_cols(float2* s, const FftPlan& P) {
 // m == 1: contiguous groups of R elements and unit twiddles).  `mul(l, k)`
 // returns the factor of line l (column of the tile) at digit-reversed position k.
 template <int N, int TC, typename MUL>
-__device__ __forceinline__ void ct_cols_fused(float2* s, const float2* __restrict__ tw, MUL mul) {
+__device__ __forceinline__ void ct_cols_fused(float2* s, const float2* __restrict__ tws, MUL mul) {
   constexpr RadixList RL = nsr_radix_list(N);
   constexpr int LAST = RL.nst - 1;
   constexpr int R = RL.r[LAST];
-  if constexpr (LAST > 0) ct_forward_upto<N, 0, LAST, true, 1, TC, false>(s, TC, tw);
+  if constexpr (LAST > 0) ct_forward_upto<N, 0, LAST, true, 1, TC, false>(s, TC, tws);
   constexpr int per_line = N / R;
   const int nb = TC * per_line;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
@@ -513,7 +538,7 @@ __device__ __forceinline__ void ct_cols_fused(float2* s, const float2* __restric
     for (int q = 0; q < R; ++q) base[q * TC] = v[q];
   }
   __syncthreads();
-  if constexpr (LAST > 0) ct_inverse<N, LAST - 1, true, 1, TC, false>(s, TC, tw);
+  if constexpr (LAST > 0) ct_inverse<N, LAST - 1, true, 1, TC, false>(s, TC, tws);
 }
 
 // Column pass with the fused middle stage for the specialised sizes; other
@@ -522,13 +547,13 @@ __device__ __forceinline__ void ct_cols_fused(float2* s, const float2* __restric
 template <int TC, typename MUL>
 __device__ __forceinline__ bool fft_cols_fused(float2* s, const FftPlan& P, MUL mul) {
   switch (P.n) {
-    case 256: ct_cols_fused<256, TC>(s, P.tw, mul); return true;
-    case 384: ct_cols_fused<384, TC>(s, P.tw, mul); return true;
-    case 512: ct_cols_fused<512, TC>(s, P.tw, mul); return true;
-    case 768: ct_cols_fused<768, TC>(s, P.tw, mul); return true;
-    case 1024: ct_cols_fused<1024, TC>(s, P.tw, mul); return true;
-    case 1536: ct_cols_fused<1536, TC>(s, P.tw, mul); return true;
-    case 2048: ct_cols_fused<2048, TC>(s, P.tw, mul); return true;
+    case 256: ct_cols_fused<256, TC>(s, P.tws, mul); return true;
+    case 384: ct_cols_fused<384, TC>(s, P.tws, mul); return true;
+    case 512: ct_cols_fused<512, TC>(s, P.tws, mul); return true;
+    case 768: ct_cols_fused<768, TC>(s, P.tws, mul); return true;
+    case 1024: ct_cols_fused<1024, TC>(s, P.tws, mul); return true;
+    case 1536: ct_cols_fused<1536, TC>(s, P.tws, mul); return true;
+    case 2048: ct_cols_fused<2048, TC>(s, P.tws, mul); return true;
     default: return false;
   }
 }

@@ -159,6 +159,28 @@ __global__ void k_fft_tables(int n, FftPlan plan, float2* tw, float* s2) {
   }
 }
 
+// Per-stage twiddle rows of the specialised transforms (layout: FftPlan::tws),
+// with the same rounding of the same angles as k_fft_tables.
+__global__ void k_fft_stage_twiddles(int n, FftPlan plan, float2* tws, int total) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    int l = n, off = 0;
+    for (int st = 0; st < plan.nst; ++st) {
+      const int r = plan.radix[st], m = l / r;
+      if (m > 1) {
+        if (e < off + m * (r - 1)) {
+          const int k = (e - off) / m + 1, j = (e - off) % m;
+          double sn, cs;
+          sincospi(-2.0 * (j * k * (n / l)) / n, &sn, &cs);
+          tws[e] = make_float2((float)cs, (float)sn);
+          break;
+        }
+        off += m * (r - 1);
+      }
+      l = m;
+    }
+  }
+}
+
 int nsr_prec_setup(const NsrGrid* g, PrecTables* t, void* table_mem, cudaStream_t st) {
   char* p = (char*)table_mem;
   t->px.n = g->nx;
@@ -169,15 +191,23 @@ int nsr_prec_setup(const NsrGrid* g, PrecTables* t, void* table_mem, cudaStream_
   float2* twz = (float2*)p; p += nsr_align(sizeof(float2) * g->nz);
   float* s2x = (float*)p; p += nsr_align(sizeof(float) * g->nx);
   float* s2z = (float*)p; p += nsr_align(sizeof(float) * g->nz);
+  const int nwx = nsr_twiddle_offset(g->nx, 0), nwz = nsr_twiddle_offset(g->nz, 0);
+  float2* twsx = (float2*)p; p += nsr_align(sizeof(float2) * nwx);
+  float2* twsz = (float2*)p; p += nsr_align(sizeof(float2) * nwz);
   t->px.tw = twx; t->pz.tw = twz; t->s2x = s2x; t->s2z = s2z;
+  t->px.tws = twsx; t->pz.tws = twsz;
   k_fft_tables<<<(g->nx + 255) / 256, 256, 0, st>>>(g->nx, t->px, twx, s2x);
   k_fft_tables<<<(g->nz + 255) / 256, 256, 0, st>>>(g->nz, t->pz, twz, s2z);
+  if (nwx > 0) k_fft_stage_twiddles<<<(nwx + 255) / 256, 256, 0, st>>>(g->nx, t->px, twsx, nwx);
+  if (nwz > 0) k_fft_stage_twiddles<<<(nwz + 255) / 256, 256, 0, st>>>(g->nz, t->pz, twsz, nwz);
   return last_error();
 }
 
 size_t nsr_prec_table_bytes(const NsrGrid* g) {
   return nsr_align(sizeof(float2) * g->nx) + nsr_align(sizeof(float2) * g->nz) +
-         nsr_align(sizeof(float) * g->nx) + nsr_align(sizeof(float) * g->nz);
+         nsr_align(sizeof(float) * g->nx) + nsr_align(sizeof(float) * g->nz) +
+         nsr_align(sizeof(float2) * nsr_twiddle_offset(g->nx, 0)) +
+         nsr_align(sizeof(float2) * nsr_twiddle_offset(g->nz, 0));
 }
 
 // Column pass: forward DIF along z, multiply by the shifted-Laplace symbol in
