@@ -389,7 +389,7 @@ def run_ours(args):
                                    "preconditioner (network set-up of each step's bins timed); plain Krylov "
                                    "(fixed shifted-Laplace, shift 0.15) under plain_krylov",
                        "systems_per_step": SYSTEMS_PER_STEP, "n_slots": N_SLOTS, "grid_zx": [rec.nz, rec.nx],
-                       "l2": f"inputs larger than L2: {slots * n * 88 / 1e9:.2f} GB resident Krylov state per GPU",
+                       "l2": f"inputs larger than L2: {slots * n * 96 / 1e9:.2f} GB resident Krylov state per GPU",
                        "parallelism": f"frequency-sharded x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
