@@ -119,6 +119,39 @@ def test_solves_through_learned_preconditioner_match_lu(cuda, gold, adjoint):
         assert rel(res_g.fields[s].cpu().numpy().ravel(), ref) < 1e-5
 
 
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_reused_slot_rebuilds_the_learned_multiplier(cuda, gold, adjoint):
+    """One slot serving systems of alternating frequencies gives, system by
+    system, exactly the iterations and receiver IQ of solving each system on
+    its own: the slot's learned multiplier plane is rebuilt for every system
+    it starts (a stale plane would only cost iterations, which is what this
+    compares)."""
+    from nsrno_b200 import solve_batched
+    from nsrno_b200.learned import LearnedPreconditioner
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    order = np.lexsort((f, th))          # consecutive systems alternate in frequency
+    f, th = f[order], th[order]
+    assert np.all(f[1:] != f[:-1])
+    params = gold["params"].astype(np.float32) * 0.5
+    params[8] = math.log(0.2)
+    st = LearnedPreconditioner(params, device=cuda).setup(med, rec.frequencies)
+    rng = np.random.default_rng(11)
+    rhs = (rng.standard_normal((len(f), rec.nz, rec.nx)) + 1j * rng.standard_normal((len(f), rec.nz, rec.nx)))
+    rhs = torch.as_tensor(rhs.astype(np.complex64), device=cuda)
+
+    def run(sel):
+        kw = dict(rhs=rhs[sel], adjoint=True) if adjoint else dict(angles=th[sel])
+        return solve_batched(med, f[sel], tolerance=1e-7, max_iterations=3000, learned=st, n_slots=1, **kw)
+
+    together = run(slice(None))
+    assert together.reasons() == ["converged"] * len(f)
+    for s in range(len(f)):
+        alone = run(slice(s, s + 1))
+        assert int(alone.iterations[0]) == int(together.iterations[s])
+        assert torch.equal(alone.iq[0], together.iq[s])
+
+
 def oracle_training_gradient(rec, params, freqs, rhs, rx, target, steps, channel_weight):
     """Float64 autograd of the training objective on the oracle: mean over
     systems of log residual + channel_weight * log receiver error."""
