@@ -173,12 +173,14 @@ int nsr_precondition(const NsrGrid* grid, const double* freq_hz, int32_t n_syste
  * of cudaMalloc, or inside a host application that owns all device memory).
  * This entry point has no counterpart in the reference.  Same arguments and
  * result as nsr_precondition, but its scratch space is a fixed 16 MiB
- * file-scope device array (held by every GPU that loads the library until the
- * process exits), so nothing is allocated.  Requests whose
+ * file-scope device array (reserved on each device where the library's module
+ * is loaded -- with lazy module loading, at the first call on that device --
+ * and held until the process exits), so nothing is allocated.  Requests whose
  * nsr_precondition_workspace_size exceeds 16 MiB return NSR_ERR_CAPACITY
- * (e.g. at most two 1024 x 768 systems per call).  The first call on a device
- * looks up the array's device address with that device current; make that
- * first call before any stream capture.  Every call shares the array and it
+ * (e.g. at most two 1024 x 768 systems per call).  The first call in a CUDA
+ * context (normally the device's primary context) looks up the array's device
+ * address with that device current and caches it for that context only; make
+ * that first call before any stream capture.  Every call shares the array and it
  * keeps the last call's contents: calls that overlap on the GPU (different
  * streams or threads, same device) race and must be serialised by the caller. */
 int nsr_precondition_noalloc(const NsrGrid* grid, const double* freq_hz, int32_t n_systems,

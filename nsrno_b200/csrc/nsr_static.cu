@@ -9,35 +9,80 @@
 // lives in a fixed file-scope device array instead of a caller workspace.
 #include "nsr_internal.cuh"
 
+#include <cuda.h>
 #include <mutex>
 
 // 16 MiB: tables plus two 1024 x 768 complex64 fields, or 32 fields of 256 x 256.
 #define NSR_STATIC_SCRATCH_BYTES ((size_t)16 << 20)
-#define NSR_STATIC_MAX_DEVICES 64
+#define NSR_STATIC_MAX_CONTEXTS 64
 
-// Every GPU that loads this library holds this array until the process exits.
+// Reserved on each device where this module is loaded (with CUDA's lazy module
+// loading, at the first use of nsr_precondition_noalloc on that device) and
+// held until the context is destroyed or the process exits.
 static __device__ __align__(256) unsigned char g_prec_scratch[NSR_STATIC_SCRATCH_BYTES];
 
 namespace {
-std::mutex g_scratch_mutex;
-void* g_scratch_addr[NSR_STATIC_MAX_DEVICES] = {nullptr};
+typedef CUresult (CUDAAPI* CtxCurrentFn)(CUcontext*);
+typedef CUresult (CUDAAPI* CtxIdFn)(CUcontext, unsigned long long*);
 
-// Device address of g_prec_scratch on the current device.  In host code the
-// symbol name is only a host-side handle, so the address is looked up once
-// per device, with that device current, and cached.
+std::mutex g_scratch_mutex;
+CtxCurrentFn g_ctx_current = nullptr;
+CtxIdFn g_ctx_id = nullptr;
+bool g_entry_points_tried = false;
+// (context id, device address of g_prec_scratch in that context)
+unsigned long long g_cache_id[NSR_STATIC_MAX_CONTEXTS] = {0};
+void* g_cache_addr[NSR_STATIC_MAX_CONTEXTS] = {nullptr};
+int g_cache_next = 0;
+
+// Unique id of the context current on this thread (never reused within the
+// process, so a context created after cudaDeviceReset gets a new one); 0 when
+// no context is current or the driver cannot say.
+unsigned long long current_context_id() {
+  if (!g_entry_points_tried) {
+    g_entry_points_tried = true;
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 4000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_current = (CtxCurrentFn)fn;
+    fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_id = (CtxIdFn)fn;
+  }
+  if (!g_ctx_current || !g_ctx_id) return 0;
+  CUcontext ctx = nullptr;
+  if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  unsigned long long id = 0;
+  if (g_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_prec_scratch in the current context.  In host code the
+// symbol name is only a host-side handle, so the address is looked up with
+// the device current (cudaGetSymbolAddress) and cached per CUDA context: the
+// module, and with it the array, can sit at another address in another
+// context of the same device or after cudaDeviceReset.
 int scratch_address(void** out) {
   int dev = -1;
   cudaError_t ce = cudaGetDevice(&dev);
   if (ce != cudaSuccess) return (int)ce;
-  if (dev < 0 || dev >= NSR_STATIC_MAX_DEVICES) return NSR_ERR_CAPACITY;
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    ce = cudaGetSymbolAddress(&p, g_prec_scratch);
-    if (ce != cudaSuccess) return (int)ce;
-    g_scratch_addr[dev] = p;
+  unsigned long long id = current_context_id();
+  if (id != 0) {
+    for (int k = 0; k < NSR_STATIC_MAX_CONTEXTS; ++k)
+      if (g_cache_id[k] == id) { *out = g_cache_addr[k]; return 0; }
   }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  ce = cudaGetSymbolAddress(&p, g_prec_scratch);   // makes the device's primary context current if none is
+  if (ce != cudaSuccess) return (int)ce;
+  if (id == 0) id = current_context_id();
+  if (id != 0) {
+    g_cache_id[g_cache_next] = id;
+    g_cache_addr[g_cache_next] = p;
+    g_cache_next = (g_cache_next + 1) % NSR_STATIC_MAX_CONTEXTS;
+  }
+  *out = p;
   return 0;
 }
 }  // namespace

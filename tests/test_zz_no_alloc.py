@@ -42,14 +42,6 @@ def _with_workspace(lib, grid, freqs, x, shift, adjoint, stream):
     return y
 
 
-def _no_alloc(lib, grid, freqs, x, shift, adjoint, stream):
-    y = torch.empty_like(x)
-    code = lib.nsr_precondition_noalloc(ctypes.byref(grid), _ptr(freqs), x.shape[0], shift, adjoint,
-                                        _ptr(x), _ptr(y), stream)
-    assert code == 0, lib.nsr_error_string(code)
-    return y
-
-
 def test_no_alloc_preconditioner_matches_workspace_version_twice(cuda):
     from nsrno_b200 import _lib
     lib = _lib.load()
@@ -63,7 +55,15 @@ def test_no_alloc_preconditioner_matches_workspace_version_twice(cuda):
         f = torch.tensor(freqs, dtype=torch.float64, device=cuda)
         x = torch.as_tensor((rng.standard_normal((len(freqs), nz, nx)) +
                              1j * rng.standard_normal((len(freqs), nz, nx))).astype(np.complex64), device=cuda)
-        got = _no_alloc(lib, grid, f, x, shift, adjoint, stream)
+        got = torch.empty_like(x)
+        torch.cuda.synchronize()
+        before = torch.cuda.memory_allocated(cuda)
+        code = lib.nsr_precondition_noalloc(ctypes.byref(grid), _ptr(f), x.shape[0], shift, adjoint,
+                                            _ptr(x), _ptr(got), stream)
+        torch.cuda.synchronize()
+        assert code == 0, lib.nsr_error_string(code)
+        # the call itself takes no memory from the caller's allocator
+        assert torch.cuda.memory_allocated(cuda) == before
         want = _with_workspace(lib, grid, f, x, shift, adjoint, stream)
         torch.cuda.synchronize()
         err = float((got - want).abs().norm() / want.abs().norm())
