@@ -36,7 +36,8 @@ enum {
   NSR_BREAKDOWN = 2,
   NSR_DIVERGED = 3,
   NSR_NONFINITE = 4,
-  NSR_NOT_RUN = 5
+  NSR_TIMEOUT = 5,        /* NsrSolveParams.time_limit_s ran out first        */
+  NSR_NOT_RUN = 6
 };
 
 /* Library error codes (cudaError_t values stay below 1000). */
@@ -45,7 +46,8 @@ enum {
   NSR_ERR_UNSUPPORTED_SIZE = 1002, /* nz or nx not 2^a 3^b in [8, 2048]       */
   NSR_ERR_WORKSPACE = 1003,      /* workspace smaller than the query returned */
   NSR_ERR_INTERNAL = 1004,       /* solver loop did not drain its queue       */
-  NSR_ERR_CAPACITY = 1005        /* request exceeds a fixed capacity          */
+  NSR_ERR_CAPACITY = 1005,       /* request exceeds a fixed capacity          */
+  NSR_ERR_TIMEOUT = 1006         /* a kernel gave up waiting on its copy ring */
 };
 
 /* Grid, PML and acquisition geometry of one record.  Mirrors the reference
@@ -62,6 +64,20 @@ typedef struct NsrGrid {
   double alpha_power;        /* power-law exponent y of alpha [dB/cm/MHz^y]    */
   double aperture_half_width;/* cosine taper half width of the source line [m] */
 } NsrGrid;
+
+/* Launch shapes of nsr_solve_batched (all zero: the built-in defaults).
+ * Chosen per grid and device by the autotuner of nsrno_b200.tune; every
+ * choice gives bitwise the same results for a fixed slot count. */
+typedef struct NsrTiles {
+  int32_t stencil_width;     /* columns per stencil work item: 256 or 512      */
+  int32_t stencil_depth;     /* row buffers of the stencil's copy ring: 4..8   */
+  int32_t stencil_rows;      /* rows per stencil work item (band): 4..64       */
+  int32_t stencil_ctas;      /* resident stencil CTAs per SM (0: occupancy)    */
+  int32_t cols_width;        /* columns per column-FFT CTA: 8 or 16            */
+  int32_t row_tile;          /* rows per row-FFT CTA: 1..8                     */
+  int32_t slot_groups;       /* independent slot groups on graph branches: 1, 2 */
+  int32_t reserved;
+} NsrTiles;
 
 /* Krylov parameters of nsr_solve_batched. */
 /* Learned preconditioner of the reference's LearnedPreconditioner
@@ -108,6 +124,11 @@ typedef struct NsrSolveParams {
   const NsrLearned* learned; /* host pointer; NULL: fixed shifted-Laplace
                                 preconditioner. Otherwise the learned one
                                 (`shift` is then unused)                        */
+  double time_limit_s;       /* wall-clock limit per system measured on the
+                                device from its start (0: none); a system still
+                                iterating then stops at its next true residual
+                                with status NSR_TIMEOUT                          */
+  const NsrTiles* tiles;     /* host pointer; NULL: built-in launch shapes      */
 } NsrSolveParams;
 
 /* Optional host-side statistics of one nsr_solve_batched call. */

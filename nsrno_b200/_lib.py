@@ -11,9 +11,10 @@ from pathlib import Path
 
 LIBRARY = Path(__file__).resolve().parent / "libnsrno_b200.so"
 
-CONVERGED, ITERATION_BUDGET, BREAKDOWN, DIVERGED, NONFINITE, NOT_RUN = range(6)
+CONVERGED, ITERATION_BUDGET, BREAKDOWN, DIVERGED, NONFINITE, TIMEOUT, NOT_RUN = range(7)
 REASONS = {CONVERGED: "converged", ITERATION_BUDGET: "iteration_budget", BREAKDOWN: "breakdown",
-           DIVERGED: "diverged", NONFINITE: "nonfinite", NOT_RUN: "not_run"}
+           DIVERGED: "diverged", NONFINITE: "nonfinite", TIMEOUT: "timeout", NOT_RUN: "not_run"}
+ERR_TIMEOUT = 1006
 
 EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_material", "nsr_apply",
            "nsr_precondition_workspace_size", "nsr_precondition", "nsr_precondition_noalloc", "nsr_plane_wave_rhs",
@@ -40,13 +41,27 @@ class NsrLearned(ctypes.Structure):
                 ("n_gain", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
+class NsrTiles(ctypes.Structure):
+    _fields_ = [("stencil_width", ctypes.c_int32), ("stencil_depth", ctypes.c_int32),
+                ("stencil_rows", ctypes.c_int32), ("stencil_ctas", ctypes.c_int32),
+                ("cols_width", ctypes.c_int32), ("row_tile", ctypes.c_int32),
+                ("slot_groups", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    FIELDS = ("stencil_width", "stencil_depth", "stencil_rows", "stencil_ctas", "cols_width", "row_tile",
+              "slot_groups")
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k in self.FIELDS}
+
+
 class NsrSolveParams(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double), ("restart_factor", ctypes.c_double),
                 ("warm_gate", ctypes.c_double), ("max_iterations", ctypes.c_int32), ("replace_every", ctypes.c_int32),
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
                 ("graph_iterations", ctypes.c_int32), ("profile_iterations", ctypes.c_int32),
                 ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("learned", ctypes.POINTER(NsrLearned))]
+                ("learned", ctypes.POINTER(NsrLearned)), ("time_limit_s", ctypes.c_double),
+                ("tiles", ctypes.POINTER(NsrTiles))]
 
 
 class NsrDenseGrid(ctypes.Structure):

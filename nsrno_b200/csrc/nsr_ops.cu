@@ -19,6 +19,7 @@ extern "C" const char* nsr_error_string(int code) {
     case NSR_ERR_WORKSPACE: return "nsrno_b200: workspace too small";
     case NSR_ERR_INTERNAL: return "nsrno_b200: solver queue did not drain";
     case NSR_ERR_CAPACITY: return "nsrno_b200: request exceeds the fixed capacity";
+    case NSR_ERR_TIMEOUT: return "nsrno_b200: a kernel timed out waiting for its shared-memory copies";
     default: break;
   }
   if (code > 0 && code < 1000) return cudaGetErrorString((cudaError_t)code);

@@ -24,6 +24,7 @@
 // nsrno/dense_wave.py:194-196.
 #include "nsr_internal.cuh"
 #include "nsr_device.cuh"
+#include "nsr_tma.cuh"
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -43,6 +44,7 @@ struct __align__(16) SlotState {
   int x0_off;       // the initial field was rejected: start from zero
   int gidx;         // gain pair of the learned preconditioner
   int pad_b2;
+  unsigned long long t_start;   // global timer (ns) when the system started
   double bnorm2, rnorm2, resid, r0norm2;
   double freq, angle;
   double2 rho, alpha, omega, beta;
@@ -56,6 +58,7 @@ struct SolveBufs {
   int* queue;         // next system to start
   int* done;          // systems finished
   int* warm;          // [2]: initial fields accepted, rejected
+  int* error;         // set by a kernel that gave up waiting on its copy ring
   double* partials;   // [n_slots][nb_inv][NSR_NPART]
   float2 *r, *rh, *p, *v, *t, *y, *w;   // [n_slots][n]
   float2* sym;        // [n_slots][n] learned multiplier of the slot's system (learned solves only)
@@ -85,6 +88,7 @@ struct SolveArgs {
   int max_it;
   int replace_every;
   int adjoint;
+  unsigned long long time_limit_ns;   // per-system wall-clock limit (0: none)
   double2* iq;
   double* residual;
   int* iterations;
@@ -317,6 +321,7 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
     if (used_x0) atomicAdd(&A.B.warm[0], 1);
     if (!isfinite(rel2)) { finish_system(A, S, NSR_NONFINITE, rel2); return; }
     if (rel2 < tol2) { finish_system(A, S, NSR_CONVERGED, sqrt(rel2)); return; }
+    S.t_start = global_ns();
     S.rho = make_double2(S.rnorm2, 0.0);
     S.r0norm2 = S.rnorm2;
     S.restart = 0;
@@ -390,6 +395,8 @@ __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const doubl
       S.force_restart = 1;
       S.breakdowns += 1;
     }
+    if (A.time_limit_ns && S.final_reason < 0 && global_ns() - S.t_start > A.time_limit_ns)
+      S.final_reason = NSR_TIMEOUT;   // stops after the FP64 true residual of the current iterate
     if (S.force_restart || S.final_reason >= 0 || S.rnorm2 < tol2 * S.bnorm2 || S.iters >= A.max_it ||
         (A.replace_every > 0 && S.iters % A.replace_every == 0)) {
       if (S.iters >= A.max_it && S.final_reason < 0) S.final_reason = NSR_ITERATION_BUDGET;
@@ -585,6 +592,260 @@ __global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
 }
 
 // ---------------------------------------------------------------------------
+// stn: the stencil of k_inv on rows staged through shared memory by bulk
+// (TMA) copies, for widths that are a multiple of 4.
+//
+// A persistent CTA walks work items (slot, band of tz rows, strip of W
+// columns).  One producer thread streams the rows of its items into a ring of
+// D row buffers with cp.async.bulk, completing on a `full` mbarrier per ring
+// entry; W/2 consumer threads (two columns each) compute row i from the
+// buffers of rows i-1, i, i+1 and release the buffer of row i-1 on an `empty`
+// mbarrier.  Every row buffer holds z (with two halo columns each side) and
+// a (four each side), and for the band's own rows b, t, rhat and, in the
+// second half, r and v: a row step moves about 22 B per column, and D-3 row
+// steps are in flight per CTA while the consumers compute.  Nothing but the
+// copies themselves touches HBM on the read side, so the loads overlap the
+// stencil and FP64 dot products completely.
+// ---------------------------------------------------------------------------
+template <int W>
+struct StnLayout {
+  static constexpr int OZ = 0;                    // float2 z[W + 4], column c0 - 2 + e
+  static constexpr int ORH = OZ + (W + 4) * 8;    // float2 rhat[W]
+  static constexpr int OR = ORH + W * 8;          // float2 r[W]
+  static constexpr int OV = OR + W * 8;           // float2 v[W]
+  static constexpr int OA = OV + W * 8;           // float a[W + 8], column c0 - 4 + e
+  static constexpr int OB = OA + (W + 8) * 4;     // float b[W]
+  static constexpr int OT = OB + W * 4;           // float t[W]
+  static constexpr int SLOT = OT + W * 4;
+  static_assert(ORH % 16 == 0 && OA % 16 == 0 && OB % 16 == 0 && OT % 16 == 0 && SLOT % 16 == 0, "alignment");
+};
+
+#define NSR_STN_WAIT_NS 2000000000ull   // a ring wait longer than 2 s is an error
+
+// Items of one launch and their decoding.
+struct StnItems {
+  int tz, nbands, nstrips, per_slot, n_items;
+};
+
+template <int W>
+__host__ __device__ inline StnItems stn_items(int nz, int nx, int tz, int ns) {
+  StnItems it;
+  it.tz = tz;
+  it.nbands = (nz + tz - 1) / tz;
+  it.nstrips = (nx + W - 1) / W;
+  it.per_slot = it.nbands * it.nstrips;
+  it.n_items = ns * it.per_slot;
+  return it;
+}
+
+template <int W, int D, bool ADJ>
+__global__ void __launch_bounds__(W / 2 + 32, W == 512 ? 2 : 3) k_stn(SolveArgs A, int half, StnItems it, int ns) {
+  typedef StnLayout<W> Ly;
+  constexpr int NC = W / 2;   // consumer threads
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ __align__(8) uint64_t full[D], empty[D];
+  __shared__ int abort_word;
+  volatile int& abort_flag = abort_word;
+  __shared__ double wsum[NC / 32][NSR_NPART];
+  __shared__ double tot[NSR_NPART];
+  __shared__ int am_last;
+  const Geo& g = A.g;
+  const int nz = g.nz, nx = g.nx;
+  const long long n = (long long)nz * nx;
+  const int want = half == 0 ? MODE_ITER_A : MODE_ITER_B;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < D; ++k) {
+      mbar_init(&full[k], 1);
+      mbar_init(&empty[k], NC / 32);
+    }
+    abort_word = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  if (threadIdx.x >= NC) {
+    // ---------------- producer ----------------
+    if (threadIdx.x != NC) return;
+    uint32_t q = 0;   // row step counter (ring entry q % D, phase q / D)
+    for (int item = blockIdx.x; item < it.n_items && !abort_flag; item += gridDim.x) {
+      const int sl = item / it.per_slot, rem = item - sl * it.per_slot;
+      const int band = rem / it.nstrips, strip = rem - band * it.nstrips;
+      const int slot = A.slot0 + sl;
+      if (A.B.slots[slot].mode != want) continue;
+      const int z0 = band * it.tz, z1 = min(z0 + it.tz, nz);
+      const int c0 = strip * W;
+      const long long soff = slot * n;
+      const float2* zsrc = A.B.w + soff;
+      const float2* rhsrc = A.B.rh + soff;
+      const float2* rsrc = A.B.r + soff;
+      const float2* vsrc = A.B.v + soff;
+      const int zlo = max(c0 - 2, 0), zhi = min(c0 + W + 2, nx);
+      const int alo = max(c0 - 4, 0), ahi = min(c0 + W + 4, nx);
+      const int phi = min(c0 + W, nx);
+      for (int row = z0 - 1; row <= z1; ++row, ++q) {
+        const int e = q % D;
+        if (q >= D && !mbar_wait(&empty[e], ((q / D) & 1) ^ 1, &abort_word, NSR_STN_WAIT_NS)) {
+          abort_flag = 1;
+          break;
+        }
+        unsigned char* buf = ring + (size_t)e * Ly::SLOT;
+        const bool in = row >= 0 && row < nz;
+        const bool own = row >= z0 && row < z1;
+        uint32_t bytes = 0;
+        if (in) bytes += (zhi - zlo) * 8 + (ahi - alo) * 4;
+        if (own) bytes += (phi - c0) * (8 + 4 + 4) + (half ? 2 * (phi - c0) * 8 : 0);
+        mbar_arrive_expect_tx(&full[e], bytes);
+        if (in) {
+          const long long ro = (long long)row * nx;
+          bulk_load(buf + Ly::OZ + (zlo - (c0 - 2)) * 8, zsrc + ro + zlo, (zhi - zlo) * 8, &full[e]);
+          bulk_load(buf + Ly::OA + (alo - (c0 - 4)) * 4, A.mat.a32 + ro + alo, (ahi - alo) * 4, &full[e]);
+          if (own) {
+            const uint32_t fb = (phi - c0) * 4, cb = (phi - c0) * 8;
+            bulk_load(buf + Ly::OB, A.mat.b32 + ro + c0, fb, &full[e]);
+            bulk_load(buf + Ly::OT, A.mat.t32 + ro + c0, fb, &full[e]);
+            bulk_load(buf + Ly::ORH, rhsrc + ro + c0, cb, &full[e]);
+            if (half) {
+              bulk_load(buf + Ly::OR, rsrc + ro + c0, cb, &full[e]);
+              bulk_load(buf + Ly::OV, vsrc + ro + c0, cb, &full[e]);
+            }
+          }
+        }
+      }
+    }
+    if (abort_flag) {
+      atomicExch(A.B.error, 1);
+      // Let the copies already issued land before the block's shared memory goes away.
+      for (uint32_t k = (q > (uint32_t)D ? q - D : 0); k < q; ++k)
+        mbar_wait(&full[k % D], (k / D) & 1, nullptr, NSR_STN_WAIT_NS);
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  uint32_t q = 0;
+  for (int item = blockIdx.x; item < it.n_items; item += gridDim.x) {
+    const int sl = item / it.per_slot, rem = item - sl * it.per_slot;
+    const int band = rem / it.nstrips, strip = rem - band * it.nstrips;
+    const int slot = A.slot0 + sl;
+    SlotState& S = A.B.slots[slot];
+    if (S.mode != want) continue;
+    const int z0 = band * it.tz, z1 = min(z0 + it.tz, nz);
+    const int nrows = z1 - z0;
+    const int c0 = strip * W;
+    const int j = c0 + 2 * tid;
+    const bool own = j < nx;
+    const bool has_w = j > 0, has_e = j + 2 < nx;
+    const long long soff = slot * n;
+    float2* __restrict__ out = (half == 0 ? A.B.v : A.B.t) + soff;
+    const SysScalars sc = sys_scalars(g, S.freq);
+    const float2 sv = f2(S.c_sv);
+    double acc[NSR_NPART];
+#pragma unroll
+    for (int k = 0; k < NSR_NPART; ++k) acc[k] = 0.0;
+    const uint32_t q0 = q;   // step of row z0 - 1
+    bool ok = !abort_flag;
+    // rows z0 - 1 and z0
+    for (uint32_t s = q0; s < q0 + 2 && ok; ++s) ok = mbar_wait(&full[s % D], (s / D) & 1, &abort_word, NSR_STN_WAIT_NS);
+    for (int k = 0; k < nrows; ++k) {
+      const int i = z0 + k;
+      const uint32_t sN = q0 + k, sC = sN + 1, sS = sN + 2;
+      if (ok) ok = mbar_wait(&full[sS % D], (sS / D) & 1, &abort_word, NSR_STN_WAIT_NS);
+      if (!ok) abort_flag = 1;
+      if (ok && own) {
+        const unsigned char* bN = ring + (size_t)(sN % D) * Ly::SLOT;
+        const unsigned char* bC = ring + (size_t)(sC % D) * Ly::SLOT;
+        const unsigned char* bS = ring + (size_t)(sS % D) * Ly::SLOT;
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float2 zero = make_float2(0.f, 0.f);
+        const int ez = (2 * tid + 2) * 8, ea = (2 * tid + 4) * 4;
+        const float4 zc = *reinterpret_cast<const float4*>(bC + Ly::OZ + ez);
+        const float4 zn = i > 0 ? *reinterpret_cast<const float4*>(bN + Ly::OZ + ez) : zero4;
+        const float4 zs = i + 1 < nz ? *reinterpret_cast<const float4*>(bS + Ly::OZ + ez) : zero4;
+        const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
+        const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 16) : zero;
+        const float2 ac = *reinterpret_cast<const float2*>(bC + Ly::OA + ea);
+        const float2 an = i > 0 ? *reinterpret_cast<const float2*>(bN + Ly::OA + ea) : make_float2(1.f, 1.f);
+        const float2 as = i + 1 < nz ? *reinterpret_cast<const float2*>(bS + Ly::OA + ea) : make_float2(1.f, 1.f);
+        const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
+        const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 8) : 1.0f;
+        const float2 bb = *reinterpret_cast<const float2*>(bC + Ly::OB + 8 * tid);
+        const float2 tt = *reinterpret_cast<const float2*>(bC + Ly::OT + 8 * tid);
+        const float4 rk = *reinterpret_cast<const float4*>(bC + Ly::ORH + 16 * tid);
+        const float2 c0v = lo2(zc), c1v = hi2(zc);
+        const float2 av0 = stencil_pts<ADJ>(g, sc, i, j, ac.x, ac.y, aw, as.x, an.x, bb.x, tt.x, c0v, c1v, zw,
+                                            lo2(zs), lo2(zn));
+        const float2 av1 = stencil_pts<ADJ>(g, sc, i, j + 1, ac.y, ae, ac.x, as.y, an.y, bb.y, tt.y, c1v, ze, c0v,
+                                            hi2(zs), hi2(zn));
+        *reinterpret_cast<float4*>(out + (long long)i * nx + j) = pack2(av0, av1);
+        if (half == 0) {
+          dot_acc(acc[0], acc[1], lo2(rk), av0);       // <rhat, v>
+          dot_acc(acc[0], acc[1], hi2(rk), av1);
+        } else {
+          const float4 rr = *reinterpret_cast<const float4*>(bC + Ly::OR + 16 * tid);
+          const float4 vv = *reinterpret_cast<const float4*>(bC + Ly::OV + 16 * tid);
+          const float2 s0 = lo2(rr) + sv * lo2(vv), s1 = hi2(rr) + sv * hi2(vv);
+          dot_acc(acc[0], acc[1], av0, s0);            // <t, s>
+          dot_acc(acc[0], acc[1], av1, s1);
+          acc[2] += (double)av0.x * av0.x + (double)av0.y * av0.y + (double)av1.x * av1.x + (double)av1.y * av1.y;
+          acc[3] += (double)s0.x * s0.x + (double)s0.y * s0.y + (double)s1.x * s1.x + (double)s1.y * s1.y;
+          dot_acc(acc[4], acc[5], lo2(rk), av0);       // <rhat, t>
+          dot_acc(acc[4], acc[5], hi2(rk), av1);
+          dot_acc(acc[6], acc[7], lo2(rk), s0);        // <rhat, s>
+          dot_acc(acc[6], acc[7], hi2(rk), s1);
+        }
+      }
+      // the buffer of row i - 1 is no longer needed
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[sN % D]);
+    }
+    // rows z1 - 1 and z1
+    __syncwarp();
+    if (lane == 0) {
+      mbar_arrive(&empty[(q0 + nrows) % D]);
+      mbar_arrive(&empty[(q0 + nrows + 1) % D]);
+    }
+    q = q0 + nrows + 2;
+
+    // Block sum of the partials (consumer threads only), then the arrival.
+#pragma unroll
+    for (int k = 0; k < NSR_NPART; ++k) {
+      const double s = warp_sum(acc[k]);
+      if (lane == 0) wsum[wid][k] = s;
+    }
+    named_sync(1, NC);
+    double* part = A.B.partials + (long long)slot * A.nb_inv * NSR_NPART;
+    if (tid == 0) {
+      for (int k = 0; k < NSR_NPART; ++k) {
+        double s = 0.0;
+        for (int w2 = 0; w2 < NC / 32; ++w2) s += wsum[w2][k];
+        part[rem * NSR_NPART + k] = s;
+      }
+      __threadfence();
+      const int prev = atomicAdd(&A.B.arrive[slot], 1);
+      am_last = (prev == it.per_slot - 1);
+    }
+    named_sync(1, NC);
+    if (am_last) {
+      __threadfence();
+      if (tid < NSR_NPART) {
+        double sacc = 0.0;
+        for (int b = 0; b < it.per_slot; ++b) sacc += __ldcg(&part[b * NSR_NPART + tid]);
+        tot[tid] = sacc;
+      }
+      named_sync(1, NC);
+      if (tid == 0) {
+        A.B.arrive[slot] = 0;
+        finalize(A, S, want, tot);
+        __threadfence();
+      }
+    }
+    named_sync(1, NC);   // wsum, tot and am_last are reused by the next item
+  }
+  if (tid == 0 && abort_flag) atomicExch(A.B.error, 1);
+}
+
+// ---------------------------------------------------------------------------
 // inv: stencil on z = M^-1 (input) + inner products of the Krylov halves.
 // k_inv1 (grids of odd width, whose rows are not 16-byte aligned): one thread
 // per column of a NSR_ST_TZ x NSR_ST_TX1 tile walks down its rows
@@ -762,6 +1023,7 @@ __global__ void k_solve_init(SolveArgs A, int n_slots) {
     *A.B.done = 0;
     A.B.warm[0] = 0;
     A.B.warm[1] = 0;
+    *A.B.error = 0;
   }
 }
 
@@ -773,6 +1035,59 @@ __global__ void k_solve_init(SolveArgs A, int n_slots) {
 static int stencil_ctas(const NsrGrid* g) {
   const int tx = (g->nx % 2 == 0) ? NSR_ST_TX : NSR_ST_TX1;
   return ((g->nz + NSR_ST_TZ - 1) / NSR_ST_TZ) * ((g->nx + tx - 1) / tx);
+}
+
+// Ring-staged stencil (k_stn): widths that are a multiple of 4 keep every
+// bulk copy 16-byte aligned.
+static bool stn_ok(const NsrGrid* g) { return g->nx % 4 == 0 && g->nx >= 8; }
+#define NSR_STN_MIN_ROWS 4
+
+// Stencil partials per slot of the finest allowed k_stn decomposition.
+static int stn_items_max(const NsrGrid* g) {
+  return ((g->nz + NSR_STN_MIN_ROWS - 1) / NSR_STN_MIN_ROWS) * ((g->nx + 255) / 256);
+}
+
+typedef void (*StnKernel)(SolveArgs, int, StnItems, int);
+
+static StnKernel stn_kernel(int w, int d, bool adj) {
+#define NSR_STN_CASE(W_, D_) \
+  if (w == W_ && d == D_) return adj ? k_stn<W_, D_, true> : k_stn<W_, D_, false>;
+  NSR_STN_CASE(256, 4) NSR_STN_CASE(256, 6) NSR_STN_CASE(256, 8) NSR_STN_CASE(512, 4) NSR_STN_CASE(512, 5)
+#undef NSR_STN_CASE
+  return nullptr;
+}
+
+static size_t stn_smem(int w, int d) {
+  return (size_t)d * (w == 512 ? StnLayout<512>::SLOT : StnLayout<256>::SLOT);
+}
+
+// Launch shapes of one call: NsrTiles with zero fields replaced by defaults.
+struct TileChoice {
+  int sw, sd, sr, sctas, tc, rows, groups;
+};
+
+static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileChoice* c) {
+  c->sw = 256; c->sd = 6; c->sr = 16; c->sctas = 0;
+  c->tc = nsr_cols_tc(g);
+  c->rows = nsr_rows_per_cta(g);
+  c->groups = n_slots >= 8 ? 2 : 1;
+  if (t) {
+    if (t->stencil_width) c->sw = t->stencil_width;
+    if (t->stencil_depth) c->sd = t->stencil_depth;
+    if (t->stencil_rows) c->sr = t->stencil_rows;
+    if (t->stencil_ctas) c->sctas = t->stencil_ctas;
+    if (t->cols_width) c->tc = t->cols_width;
+    if (t->row_tile) c->rows = t->row_tile;
+    if (t->slot_groups) c->groups = t->slot_groups;
+  }
+  if (!stn_kernel(c->sw, c->sd, false)) return NSR_ERR_ARGUMENT;
+  if (c->sr < NSR_STN_MIN_ROWS || c->sr > 64 || c->sctas < 0 || c->sctas > 8) return NSR_ERR_ARGUMENT;
+  if (!(c->tc == 8 || c->tc == 16) || (size_t)g->nz * c->tc * sizeof(float2) > 200 * 1024) return NSR_ERR_ARGUMENT;
+  if (c->rows < 1 || c->rows > 8 || sizeof(float2) * (size_t)c->rows * nsr_row_stride(g->nx) > 200 * 1024)
+    return NSR_ERR_ARGUMENT;
+  if (c->groups < 1 || c->groups > 2) return NSR_ERR_ARGUMENT;
+  if (n_slots < 2) c->groups = 1;
+  return 0;
 }
 
 static int band_rows(const NsrGrid* g) {
@@ -793,13 +1108,14 @@ static Layout layout(const NsrGrid* g, int n_slots) {
   const size_t n = (size_t)g->nz * g->nx;
   const int tz = band_rows(g);
   const int nb_res = (g->nz + tz - 1) / tz;
-  const int nb_st = stencil_ctas(g);
+  int nb_st = stencil_ctas(g);
+  if (stn_ok(g) && stn_items_max(g) > nb_st) nb_st = stn_items_max(g);
   L.nb_inv = nb_res > nb_st ? nb_res : nb_st;
   size_t off = 0;
   L.tables = off; off += nsr_align(nsr_prec_table_bytes(g));
   L.slots = off; off += nsr_align(sizeof(SlotState) * n_slots);
   L.arrive = off; off += nsr_align(sizeof(int) * n_slots);
-  L.queue = off; off += nsr_align(sizeof(int) * 4);
+  L.queue = off; off += nsr_align(sizeof(int) * 8);
   L.partials = off; off += nsr_align(sizeof(double) * NSR_NPART * (size_t)L.nb_inv * n_slots);
   L.vec = off; off += 8 * nsr_align(sizeof(float2) * n * n_slots);
   L.x = off; off += nsr_align(sizeof(double2) * n * 2 * n_slots);
@@ -817,7 +1133,7 @@ extern "C" size_t nsr_solve_workspace_size(const NsrGrid* grid, int32_t n_slots)
 static int* pinned_counter() {
   static thread_local int* p = nullptr;
   if (!p) {
-    if (cudaHostAlloc((void**)&p, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) p = nullptr;
+    if (cudaHostAlloc((void**)&p, 8 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) p = nullptr;
   }
   return p;
 }
@@ -843,7 +1159,10 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
       !(params->shift >= 0) || params->replace_every < 0 || !(params->restart_factor >= 0) ||
       params->restart_factor >= 1.0) return NSR_ERR_ARGUMENT;
   if (params->learned && !params->learned->params) return NSR_ERR_ARGUMENT;
-  if (n_systems == 0) return 0;
+  if (!(params->time_limit_s >= 0.0)) return NSR_ERR_ARGUMENT;
+  TileChoice T;
+  err = resolve_tiles(grid, params->tiles, n_slots, &T);
+  if (err) return err;
   const Layout L = layout(grid, n_slots);
   if (workspace_bytes < L.total) return NSR_ERR_WORKSPACE;
   const size_t n = (size_t)grid->nz * grid->nx;
@@ -889,6 +1208,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     A.B.queue = (int*)(ws + L.queue);
     A.B.done = A.B.queue + 1;
     A.B.warm = A.B.queue + 2;
+    A.B.error = A.B.queue + 4;
     A.B.partials = (double*)(ws + L.partials);
     const size_t vb = nsr_align(sizeof(float2) * n * n_slots);
     float2** vecs[8] = {&A.B.r, &A.B.rh, &A.B.p, &A.B.v, &A.B.t, &A.B.y, &A.B.w, &A.B.sym};
@@ -902,8 +1222,8 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     A.rx = rx_index;
     A.n_rx = n_rx;
     A.n_systems = n_systems;
-    A.rows = nsr_rows_per_cta(grid);
-    A.tc = nsr_cols_tc(grid);
+    A.rows = T.rows;
+    A.tc = T.tc;
     A.tz = band_rows(grid);
     A.nb_inv = L.nb_inv;
     A.tol2 = params->tolerance * params->tolerance;
@@ -913,6 +1233,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     A.max_it = params->max_iterations;
     A.replace_every = params->replace_every;
     A.adjoint = params->adjoint;
+    A.time_limit_ns = params->time_limit_s > 0.0 ? (unsigned long long)(params->time_limit_s * 1e9) : 0ull;
     A.iq = (double2*)iq;
     A.residual = residual;
     A.iterations = iterations;
@@ -930,6 +1251,24 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     const int nb_res = (grid->nz + A.tz - 1) / A.tz;
     const int nb_st = stencil_ctas(grid);
     const bool pairs = grid->nx % 2 == 0;
+    const bool use_stn = stn_ok(grid);
+    const StnKernel stn_fn = stn_kernel(T.sw, T.sd, A.adjoint != 0);
+    const size_t stn_sm = stn_smem(T.sw, T.sd);
+    int stn_per_sm = T.sctas;
+    int n_sms = 1;
+    {
+      int dev = 0;
+      NSR_TRY(cudaGetDevice(&dev));
+      NSR_TRY(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    if (use_stn) {
+      NSR_TRY(cudaFuncSetAttribute((const void*)stn_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stn_sm));
+      if (stn_per_sm <= 0) {
+        NSR_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&stn_per_sm, (const void*)stn_fn, T.sw / 2 + 32,
+                                                              stn_sm));
+        if (stn_per_sm < 1) { err = NSR_ERR_ARGUMENT; goto cleanup; }
+      }
+    }
     NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(k_cols<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
@@ -943,7 +1282,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
 
     // The slots run as two independent groups on two branches of the captured
     // graph, so that one group's kernels fill the tail waves of the other's.
-    const int n_groups = n_slots >= 8 ? 2 : 1;
+    const int n_groups = T.groups;
     int g_first[2] = {0, 0}, g_count[2] = {n_slots, 0};
     if (n_groups == 2) {
       g_count[0] = (n_slots + 1) / 2;
@@ -977,6 +1316,17 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
       } else if (which == 2) {
         if (A.adjoint) k_res<true><<<g_res, 256, 0, sq>>>(Ag);
         else k_res<false><<<g_res, 256, 0, sq>>>(Ag);
+      } else if (which == 3 && use_stn) {
+        StnItems si;
+        si.tz = T.sr;
+        si.nbands = (grid->nz + T.sr - 1) / T.sr;
+        si.nstrips = (grid->nx + T.sw - 1) / T.sw;
+        si.per_slot = si.nbands * si.nstrips;
+        si.n_items = ns * si.per_slot;
+        int hv = half, nsv = ns;
+        const int gx = si.n_items < stn_per_sm * n_sms ? si.n_items : stn_per_sm * n_sms;
+        void* args[] = {&Ag, &hv, &si, &nsv};
+        cudaLaunchKernel((const void*)stn_fn, dim3(gx), dim3(T.sw / 2 + 32), args, stn_sm, sq);
       } else if (which == 3) {
         if (pairs) {
           if (A.adjoint) k_inv<true><<<g_inv, 256, 0, sq>>>(Ag, half);
@@ -1045,29 +1395,33 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     const long long waves = (n_systems + n_slots - 1) / n_slots + 1;
     const long long max_launch = waves * ((per_sys + K - 1) / K) + 4;
     long long launched = 0;
-    bool drained = false;
+    bool drained = false, failed = false;
     int pending = -1;
     while (launched < max_launch) {
       NSR_TRY(cudaGraphLaunch(exec, st));
       ++graph_launches;
       launches += (long long)NSR_LAUNCHES_PER_IT * K * n_groups;
       const int slot_i = (int)(launched & 1);
-      NSR_TRY(cudaMemcpyAsync(&host[slot_i], A.B.done, sizeof(int), cudaMemcpyDeviceToHost, st));
+      // done, warm[2], error
+      NSR_TRY(cudaMemcpyAsync(&host[4 * slot_i], A.B.done, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
       NSR_TRY(cudaEventRecord(ev_poll[slot_i], st));
       ++launched;
       if (pending >= 0) {
         NSR_TRY(cudaEventSynchronize(ev_poll[pending]));
-        if (host[pending] >= n_systems) { drained = true; break; }
+        if (host[4 * pending + 3]) { failed = true; break; }
+        if (host[4 * pending] >= n_systems) { drained = true; break; }
       }
       pending = slot_i;
     }
-    if (!drained && pending >= 0) {
+    if (!drained && !failed && pending >= 0) {
       NSR_TRY(cudaEventSynchronize(ev_poll[pending]));
-      drained = host[pending] >= n_systems;
+      failed = host[4 * pending + 3] != 0;
+      drained = host[4 * pending] >= n_systems;
     }
     NSR_TRY(cudaEventRecord(ev_loop[1], st));
     NSR_TRY(cudaStreamSynchronize(st));
-    if (!drained) err = NSR_ERR_INTERNAL;
+    if (failed) err = NSR_ERR_TIMEOUT;
+    else if (!drained) err = NSR_ERR_INTERNAL;
     if (stats) {
       int warm_host[2] = {0, 0};
       NSR_TRY(cudaMemcpyAsync(warm_host, A.B.warm, sizeof(warm_host), cudaMemcpyDeviceToHost, st));

@@ -147,7 +147,7 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                   max_iterations=2000, shift=DEFAULT_SHIFT, replace_every=DEFAULT_REPLACE, n_slots=16,
                   adjoint=False, return_fields=False, rx_index=None, graph_iterations=16,
                   profile_iterations=0, restart_factor=DEFAULT_RESTART, warm_gate=1.0, fields_dtype=torch.complex64,
-                  learned=None, gain_index=None,
+                  learned=None, gain_index=None, time_limit=0.0, tiles=None,
                   workspace: Workspace | None = None, out: BatchResult | None = None) -> BatchResult:
     """Solve every (frequency, angle) system of a record with batched BiCGSTAB.
 
@@ -156,7 +156,11 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
     ``x0`` (complex64 [S, nz, nx]) is a warm start.  ``learned`` (a
     :class:`nsrno_b200.learned.LearnedSetup`) replaces the fixed preconditioner
     by the learned one; ``gain_index`` (int [S]) picks each system's gain pair
-    (default: its position in ``learned.freqs``).
+    (default: its position in ``learned.freqs``).  ``time_limit`` (seconds,
+    0: none) bounds each system's solve on the device: a system still running
+    then stops at its next true residual with reason ``"timeout"``.
+    ``tiles`` (a dict of :class:`nsrno_b200._lib.NsrTiles` fields, e.g. from
+    :func:`nsrno_b200.tune.tuned_tiles`) overrides the launch shapes.
     """
     lib = _lib.load()
     g = medium.geometry
@@ -205,16 +209,37 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                                  int(n_slots), int(bool(adjoint)), int(graph_iterations), int(profile_iterations),
                                  int(fields_dtype == torch.complex128), 0)
     keep = _learned_params(params, learned, gain_index, freqs)
+    if not time_limit >= 0.0:
+        raise ValueError("time_limit must be >= 0")
+    params.time_limit_s = float(time_limit)
+    tiles_struct = _tiles_struct(tiles)
+    if tiles_struct is not None:
+        params.tiles = ctypes.pointer(tiles_struct)
     stats = _lib.NsrSolveStats()
     _lib.check(lib.nsr_solve_batched(
         ctypes.byref(grid), _ptr(medium.material), _ptr(freqs), _ptr(angles), S,
         _ptr(rhs), _ptr(x0), _ptr(rx_index), n_rx, ctypes.byref(params),
         _ptr(ws), ws.numel(), _ptr(out.iq), _ptr(out.residual), _ptr(out.iterations), _ptr(out.status),
         _ptr(out.fields), ctypes.byref(stats), _stream()))
-    del keep
+    del keep, tiles_struct
     out.extra["stats"] = stats.as_dict()
     out.extra["n_slots"] = n_slots
     return out
+
+
+def _tiles_struct(tiles):
+    """NsrTiles from a dict of its fields (None: built-in launch shapes)."""
+    if tiles is None:
+        return None
+    if isinstance(tiles, _lib.NsrTiles):
+        return tiles
+    unknown = set(tiles) - set(_lib.NsrTiles.FIELDS)
+    if unknown:
+        raise ValueError(f"unknown tile fields {sorted(unknown)}")
+    t = _lib.NsrTiles()
+    for k, v in tiles.items():
+        setattr(t, k, int(v))
+    return t
 
 
 def _learned_params(params, learned, gain_index, freqs):

@@ -90,3 +90,32 @@ def test_header_is_plain_c(tmp_path):
                    ' (void)p; (void)l; (void)g; return 0; }\n')
     subprocess.run([cc, "-std=c99", "-Wall", "-Werror", f"-I{ROOT / 'include'}", "-fsyntax-only", str(src)],
                    check=True)
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """The ctypes mirrors have the C layout: size and every field offset."""
+    import shutil
+    import subprocess
+    from nsrno_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"NsrGrid": _lib.NsrGrid, "NsrLearned": _lib.NsrLearned, "NsrTiles": _lib.NsrTiles,
+               "NsrSolveParams": _lib.NsrSolveParams, "NsrGmresParams": _lib.NsrGmresParams,
+               "NsrSolveStats": _lib.NsrSolveStats, "NsrDenseGrid": _lib.NsrDenseGrid}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "nsrno_b200.h"', 'int main(void) {']
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{name} {field} %zu\\n", offsetof({name}, {field}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    for line in filter(None, out):
+        name, field, value = line.split()
+        cls = structs[name]
+        got = ctypes.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        assert got == int(value), (name, field, got, value)

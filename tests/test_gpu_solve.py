@@ -235,3 +235,60 @@ def test_largest_grid_converges(cuda):
     tr = true_residual(med, res.fields, f[:2], th[:2]).cpu().numpy()
     assert (tr < 1e-6).all()
     assert np.allclose(tr, res.residual.cpu().numpy(), rtol=1e-6)
+
+
+def test_even_width_not_multiple_of_four_matches_lu(cuda):
+    """96 x 54 (even, not a multiple of 4: the two-column register stencil
+    instead of the ring-staged one) against SuperLU."""
+    from nsrno_b200 import Geometry, Medium, solve_batched
+    from nsrno_b200.media import blob_record
+    rec = blob_record(nz=96, nx=54, h=1e-4, n_pml=8, n_blobs=2, frequencies=(1.2e6,), n_rx=16, rx_pitch=2)
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=cuda)
+    f, th = rec.systems()
+    spec = spec_of(rec)
+    a, b, t = med.coef64.cpu().numpy()
+    res = solve_batched(med, f, th, tolerance=1e-9, max_iterations=3000, return_fields=True)
+    assert res.reasons() == ["converged"] * len(f)
+    A = H.operator_planes(spec, a, b, t, f[0])
+    for s in range(len(f)):
+        ref = H.solve_lu(A, H.plane_wave_rhs(spec, f[s], th[s]))
+        assert rel(res.fields[s].cpu().numpy().ravel(), ref) < 1e-5
+
+
+def test_time_limit_reports_timeout(cuda):
+    """A per-system time limit that runs out ends the system with reason
+    'timeout' and the FP64 true residual of the iterate it reached; systems
+    that converge first are unaffected."""
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    r = solve_batched(med, f[:2], th[:2], tolerance=1e-12, max_iterations=4000, time_limit=1e-6)
+    assert r.reasons() == ["timeout"] * 2
+    res = r.residual.cpu().numpy()
+    assert np.all(np.isfinite(res)) and np.all(res < 1.0)
+    assert (r.iterations.cpu() < 40).all()
+    ok = solve_batched(med, f[:2], th[:2], tolerance=1e-6, time_limit=60.0)
+    assert ok.reasons() == ["converged"] * 2
+
+
+@pytest.mark.parametrize("tiles", [
+    dict(cols_width=8, row_tile=2, slot_groups=1),
+    dict(stencil_width=512, stencil_depth=4, stencil_rows=8),
+    dict(stencil_width=512, stencil_depth=5, stencil_rows=32, stencil_ctas=1),
+    dict(stencil_width=256, stencil_depth=8, stencil_rows=4, slot_groups=1),
+])
+def test_launch_shapes_agree(cuda, tiles):
+    """Every launch shape the autotuner may pick solves the same systems.  Shapes
+    of the transforms and of the slot groups leave each slot's arithmetic as it
+    is (bitwise equal); stencil shapes regroup the FP64 partial sums of the
+    inner products, so those agree to the solve tolerance."""
+    from nsrno_b200 import solve_batched
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    base = solve_batched(med, f, th, tolerance=1e-7, n_slots=6, max_iterations=3000)
+    got = solve_batched(med, f, th, tolerance=1e-7, n_slots=6, max_iterations=3000, tiles=tiles)
+    assert got.reasons() == ["converged"] * len(f)
+    if not any(k.startswith("stencil") for k in tiles):
+        assert torch.equal(got.iq, base.iq) and torch.equal(got.iterations, base.iterations)
+    else:
+        assert rel(got.iq.cpu().numpy(), base.iq.cpu().numpy()) < 1e-5
