@@ -326,6 +326,44 @@ int nsr_dense_precondition(const NsrDenseGrid* grid, double k0dx2, double shift,
                            int32_t adjoint, const float* x, float* y, void* workspace, size_t workspace_bytes,
                            void* stream);
 
+/* Converged dense-path solve A x = b (adjoint 0) or A^H x = b (adjoint 1) of
+ * n_fields fields sharing one coefficient set, all fields treated as one
+ * vector as the reference does: restarted right-preconditioned GMRES(restart)
+ * with two classical Gram-Schmidt passes and the fixed preconditioner of
+ * nsr_dense_precondition; complex64 Krylov vectors, FP64 inner products,
+ * Hessenberg/Givens recurrence and triangular solve on the device, a
+ * complex128 iterate and an FP64 true residual at every restart.  Replaces
+ * the GMRES branch of solve_system (nsrno/dense_wave.py:212-220, gmres of
+ * nsrno/wave_solver.py:9-36) and its mixed FP32 inverse / FP64 residual
+ * refinement (nsrno/dense_wave.py:168-191).  rhs and x: c128
+ * [n_fields][H][W] (x holds the initial field on entry, the solution on
+ * return); field_residual: NULL or device double [n_fields], the final
+ * relative residual of every field.  Synchronises its stream once per
+ * restart cycle. */
+typedef struct NsrDenseSolveParams {
+  double tolerance;          /* FP64 relative residual over all fields         */
+  double shift;              /* preconditioner shift (0.15)                    */
+  double k0dx2;              /* (k0 dx)^2 of the preconditioner                */
+  double scal_re, scal_im;   /* (D-1)/(D k0^2), as nsr_dense_apply             */
+  int32_t restart;           /* Arnoldi steps per cycle (1..64; 24 or 32)      */
+  int32_t max_cycles;        /* restart cycles                                 */
+  int32_t adjoint;           /* 0: A x = b; 1: A^H x = b                       */
+  int32_t reserved;
+} NsrDenseSolveParams;
+
+typedef struct NsrDenseSolveInfo {
+  int32_t status;            /* NSR_CONVERGED, NSR_ITERATION_BUDGET, NSR_NONFINITE */
+  int32_t steps;             /* Arnoldi steps (operator applications)          */
+  int32_t cycles;            /* restart cycles                                 */
+  int32_t reserved;
+  double residual;           /* FP64 relative residual of the returned x        */
+} NsrDenseSolveInfo;
+
+size_t nsr_dense_solve_workspace_size(const NsrDenseGrid* grid, int32_t n_fields, int32_t restart);
+int nsr_dense_solve(const NsrDenseGrid* grid, const double* coef, const NsrDenseSolveParams* params,
+                    int32_t n_fields, const double* rhs, double* x, double* field_residual,
+                    NsrDenseSolveInfo* info, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Band-limited RF traces rf[ch][t] (double) from receiver spectra
  * spectrum[ch][b] (c128) on positive bins 0 < bins[b] < n_samples/2:
  * the irfft with 'forward' normalisation of predict_band_rf

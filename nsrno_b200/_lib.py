@@ -24,7 +24,8 @@ EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_m
            "nsr_learned_backward_workspace_size", "nsr_learned_map_backward", "nsr_learned_network_backward",
            "nsr_learned_spectral_workspace_size", "nsr_learned_spectral_backward", "nsr_learned_adam",
            "nsr_tangent_rhs", "nsr_dense_precondition_workspace_size", "nsr_dense_precondition", "nsr_band_rf",
-           "nsr_true_residual_workspace_size", "nsr_true_residual")
+           "nsr_true_residual_workspace_size", "nsr_true_residual", "nsr_dense_solve_workspace_size",
+           "nsr_dense_solve")
 
 LEARNED_PARAMS = 3645
 
@@ -75,6 +76,17 @@ class NsrGmresParams(ctypes.Structure):
                 ("n_slots", ctypes.c_int32), ("adjoint", ctypes.c_int32),
                 ("fields_fp64", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("learned", ctypes.POINTER(NsrLearned))]
+
+
+class NsrDenseSolveParams(ctypes.Structure):
+    _fields_ = [("tolerance", ctypes.c_double), ("shift", ctypes.c_double), ("k0dx2", ctypes.c_double),
+                ("scal_re", ctypes.c_double), ("scal_im", ctypes.c_double), ("restart", ctypes.c_int32),
+                ("max_cycles", ctypes.c_int32), ("adjoint", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class NsrDenseSolveInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("steps", ctypes.c_int32), ("cycles", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("residual", ctypes.c_double)]
 
 
 class NsrSolveStats(ctypes.Structure):
@@ -140,6 +152,10 @@ def load():
     lib.nsr_dense_precondition_workspace_size.restype = S
     lib.nsr_dense_precondition_workspace_size.argtypes = [DG, I]
     lib.nsr_dense_precondition.argtypes = [DG, D, D, I, I, P, P, P, S, P]
+    lib.nsr_dense_solve_workspace_size.restype = S
+    lib.nsr_dense_solve_workspace_size.argtypes = [DG, I, I]
+    lib.nsr_dense_solve.argtypes = [DG, P, ctypes.POINTER(NsrDenseSolveParams), I, P, P, P,
+                                    ctypes.POINTER(NsrDenseSolveInfo), P, S, P]
     L = ctypes.POINTER(NsrLearned)
     lib.nsr_learned_state_bytes.restype = S
     lib.nsr_learned_state_bytes.argtypes = [G, I]

@@ -223,69 +223,54 @@ def assemble(system: DenseSystem, reference: DenseSystem, line, pref):
     return system.source(line) - reference.source(line) - system.apply(pref) + reference.apply(pref)
 
 
-def gmres(operator, precondition, rhs, x, callback=None, restart=32, max_cycles=80, tolerance=1e-4):
-    """Restarted right-preconditioned GMRES with two classical Gram-Schmidt passes
-    over the whole field batch as one vector (nsrno/wave_solver.py:9-36): happy
-    breakdown below 1e-12, preconditioned directions kept, the small least
-    squares in complex128 on the host.  Returns ``(x, reason, steps)``."""
-    shape = rhs.shape
-    n = rhs.numel()
-    scale = rhs.norm().clamp_min(1e-30)
-    basis = torch.empty((restart + 1, n), dtype=rhs.dtype, device=rhs.device)
-    directions = torch.empty((restart, n), dtype=rhs.dtype, device=rhs.device)
-    steps = 0
-    for _ in range(max_cycles):
-        residual = rhs - operator(x)
-        beta = residual.norm()
-        relative = float(beta / scale)
-        if callback is not None:
-            callback(steps, x, relative)
-        if relative < tolerance:
-            return x, "converged", steps
-        basis[0] = residual.flatten() / beta
-        h = torch.zeros((restart + 1, restart), dtype=rhs.dtype, device=rhs.device)
-        used = restart
-        for j in range(restart):
-            z = precondition(basis[j].reshape(shape))
-            directions[j] = z.flatten()
-            w = operator(z).flatten()
-            steps += 1
-            for _ in range(2):
-                coefficients = basis[: j + 1].conj() @ w
-                w = w - basis[: j + 1].T @ coefficients
-                h[: j + 1, j] += coefficients
-            h[j + 1, j] = w.norm()
-            if float(h[j + 1, j].abs()) < 1e-12:
-                used = j + 1
-                break
-            basis[j + 1] = w / h[j + 1, j]
-        q = torch.zeros(used + 1, dtype=torch.complex128)
-        q[0] = complex(beta)
-        y = torch.linalg.lstsq(h[: used + 1, :used].cpu().to(torch.complex128), q).solution
-        x = x + (directions[:used].T @ y.to(rhs.device, rhs.dtype)).reshape(shape)
-    final = float((rhs - operator(x)).norm() / scale)
-    if callback is not None:
-        callback(steps, x, final)
-    return x, ("converged" if final < tolerance else "iteration_budget"), steps
-
-
-def solve(system: DenseSystem, rhs, adjoint=False, tolerance=1e-5, restart=32, max_cycles=100, shift=0.15,
+def solve(system: DenseSystem, rhs, adjoint=False, tolerance=1e-5, restart=24, max_cycles=100, shift=0.15,
           initial=None):
-    """Converged dense-path solve of ``A x = rhs`` (or ``A^H x = rhs``) with the
-    fixed preconditioner: the GMRES branch of ``solve_system``
-    (nsrno/dense_wave.py:217-220).  Returns ``(x, info)``."""
+    """Converged dense-path solve of ``A x = rhs`` (or ``A^H x = rhs``): the
+    GMRES branch of ``solve_system`` (nsrno/dense_wave.py:212-225) with the
+    fixed preconditioner, run on the device by ``nsr_dense_solve`` -- all
+    fields (angles) as one vector, complex64 Krylov vectors with FP64 inner
+    products and Givens recurrence, a complex128 iterate and an FP64 true
+    residual at every restart.  ``rhs`` is ``[n, H, W]`` or ``[H, W]``.
+    Returns ``(x, info)`` with the reference's info keys."""
     import time
     started = time.perf_counter()
+    g = system.g
     rhs = torch.as_tensor(rhs)
-    op = system.adjoint if adjoint else system.apply
-    pre = system.fixed_preconditioner(shift, adjoint=adjoint)
-    trace = []
-    x0 = torch.zeros_like(rhs) if initial is None else torch.as_tensor(initial).to(rhs.dtype)
-    x, reason, steps = gmres(op, pre, rhs, x0, lambda k, u, r: trace.append({"steps": k, "residual": r}),
-                             restart=restart, max_cycles=max_cycles, tolerance=tolerance)
-    return x, {"reason": reason, "steps": steps, "residual": trace[-1]["residual"],
-               "seconds": time.perf_counter() - started, "dtype": str(rhs.dtype), "method": "gmres",
-               "trace": trace}
+    squeeze = rhs.dim() == 2
+    b = (rhs[None] if squeeze else rhs)
+    if b.dim() != 3 or tuple(b.shape[1:]) != (g.H, g.W):
+        raise ValueError(f"rhs must be [n, {g.H}, {g.W}]")
+    if not b.is_cuda:
+        raise ValueError("rhs must be a CUDA tensor (no CPU path)")
+    b = b.to(torch.complex128).contiguous()
+    n_fields = b.shape[0]
+    if initial is None:
+        x = torch.zeros_like(b)
+    else:
+        x = torch.as_tensor(initial).to(b.device, torch.complex128).reshape(b.shape).clone().contiguous()
+    lib = _lib.load()
+    nbytes = lib.nsr_dense_solve_workspace_size(ctypes.byref(g.struct), n_fields, int(restart))
+    if nbytes == 0:
+        raise ValueError("unsupported dense grid for the preconditioner's transforms, or a bad restart length")
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=b.device)
+    per_field = torch.empty(n_fields, dtype=torch.float64, device=b.device)
+    params = _lib.NsrDenseSolveParams(float(tolerance), float(shift), float((system.k0 * g.dx) ** 2),
+                                      float(system.scal.real), float(system.scal.imag), int(restart),
+                                      int(max_cycles), int(bool(adjoint)), 0)
+    info = _lib.NsrDenseSolveInfo()
+    _lib.check(lib.nsr_dense_solve(ctypes.byref(g.struct), ctypes.c_void_p(system.coef.data_ptr()),
+                                   ctypes.byref(params), n_fields, ctypes.c_void_p(b.data_ptr()),
+                                   ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(per_field.data_ptr()),
+                                   ctypes.byref(info), ctypes.c_void_p(ws.data_ptr()), nbytes,
+                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    reason = _lib.REASONS[int(info.status)]
+    if reason == "nonfinite":
+        reason = "iteration_budget"   # the reference's GMRES knows only these two reasons
+    x = x.to(rhs.dtype) if rhs.dtype in (torch.complex64, torch.complex128) else x
+    return (x[0] if squeeze else x), {
+        "reason": reason, "steps": int(info.steps), "residual": float(info.residual),
+        "max_angle_residual": float(per_field.max()), "seconds": time.perf_counter() - started,
+        "dtype": "complex64 Krylov / FP64 residual", "method": "gmres", "cycles": int(info.cycles)}
 
 
 def homogeneous_reference(geometry: DenseGeometry, frequencies, lines, tolerance=1e-4, device="cuda"):
@@ -303,7 +288,7 @@ def homogeneous_reference(geometry: DenseGeometry, frequencies, lines, tolerance
         src = s0.source(lines[k].to(torch.complex128))
         p, info = solve(s0, src, tolerance=tolerance, restart=32, max_cycles=80)
         if info["reason"] != "converged":
-            raise RuntimeError(f"Homogeneous reference failed at {f} Hz: {info['trace'][-1]}")
+            raise RuntimeError(f"Homogeneous reference failed at {f} Hz: {info}")
         out[:, k] = p[:, g.pz:g.pz + g.h, g.px:g.px + g.w].to(torch.complex64)
     return out
 

@@ -1,7 +1,7 @@
 """Generate golden vectors from the reference implementation (run in a container
 that has the reference checked out; machines that only run the tests do not need this script).
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py REFERENCE_CHECKOUT
 
 Writes ``tests/golden/reference_5pt.npz`` holding, from the reference's own
 ``nsrno.theranostic.wave`` module:
@@ -80,4 +80,6 @@ def main(reference_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} REFERENCE_CHECKOUT")
+    main(sys.argv[1])

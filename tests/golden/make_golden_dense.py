@@ -1,7 +1,7 @@
 """Generate golden vectors of the reference's 8th-order dense operator
 (run in a container that has the reference checked out; not needed where the tests only run).
 
-    python tests/golden/make_golden_dense.py /root/reference
+    python tests/golden/make_golden_dense.py REFERENCE_CHECKOUT
 
 Writes ``tests/golden/reference_dense.npz`` with a synthetic acquisition spec
 (the V5 metadata is not part of the reference checkout), a seeded medium and
@@ -92,4 +92,6 @@ def main(reference_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} REFERENCE_CHECKOUT")
+    main(sys.argv[1])

@@ -2,7 +2,7 @@
 implementation (run in a container that has the reference checked out; the GPU
 box does not need this script).
 
-    python tests/golden/make_golden_learned.py /root/reference
+    python tests/golden/make_golden_learned.py REFERENCE_CHECKOUT
 
 Writes ``tests/golden/reference_learned.npz``.  The reference's own
 ``LearnedPreconditioner`` (nsrno/conditioned_wave.py:94-117) and ``learned_apply``
@@ -83,4 +83,6 @@ def main(reference_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} REFERENCE_CHECKOUT")
+    main(sys.argv[1])
