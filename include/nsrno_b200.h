@@ -43,7 +43,8 @@ enum {
 /* Library error codes (cudaError_t values stay below 1000). */
 enum {
   NSR_ERR_ARGUMENT = 1001,       /* null pointer, bad size or bad parameter   */
-  NSR_ERR_UNSUPPORTED_SIZE = 1002, /* nz or nx not 2^a 3^b in [8, 2048]       */
+  NSR_ERR_UNSUPPORTED_SIZE = 1002, /* nz or nx outside [8, 2048] or with a
+                                    prime factor above 61 (FFT sizes)    */
   NSR_ERR_WORKSPACE = 1003,      /* workspace smaller than the query returned */
   NSR_ERR_INTERNAL = 1004,       /* solver loop did not drain its queue       */
   NSR_ERR_CAPACITY = 1005,       /* request exceeds a fixed capacity          */
@@ -319,7 +320,7 @@ int nsr_tangent_rhs(const NsrGrid* grid, const void* coef, const double* freq_hz
  * m = 1/(1 + lap/k0^2 - i shift) and the 8th-order staggered symbols in lap
  * (nsrno/conditioned_wave.py:90-92, nsrno/dense_wave.py:194-196); adjoint = 1
  * conjugates m as the reference's adjoint solve does.  k0dx2 = (k0 dx)^2 with
- * the system's k0 = 2 sin(pi f dt)/(dt c0).  H and W must be 2^a 3^b in
+ * the system's k0 = 2 sin(pi f dt)/(dt c0).  H and W must be FFT sizes (see NSR_ERR_UNSUPPORTED_SIZE) in
  * [8, 2048].  x, y: c64 [n_fields][H][W]. */
 size_t nsr_dense_precondition_workspace_size(const NsrDenseGrid* grid, int32_t n_fields);
 int nsr_dense_precondition(const NsrDenseGrid* grid, double k0dx2, double shift, int32_t n_fields,

@@ -11,6 +11,8 @@
 
 #define NSR_MAX_RADIX_STAGES 12
 #define NSR_MAX_LINE 2048
+// Largest prime radix of the transforms (direct DFT stages, see fft_stage_prime).
+#define NSR_MAX_PRIME_RADIX 61
 #define NSR_PI 3.14159265358979323846
 
 // ---------------------------------------------------------------------------
@@ -283,6 +285,44 @@ __device__ __forceinline__ void fft_stage(float2* s, int nl, int lstride, int es
   }
 }
 
+// One DIF stage (forward) or its inverse for a prime radix R > 3, as a direct
+// R-point DFT: y_k = sum_q v_q W_R^(q k), W_R^e = tw[e n / R].  The cost is
+// R complex multiply-adds per point, which the sizes that need these stages
+// (paddings such as 1056 = 2^5 3 11 and 1216 = 2^6 19) can afford.
+template <bool INV>
+__device__ __noinline__ void fft_stage_prime(float2* s, int nl, int lstride, int estride, bool line_fast,
+                                             const FftPlan& P, int L, int R) {
+  const int m = L / R;
+  const int per_line = P.n / R;
+  const int nb = nl * per_line;
+  const int tstep = P.n / L;
+  const int rstep = P.n / R;
+  float2 v[NSR_MAX_PRIME_RADIX], y[NSR_MAX_PRIME_RADIX];
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    int l, bb;
+    if (line_fast) { l = b % nl; bb = b / nl; } else { l = b / per_line; bb = b % per_line; }
+    const int o = bb / m, j = bb - o * m;
+    float2* base = s + l * lstride + (o * L + j) * estride;
+    for (int q = 0; q < R; ++q) v[q] = base[q * m * estride];
+    if (INV)
+      for (int k = 1; k < R; ++k) v[k] = v[k] * conjc(__ldg(&P.tw[j * k * tstep]));
+    for (int k = 0; k < R; ++k) {
+      float2 acc = v[0];
+      int e = 0;
+      for (int q = 1; q < R; ++q) {
+        e += k;
+        if (e >= R) e -= R;
+        const float2 w = __ldg(&P.tw[e * rstep]);
+        acc = acc + v[q] * (INV ? conjc(w) : w);
+      }
+      y[k] = acc;
+    }
+    if (!INV)
+      for (int k = 1; k < R; ++k) y[k] = y[k] * __ldg(&P.tw[j * k * tstep]);
+    for (int q = 0; q < R; ++q) base[q * m * estride] = y[q];
+  }
+}
+
 template <bool INV>
 __device__ void fft_lines(float2* s, int nl, int lstride, int estride, bool line_fast, const FftPlan& P) {
   if (!INV) {
@@ -294,7 +334,8 @@ __device__ void fft_lines(float2* s, int nl, int lstride, int estride, bool line
         case 3: fft_stage<3, false>(s, nl, lstride, estride, line_fast, P, L); break;
         case 4: fft_stage<4, false>(s, nl, lstride, estride, line_fast, P, L); break;
         case 8: fft_stage<8, false>(s, nl, lstride, estride, line_fast, P, L); break;
-        default: fft_stage<16, false>(s, nl, lstride, estride, line_fast, P, L); break;
+        case 16: fft_stage<16, false>(s, nl, lstride, estride, line_fast, P, L); break;
+        default: fft_stage_prime<false>(s, nl, lstride, estride, line_fast, P, L, R); break;
       }
       __syncthreads();
       L /= R;
@@ -311,7 +352,8 @@ __device__ void fft_lines(float2* s, int nl, int lstride, int estride, bool line
         case 3: fft_stage<3, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
         case 4: fft_stage<4, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
         case 8: fft_stage<8, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
-        default: fft_stage<16, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+        case 16: fft_stage<16, true>(s, nl, lstride, estride, line_fast, P, Ls[st]); break;
+        default: fft_stage_prime<true>(s, nl, lstride, estride, line_fast, P, Ls[st], R); break;
       }
       __syncthreads();
     }
@@ -327,15 +369,29 @@ struct RadixList {
   int r[NSR_MAX_RADIX_STAGES];
 };
 
+__host__ __device__ constexpr bool nsr_is_prime(int p) {
+  if (p < 2) return false;
+  for (int d = 2; d * d <= p; ++d)
+    if (p % d == 0) return false;
+  return true;
+}
+
 __host__ __device__ constexpr RadixList nsr_radix_list(int n) {
-  // n = 2^a 3^b: the radix-3 stages first, then 2^(a mod 4) (one radix-2, -4 or
-  // -8 stage), then radix-16 stages, so that every size divisible by 16 ends
-  // with a radix-16 stage on contiguous 16-element groups.
+  // n = p1 p2 ... 2^a 3^b with primes 5 <= p <= NSR_MAX_PRIME_RADIX: one
+  // direct-DFT stage per such prime first, then the radix-3 stages, then
+  // 2^(a mod 4) (one radix-2, -4 or -8 stage), then radix-16 stages, so that
+  // every size divisible by 16 ends with a radix-16 stage on contiguous
+  // 16-element groups.  nst = 0 for sizes with a larger prime factor.
   RadixList L{0, {0}};
   int a = 0, b = 0, m = n;
+  int k = 0;
+  for (int p = 5; p <= NSR_MAX_PRIME_RADIX; p += 2) {
+    if (!nsr_is_prime(p)) continue;
+    while (m % p == 0 && k < NSR_MAX_RADIX_STAGES) { m /= p; L.r[k++] = p; }
+  }
   while (m % 2 == 0) { m /= 2; ++a; }
   while (m % 3 == 0) { m /= 3; ++b; }
-  int k = 0;
+  if (m != 1 || n < 2) return RadixList{0, {0}};
   for (int i = 0; i < b && k < NSR_MAX_RADIX_STAGES; ++i) L.r[k++] = 3;
   const int rem = a % 4;
   if (rem > 0 && k < NSR_MAX_RADIX_STAGES) L.r[k++] = 1 << rem;
@@ -558,15 +614,15 @@ __device__ __forceinline__ bool fft_cols_fused(float2* s, const FftPlan& P, MUL 
   }
 }
 
-// Host-side radix plan: n = 2^a 3^b, 8 <= n <= 2048.  Powers of two are split
-// into 8s with 4s and 2s so that stages stay balanced (1024 = 8*8*4*4).
+// Host-side radix plan of a line of n points, 8 <= n <= 2048, every prime
+// factor at most NSR_MAX_PRIME_RADIX (the stages of nsr_radix_list).
 __host__ __device__ inline bool nsr_make_radices(int n, int* radix, int* nst) {
   if (n < 8 || n > NSR_MAX_LINE) return false;
-  int m = n;
-  while (m % 2 == 0) m /= 2;
-  while (m % 3 == 0) m /= 3;
-  if (m != 1) return false;
   const RadixList L = nsr_radix_list(n);
+  if (L.nst == 0) return false;
+  int prod = 1;
+  for (int k = 0; k < L.nst; ++k) prod *= L.r[k];
+  if (prod != n) return false;
   for (int k = 0; k < L.nst; ++k) radix[k] = L.r[k];
   *nst = L.nst;
   return true;

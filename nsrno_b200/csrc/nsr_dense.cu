@@ -228,7 +228,8 @@ extern "C" int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, dou
 //   M r = mask * IFFT((1 + lap/k0^2 - i shift)^-1 FFT(r)),
 // lap = -(|Dx|^2 + |Dz|^2) with the 8th-order staggered symbols
 // |D(q)|^2 = (2 sum_k a_k sin((k + 1/2) q))^2 / dx^2 (conditioned_wave.py:24-27).
-// The transforms are the solver's row and column FFTs (grids of 2^a 3^b).
+// The transforms are the solver's row and column FFTs (sizes 8..2048 whose
+// prime factors are at most 61, e.g. the 1056 x 1216 padding of the reference).
 // ---------------------------------------------------------------------------
 __global__ void k_dense_symbol(int n, FftPlan plan, float* d2) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {

@@ -15,7 +15,7 @@ extern "C" const char* nsr_error_string(int code) {
   switch (code) {
     case 0: return "ok";
     case NSR_ERR_ARGUMENT: return "nsrno_b200: invalid argument";
-    case NSR_ERR_UNSUPPORTED_SIZE: return "nsrno_b200: nz and nx must be 2^a 3^b between 8 and 2048";
+    case NSR_ERR_UNSUPPORTED_SIZE: return "nsrno_b200: nz and nx must be between 8 and 2048 with no prime factor above 61";
     case NSR_ERR_WORKSPACE: return "nsrno_b200: workspace too small";
     case NSR_ERR_INTERNAL: return "nsrno_b200: solver queue did not drain";
     case NSR_ERR_CAPACITY: return "nsrno_b200: request exceeds the fixed capacity";

@@ -179,7 +179,7 @@ class DenseSystem:
             lib = _lib.load()
             nbytes = lib.nsr_dense_precondition_workspace_size(ctypes.byref(g.struct), x.shape[0])
             if nbytes == 0:
-                raise ValueError("the dense preconditioner needs H and W of the form 2^a 3^b in [8, 2048]")
+                raise ValueError("the dense preconditioner needs H and W in [8, 2048] with no prime factor above 61")
             ws = torch.empty(nbytes, dtype=torch.uint8, device=x.device)
             y = torch.empty_like(x)
             _lib.check(lib.nsr_dense_precondition(ctypes.byref(g.struct), float(k0dx2), float(shift), x.shape[0],

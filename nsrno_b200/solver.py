@@ -190,7 +190,7 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
     grid = medium._grid
     ws_bytes = lib.nsr_solve_workspace_size(ctypes.byref(grid), n_slots)
     if ws_bytes == 0:
-        raise ValueError("unsupported grid for the batched solver (nz, nx must be 2^a 3^b in [8, 2048])")
+        raise ValueError("unsupported grid for the batched solver (nz, nx in [8, 2048] with no prime factor above 61)")
     ws = (workspace or _default_ws).get(ws_bytes, dev)
     if out is None:
         out = BatchResult(iq=torch.empty((S, n_rx), dtype=torch.complex128, device=dev),

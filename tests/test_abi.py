@@ -40,7 +40,7 @@ def test_version_and_error_strings(lib):
     from nsrno_b200 import _lib
     assert lib.nsr_version() >= 100
     assert b"invalid argument" in lib.nsr_error_string(1001)
-    assert b"2^a 3^b" in lib.nsr_error_string(1002)
+    assert b"prime factor" in lib.nsr_error_string(1002)
     with pytest.raises(RuntimeError, match="workspace"):
         _lib.check(1003)
     assert _lib.check(0) == 0
@@ -72,7 +72,8 @@ def test_workspace_queries(lib):
     # iterates per slot, plus tables
     assert ws >= 16 * n * (8 * 8 + 2 * 16)
     assert ws < 16 * n * (8 * 8 + 2 * 16) + (1 << 22)
-    assert lib.nsr_solve_workspace_size(ctypes.byref(grid(nz=7 * 16)), 4) == 0   # 112 = 2^4 * 7
+    assert lib.nsr_solve_workspace_size(ctypes.byref(grid(nz=2 * 67)), 4) == 0   # prime factor 67 > 61
+    assert lib.nsr_solve_workspace_size(ctypes.byref(grid(nz=7 * 16)), 4) > 0    # 112 = 7 * 2^4
     assert lib.nsr_solve_workspace_size(ctypes.byref(g), 0) == 0
     assert lib.nsr_precondition_workspace_size(ctypes.byref(g), 2) >= 2 * n * 8
     assert lib.nsr_precondition_workspace_size(ctypes.byref(grid(nx=4096)), 1) == 0

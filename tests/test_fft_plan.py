@@ -14,7 +14,19 @@ import pytest
 
 from conftest import ROOT
 
-SIZES = [8, 24, 48, 64, 81, 96, 162, 256, 384, 512, 768, 1024, 1536, 2048]
+SIZES = [8, 24, 48, 64, 81, 96, 162, 256, 384, 512, 768, 1024, 1536, 2048,
+         35, 110, 770, 961, 1056, 1121, 1216, 1210, 2 * 61]
+
+
+def _smooth(n):
+    """True for n = 2^a 3^b."""
+    for p in (2, 3):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
+SMOOTH = [n for n in SIZES if _smooth(n)]
 
 PROBE = r"""
 #include <cstdio>
@@ -82,9 +94,26 @@ def dif_forward(x, radix):
 
 def test_every_size_has_a_plan(plans):
     assert sorted(plans) == sorted(SIZES)
+    primes = {q for q in range(5, 62) if all(q % r for r in range(2, q))}
     for n, p in plans.items():
         assert int(np.prod(p["radix"])) == n
-        assert set(p["radix"]) <= {2, 3, 4, 8, 16}
+        assert set(p["radix"]) <= {2, 3, 4, 8, 16} | primes
+        if n in SMOOTH:   # 2^a 3^b: the power-of-two and radix-3 stages only
+            assert set(p["radix"]) <= {2, 3, 4, 8, 16}
+
+
+def test_sizes_with_a_prime_factor_above_61_have_no_plan(tmp_path):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(nvcc).exists():
+        pytest.skip("nvcc not available")
+    src, exe = tmp_path / "bad.cu", tmp_path / "bad"
+    src.write_text('#include <cstdio>\n#include "nsr_common.cuh"\nint main() { int r[NSR_MAX_RADIX_STAGES], k;'
+                   ' std::printf("%d %d %d %d\\n", nsr_make_radices(134, r, &k), nsr_make_radices(2 * 1021, r, &k),'
+                   ' nsr_make_radices(4096, r, &k), nsr_make_radices(122, r, &k)); return 0; }\n')
+    subprocess.run([nvcc, "-std=c++17", f"-I{ROOT / 'include'}", f"-I{ROOT / 'nsrno_b200' / 'csrc'}",
+                    str(src), "-o", str(exe)], check=True)
+    assert subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split() == \
+        ["0", "0", "0", "1"]
 
 
 def test_sizes_divisible_by_16_end_with_a_radix_16_stage(plans):
