@@ -137,3 +137,55 @@ def test_homogeneous_reference_fields(cuda, gold, tmp_path):
             assert rel(s0.apply(p), src[a]) < 1e-5
     save_reference(tmp_path, fields)
     assert np.load(tmp_path / "a01.npy").shape == (2, g.h, g.w)
+
+
+def _spec(h, w):
+    return {"medium_shape": [h, w], "dx_m": 5e-5, "x0_m": -0.004, "z0_m": -0.0002, "native_dt_s": 2.5e-9,
+            "pml": 12, "eta_per_unit_alpha": [0.012, 0.021], "taus_s": [2.0e-8, 1.5e-7],
+            "source_c_lookup_zx": [10, 20]}
+
+
+def _medium(h, w, seed):
+    rng = np.random.default_rng(seed)
+    medium = np.stack((1500 + 40 * rng.standard_normal((h, w)), 1000 + 30 * rng.standard_normal((h, w))))
+    return medium, rng.uniform(0.1, 1.0, (h, w))
+
+
+def test_dense_preconditioner_at_the_reference_padding(cuda):
+    """The reference pads its 961 x 1121 medium to 1056 x 1216 = (2^5 3 11) x (2^6 19)
+    (nsrno/conditioned_wave.py:16-22); the preconditioner runs at that size."""
+    from nsrno_b200.dense import DenseGeometry, DenseSystem
+    spec = _spec(961, 1121)
+    g = DenseGeometry(spec)
+    assert (g.H, g.W) == (1056, 1216)
+    medium, alpha = _medium(961, 1121, 3)
+    s = DenseSystem(g, medium, alpha, 6.2e6, device=cuda)
+    o = D.DenseSystem(D.DenseGeometry(spec), medium, alpha, 6.2e6)
+    rng = np.random.default_rng(4)
+    p = rng.standard_normal((g.H, g.W)) + 1j * rng.standard_normal((g.H, g.W))
+    for adjoint in (False, True):
+        y = s.fixed_preconditioner(adjoint=adjoint)(torch.as_tensor(p, device=cuda)).cpu().numpy()
+        assert rel(y, o.fixed_preconditioner(p, adjoint=adjoint)) < 2e-5
+
+
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_dense_device_solve_on_a_prime_padding(cuda, adjoint):
+    """80 x 150 pads to 160 x 224 = (2^5 5) x (2^5 7): GMRES(24) on the device
+    for three fields as one vector; the FP64 residual of every field, checked
+    with the oracle operator, meets the tolerance."""
+    from nsrno_b200.dense import DenseGeometry, DenseSystem, solve
+    spec = _spec(80, 150)
+    g = DenseGeometry(spec)
+    assert (g.H, g.W) == (160, 224)
+    medium, alpha = _medium(80, 150, 5)
+    s = DenseSystem(g, medium, alpha, 5.1e6, device=cuda)
+    o = D.DenseSystem(D.DenseGeometry(spec), medium, alpha, 5.1e6)
+    rng = np.random.default_rng(6)
+    b = (rng.standard_normal((3, g.H, g.W)) + 1j * rng.standard_normal((3, g.H, g.W))) * o.g.mask
+    x, info = solve(s, torch.as_tensor(b, device=cuda), adjoint=adjoint, tolerance=1e-8, max_cycles=400)
+    assert info["reason"] == "converged" and info["residual"] < 1e-8
+    assert info["max_angle_residual"] < 1e-7
+    x = x.cpu().numpy()
+    for k in range(3):
+        ax = o.adjoint(x[k]) if adjoint else o.apply(x[k])
+        assert rel(ax, b[k]) < 1e-7

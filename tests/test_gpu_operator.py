@@ -96,7 +96,8 @@ def numpy_precondition(x, nz, nx, kh2, shift, adjoint=False):
     return np.fft.ifft2(np.fft.fft2(x) * mul)
 
 
-@pytest.mark.parametrize("shape", [(48, 64), (81, 81), (162, 96), (256, 256), (768, 1024), (24, 2048)])
+@pytest.mark.parametrize("shape", [(48, 64), (81, 81), (162, 96), (256, 256), (768, 1024), (24, 2048),
+                                   (110, 140), (961, 122), (1056, 1216)])
 @pytest.mark.parametrize("adjoint", [False, True])
 def test_precondition_matches_numpy_fft(cuda, shape, adjoint):
     from nsrno_b200 import precondition
