@@ -120,3 +120,40 @@ def test_learned_and_fixed_gradients_agree(cuda):
         outs.append(out.detach().cpu().numpy())
     assert rel(outs[1], outs[0]) < 1e-6
     assert rel(grads[1], grads[0]) < 1e-5
+
+
+def test_truncated_is_one_learned_gmres_cycle(cuda):
+    """``truncated`` is one GMRES cycle of K steps with the learned
+    preconditioner (nsrno/dense_surrogate.py:30-36 through batched_gmres_cycle,
+    nsrno/dense_wave.py:84-116): channels and the actual residual equal the
+    oracle's restated cycle (complex128, SciPy operator, oracle network)."""
+    import math
+    from oracle import learned_ref as L
+    from nsrno_b200 import HelmholtzSurrogate, bin_frequency
+    from nsrno_b200.learned import LearnedPreconditioner
+    rec, med = small_breast(cuda)
+    geo = med.geometry
+    net = LearnedPreconditioner.load(device=cuda)
+    sur = HelmholtzSurrogate(geo, np.rad2deg(rec.angles), bins=[300], response=False, preconditioner=net)
+    medium = torch.as_tensor(np.stack((rec.c, rec.rho)).astype(np.float64), device=cuda)
+    alpha = torch.as_tensor(rec.alpha.astype(np.float64), device=cuda)
+    f = bin_frequency(300)
+    K = 8
+    spec = spec_of(rec)
+    a, b, t = med.coef64.cpu().numpy()
+    A = H.operator_planes(spec, a, b, t, f) * rec.h ** 2
+    lp = L.Learned(net.params.double().cpu(), med.c.double().cpu(), med.rho.double().cpu(), med.alpha.double().cpu(),
+                   f, rec.h, rec.c0)
+    pre = lambda v: lp.apply(torch.as_tensor(v.reshape(rec.nz, rec.nx))).numpy().ravel()
+    ch, res = sur.truncated(medium, alpha, 300, angles=[0, 2], iterations=K)
+    rr, bb = 0.0, 0.0
+    for k, a_idx in enumerate([0, 2]):
+        rhs = H.plane_wave_rhs(spec, f, rec.angles[a_idx]) * rec.h ** 2
+        x_ref, _, steps = H.gmres(lambda v: A @ v, rhs, restart=K, max_cycles=1, tolerance=1e-30, precondition=pre)
+        assert rel(ch[k].cpu().numpy(), H.receivers(spec, x_ref)) < 1e-4
+        rr += np.linalg.norm(A @ x_ref - rhs) ** 2
+        bb += np.linalg.norm(rhs) ** 2
+    assert abs(res - math.sqrt(rr / bb)) < 1e-4 * res
+    # more steps, smaller residual
+    _, res16 = sur.truncated(medium, alpha, 300, angles=[0, 2], iterations=16)
+    assert res16 < res
