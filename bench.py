@@ -3,16 +3,22 @@
 Workload: the synthetic breast record, 1024 (x) x 768 (z) nodes at 0.05 mm,
 11 plane-wave angles x 294 frequency bins (4.015-8.896 MHz) = 3234 systems,
 BiCGSTAB to a true relative residual of 1e-6.  One step solves a batch of
-SYSTEMS_PER_STEP systems (4 bins x 11 angles, bins spread over the band by a
-fixed stride permutation) through the resident-slot queue.  Under torchrun
-every rank takes different bins (weak scaling, no collective on the data path).
+SYSTEMS_PER_STEP systems (4 bins x 11 angles) through the resident-slot queue;
+a rank's bins come from the longest-first partition of the band over the ranks
+(``nsrno_b200.shard.partition_bins``), visited by a fixed stride so that every
+step sees low and high frequencies.  Under torchrun every rank takes different
+bins (weak scaling, no collective on the data path).
 
 Two arms run on the same GPU and the same steps: the headline "learned-init"
 arm (the trained learned preconditioner: its network set-up for the step's
 bins is inside the timed region) and the "plain Krylov" arm (the fixed
 shifted-Laplace preconditioner, shift 0.15), reported under ``plain_krylov``.
+Before timing, the launch shapes of both arms are chosen by the autotuner
+(``nsrno_b200.tune``; cached per GPU and grid).  Per-kernel durations come from
+a separate, untimed profiling pass.  ``record`` pushes all 3234 systems of the
+record through one solve queue (learned arm; ``--record`` adds the plain arm).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--record]
 
 Prints one JSON line on rank 0.
 """
@@ -22,6 +28,7 @@ import argparse
 import json
 import math
 import os
+import platform
 import re
 import statistics
 import subprocess
@@ -71,6 +78,10 @@ def parse():
     p.add_argument("--cpu-sample-bins", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-Krylov comparison arm")
+    p.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
+    p.add_argument("--retune", action="store_true", help="tune even when a cached choice exists")
+    p.add_argument("--record", action="store_true", help="also run the plain arm over the whole record")
+    p.add_argument("--no-record", action="store_true", help="skip the whole-record run")
     p.add_argument("--plain-only", action="store_true",
                    help="run only the plain-Krylov arm (for profiling it); prints a short line, not the bench line")
     return p.parse_args()
@@ -83,16 +94,28 @@ def dist_env():
     return rank, world, local
 
 
-def bin_permutation(n_bins=294, stride=151):
-    """Fixed stride permutation so that consecutive steps sample the whole band."""
-    return (np.arange(n_bins) * stride) % n_bins
+def _coprime_stride(n, target):
+    s = max(1, int(round(target)))
+    while math.gcd(s, n) != 1:
+        s += 1
+    return s
+
+
+def rank_bins(record, rank, world):
+    """This rank's bins (longest-first partition of the band), in a stride
+    order that spreads consecutive steps over the whole band."""
+    from nsrno_b200.shard import partition_bins
+    mine = partition_bins(record.frequencies, world)[rank]
+    n = len(mine)
+    order = (np.arange(n) * _coprime_stride(n, 0.514 * n)) % n
+    return mine[order]
 
 
 def step_systems(record, step, rank, world):
     """(freqs, angles) of one step on one rank, highest frequency first."""
-    perm = bin_permutation(len(record.frequencies))
-    first = (step * world + rank) * BINS_PER_STEP
-    bins = [perm[(first + k) % len(perm)] for k in range(BINS_PER_STEP)]
+    mine = rank_bins(record, rank, world)
+    first = step * BINS_PER_STEP
+    bins = [mine[(first + k) % len(mine)] for k in range(BINS_PER_STEP)]
     f = np.repeat(record.frequencies[bins], N_ANGLES)
     a = np.tile(record.angles, BINS_PER_STEP)
     order = np.argsort(-f, kind="stable")
@@ -172,37 +195,140 @@ def profiled_traffic(arm, kernel):
     return None
 
 
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
+
+
 # ---------------------------------------------------------------------------
 # CPU arm: the reference algorithm of the path (assemble, one SuperLU factor
-# per frequency shared by all angles, solve) restated by the oracle.
+# per frequency shared by all angles, solve) restated by the oracle.  Worker
+# processes build the record once, outside any timed region.
 # ---------------------------------------------------------------------------
-def _cpu_one_bin(args):
-    import os as _os
-    _os.environ.setdefault("OMP_NUM_THREADS", "1")
+_REC = None
+_SPEC = None
+
+
+def _cpu_init():
+    os.environ["OMP_NUM_THREADS"] = "1"
+    global _REC, _SPEC
     from oracle import helmholtz_ref as H
     from nsrno_b200.media import breast_record
-    rec = breast_record()
-    spec = H.Spec(nz=rec.nz, nx=rec.nx, h=rec.h, n_pml=rec.n_pml, c0=rec.c0, rho0=rec.rho0,
-                  pml_strength=rec.pml_strength, face=rec.face, rx_cols=rec.rx_cols,
-                  aperture_half_width=rec.aperture_half_width, alpha_power=rec.alpha_power)
-    fields, seconds, res = H.time_lu_frequency(spec, rec.c, rec.rho, rec.alpha, rec.frequencies[args], rec.angles)
+    try:
+        from threadpoolctl import threadpool_limits
+        threadpool_limits(1)
+    except ImportError:
+        pass
+    _REC = breast_record()
+    r = _REC
+    _SPEC = H.Spec(nz=r.nz, nx=r.nx, h=r.h, n_pml=r.n_pml, c0=r.c0, rho0=r.rho0, pml_strength=r.pml_strength,
+                   face=r.face, rx_cols=r.rx_cols, aperture_half_width=r.aperture_half_width,
+                   alpha_power=r.alpha_power)
+
+
+def _cpu_one_bin(b):
+    from oracle import helmholtz_ref as H
+    rec = _REC
+    fields, seconds, res = H.time_lu_frequency(_SPEC, rec.c, rec.rho, rec.alpha, rec.frequencies[b], rec.angles)
     return seconds, res, len(rec.angles)
 
 
-def cpu_sample(n_bins, processes):
-    """Wall time of n_bins frequencies (11 angles each) on `processes` host processes."""
-    import multiprocessing as mp
-    perm = bin_permutation()
-    bins = [int(perm[k]) for k in range(n_bins)]
+def _noop(_):
+    return os.getpid()
+
+
+class CpuPool:
+    """A warmed pool of `n` single-threaded worker processes (spawn)."""
+
+    def __init__(self, n):
+        import multiprocessing as mp
+        self.n = n
+        self.pool = None
+        if n > 1:
+            self.pool = mp.get_context("spawn").Pool(n, initializer=_cpu_init)
+            self.pool.map(_noop, range(4 * n))
+        else:
+            _cpu_init()
+
+    def bins(self, bins):
+        t0 = time.perf_counter()
+        out = self.pool.map(_cpu_one_bin, bins, chunksize=1) if self.pool else [_cpu_one_bin(b) for b in bins]
+        wall = time.perf_counter() - t0
+        return wall, sum(o[2] for o in out), max(o[1] for o in out)
+
+    def close(self):
+        if self.pool:
+            self.pool.close()
+            self.pool.join()
+
+
+def _config1_gmres(args):
+    """One config-1 system by the oracle's GMRES(30) to 1e-7 (nsrno/wave_solver.py:9-36 restated), 1 thread."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+    try:
+        from threadpoolctl import threadpool_limits
+        threadpool_limits(1)
+    except ImportError:
+        pass
+    from oracle import helmholtz_ref as H
+    from nsrno_b200.media import blob_record
+    s = args
+    rec = blob_record()
+    spec = H.Spec(nz=rec.nz, nx=rec.nx, h=rec.h, n_pml=rec.n_pml, c0=rec.c0, rho0=rec.rho0,
+                  pml_strength=rec.pml_strength, face=rec.face, rx_cols=rec.rx_cols,
+                  aperture_half_width=rec.aperture_half_width, alpha_power=rec.alpha_power)
+    f, th = rec.systems()
     t0 = time.perf_counter()
-    if processes <= 1:
-        out = [_cpu_one_bin(b) for b in bins]
-    else:
-        with mp.get_context("spawn").Pool(processes) as pool:
-            out = pool.map(_cpu_one_bin, bins)
-    wall = time.perf_counter() - t0
-    solves = sum(o[2] for o in out)
-    return solves / wall, wall, solves, max(o[1] for o in out)
+    A = H.operator(spec, rec.c, rec.rho, rec.alpha, f[s]) * rec.h ** 2
+    b = H.plane_wave_rhs(spec, f[s], th[s]) * rec.h ** 2
+    kh2 = (2 * math.pi * f[s] / rec.c0 * rec.h) ** 2
+    qz = np.sin(np.pi * np.arange(rec.nz) / rec.nz) ** 2
+    qx = np.sin(np.pi * np.arange(rec.nx) / rec.nx) ** 2
+    mul = 1.0 / (-4.0 * (qz[:, None] + qx[None, :]) + kh2 * (1 + 0.15j))
+    pre = lambda v: np.fft.ifft2(np.fft.fft2(v.reshape(rec.nz, rec.nx)) * mul).ravel()
+    x, reason, steps = H.gmres(lambda v: A @ v, b, restart=30, max_cycles=400, tolerance=1e-7, precondition=pre)
+    return time.perf_counter() - t0, reason, steps
+
+
+def config1_cpu(cores):
+    """Config 1 (256x256 blobs, 6 systems) on the host: the oracle's SuperLU
+    (one factorisation per frequency) and its GMRES(30) to 1e-7, at 1 thread
+    and over all cores (one process per system)."""
+    import multiprocessing as mp
+    from oracle import helmholtz_ref as H
+    from nsrno_b200.media import blob_record
+    try:
+        from threadpoolctl import threadpool_limits
+        limit = threadpool_limits(1)
+    except ImportError:
+        limit = None
+    rec = blob_record()
+    spec = H.Spec(nz=rec.nz, nx=rec.nx, h=rec.h, n_pml=rec.n_pml, c0=rec.c0, rho0=rec.rho0,
+                  pml_strength=rec.pml_strength, face=rec.face, rx_cols=rec.rx_cols,
+                  aperture_half_width=rec.aperture_half_width, alpha_power=rec.alpha_power)
+    t0 = time.perf_counter()
+    for f in rec.frequencies:
+        H.time_lu_frequency(spec, rec.c, rec.rho, rec.alpha, f, rec.angles)
+    lu_s = time.perf_counter() - t0
+    n_sys = len(rec.frequencies) * len(rec.angles)
+    one = [_config1_gmres(s) for s in range(n_sys)]
+    procs = max(1, min(cores, n_sys))
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        par = pool.map(_config1_gmres, range(n_sys), chunksize=1)
+    all_s = time.perf_counter() - t0
+    if limit is not None:
+        limit.restore_original_limits()
+    return {"systems": n_sys, "superlu_1thread_solves_per_s": n_sys / lu_s,
+            "gmres30_1thread_solves_per_s": n_sys / sum(o[0] for o in one),
+            "gmres30_allcores_solves_per_s": n_sys / all_s, "gmres30_allcores_processes": procs,
+            "gmres30_steps_mean": float(np.mean([o[2] for o in one])),
+            "gmres30_converged": all(o[1] == "converged" for o in one) and all(o[1] == "converged" for o in par)}
 
 
 def run_reference(args):
@@ -210,18 +336,32 @@ def run_reference(args):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    procs = max(1, min(cores, 8, args.cpu_sample_bins * max(1, args.steps)))
-    # each step: one bin per process (11 angles each), in parallel
-    for _ in range(args.warmup):
-        pass  # the factorisation has no warm state worth priming; warm-up steps are skipped
-    values = []
+    from nsrno_b200.media import breast_record
+    rec = breast_record()
+    # every host core, bounded by memory (a SuperLU factorisation of the
+    # 786,432-node system holds about 2 GB)
+    try:
+        import psutil
+        by_mem = max(1, int(psutil.virtual_memory().available // (3 << 30)))
+    except ImportError:
+        by_mem = cores
+    procs = max(1, min(cores, by_mem, len(rec.frequencies)))
+    pool = CpuPool(procs)
+    perm = rank_bins(rec, 0, 1)
+    # each step: `procs` bins (11 angles each) over the warmed worker processes
+    pos = 0
+    for _ in range(min(args.warmup, 1)):
+        pool.bins([int(perm[pos % len(perm)])])   # primes each worker's scipy state
+        pos += 1
     t_total = 0.0
     solves_total = 0
     for _ in range(max(1, args.steps)):
-        v, wall, solves, res = cpu_sample(procs, procs)
-        values.append(v)
+        bins = [int(perm[(pos + k) % len(perm)]) for k in range(procs)]
+        pos += procs
+        wall, solves, res = pool.bins(bins)
         t_total += wall
         solves_total += solves
+    pool.close()
     value = solves_total / t_total
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / max(1, args.steps),
@@ -230,7 +370,9 @@ def run_reference(args):
                                    "factor per bin + 11 angle solves (theranostic/wave.py:240-273 restated)",
                        "bins_per_step": procs},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
-                             "sample": f"{procs} bins x 11 angles per step on {procs} processes"},
+                             "host_cores": cores, "cpu_model": cpu_model(), "memory_bound_processes": by_mem,
+                             "sample": f"{procs} bins x 11 angles per step on {procs} single-threaded processes "
+                                       f"(pool and medium built outside the timed wall)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -242,7 +384,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    from nsrno_b200 import Geometry, Medium, Workspace, _lib, solve_batched
+    from nsrno_b200 import Geometry, Medium, Workspace, _lib, solve_batched, tune
     from nsrno_b200.learned import LearnedPreconditioner
     from nsrno_b200.media import breast_record
 
@@ -259,6 +401,23 @@ def run_ours(args):
     net = LearnedPreconditioner.load(device=dev)
     ws = Workspace()
 
+    # Launch shapes of both arms (autotuner, untimed; cached per GPU and grid).
+    shapes = {True: ({}, 16), False: ({}, 16)}
+    tuning = {}
+    if not args.no_tune:
+        f_s, a_s = step_systems(rec, 0, rank, world)
+        sample_setup = net.setup(med, np.unique(f_s))
+        for learned in (True, False):
+            if learned is False and args.no_plain:
+                continue
+            r = tune.tuned_config(med, f_s, a_s, learned=sample_setup if learned else None, n_slots=N_SLOTS,
+                                  refresh=args.retune)
+            shapes[learned] = tune.split(r["config"])
+            tuning["learned" if learned else "plain"] = {
+                "config": r["config"], "cached": r["cached"], "us_per_system_iteration": 1e6 * r["cost_s"],
+                "default_us_per_system_iteration": 1e6 * r["default_cost_s"], "gain": r["gain"]}
+        del sample_setup
+
     def one_step(step, learned, medium=med, profile=0, host=False):
         f, a = step_systems(rec, step, rank, world)
         if host:
@@ -267,8 +426,10 @@ def run_ours(args):
         setup = None
         if learned:
             setup = net.setup(medium, torch.unique(torch.as_tensor(f, device=dev)))
+        tiles, k = shapes[learned]
         return solve_batched(medium, f, a, tolerance=TOL, max_iterations=MAX_ITERS, n_slots=N_SLOTS,
-                             profile_iterations=profile, workspace=ws, learned=setup)
+                             profile_iterations=profile, workspace=ws, learned=setup, tiles=tiles,
+                             graph_iterations=k)
 
     def barrier():
         if world > 1:
@@ -276,6 +437,12 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     stream = torch.cuda.current_stream()
+
+    def max_ms(ms):
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t)
 
     def timed(learned, sample_clocks=False):
         for w in range(args.warmup):
@@ -289,26 +456,27 @@ def run_ours(args):
         results = []
         t0.record(stream)
         for k in range(args.steps):
-            results.append(one_step(k, learned, profile=PROFILE_ITERS))
+            results.append(one_step(k, learned))
         t1.record(stream)
         barrier()
         clock_info = clocks.stop() if clocks else None
-        ms_t = torch.tensor([t0.elapsed_time(t1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-        return float(ms_t), results, clock_info
+        return max_ms(t0.elapsed_time(t1)), results, clock_info
+
+    def profiled(learned):
+        """Per-kernel event durations of one step (untimed pass, launches not graphed)."""
+        r = one_step(0, learned, profile=PROFILE_ITERS)
+        torch.cuda.synchronize()
+        return r.extra["stats"]["kernel_ms"]
 
     n = rec.nz * rec.nx
     slots = min(N_SLOTS, SYSTEMS_PER_STEP)
     peak, peak_kind = peak_hbm()
     solves = SYSTEMS_PER_STEP * args.steps * world
 
-    def summarise(ms_max, results, per_node):
+    def summarise(ms_max, results, kms, per_node):
         status = torch.cat([r.status for r in results]).cpu().numpy()
         iters = torch.cat([r.iterations for r in results]).cpu().numpy()
         resid = torch.cat([r.residual for r in results]).cpu().numpy()
-        # per-kernel durations measured by events between launches (first iterations of every step)
-        kms = {k: float(np.mean([r.extra["stats"]["kernel_ms"][k] for r in results])) for k in per_node}
         alg = {k: n * (per_node[k] * slots + COEF_BYTES.get(k, 0)) for k in per_node}
         dominant = max(kms, key=kms.get)
         iter_ms = sum(kms.values())
@@ -322,7 +490,7 @@ def run_ours(args):
 
     if args.plain_only:
         ms_p, res_p, _ = timed(False)
-        P = summarise(ms_p, res_p, KERNEL_BYTES)
+        P = summarise(ms_p, res_p, profiled(False), KERNEL_BYTES)
         if rank == 0:
             print(json.dumps({"arm": "plain", "value": P["value"], "unit": UNIT, "kernel_ms": P["kms"],
                               "solves": P["solves"]}), flush=True)
@@ -331,11 +499,12 @@ def run_ours(args):
             dist.destroy_process_group()
         return
     ms_l, res_l, clock_info = timed(True, sample_clocks=True)
-    L = summarise(ms_l, res_l, LEARNED_BYTES)
     P = None
     if not args.no_plain:
         ms_p, res_p, _ = timed(False)
-        P = summarise(ms_p, res_p, KERNEL_BYTES)
+    L = summarise(ms_l, res_l, profiled(True), LEARNED_BYTES)
+    if not args.no_plain:
+        P = summarise(ms_p, res_p, profiled(False), KERNEL_BYTES)
     value = L["value"]
     dominant = L["dominant"]
     achieved = L["achieved"]
@@ -367,17 +536,47 @@ def run_ours(args):
             d2h = sum(t.numel() * t.element_size() for t in out)
         e1.record(stream)
         barrier()
-        e2e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-        e2e_value = solves / (float(e2e_ms) / 1e3)
+        e2e_value = solves / (max_ms(e0.elapsed_time(e1)) / 1e3)
+
+    # The whole record through one queue: every system of this rank's bins.
+    record = None
+    if not args.no_record:
+        mine = rank_bins(rec, rank, world)
+        f_all = np.repeat(rec.frequencies[mine], N_ANGLES)
+        a_all = np.tile(rec.angles, len(mine))
+        order = np.argsort(-f_all, kind="stable")
+        f_all, a_all = f_all[order], a_all[order]
+        record = {"systems": int(len(f_all) * world), "bins": int(len(mine) * world)}
+        for learned in ((True, False) if args.record and not args.no_plain else (True,)):
+            barrier()
+            r0 = torch.cuda.Event(enable_timing=True)
+            r1 = torch.cuda.Event(enable_timing=True)
+            r0.record(stream)
+            setup = net.setup(med, np.unique(f_all)) if learned else None
+            tiles, k = shapes[learned]
+            res = solve_batched(med, f_all, a_all, tolerance=TOL, max_iterations=MAX_ITERS, n_slots=N_SLOTS,
+                                workspace=ws, learned=setup, tiles=tiles, graph_iterations=k)
+            r1.record(stream)
+            barrier()
+            ms = max_ms(r0.elapsed_time(r1))
+            st = res.status.cpu().numpy()
+            record["learned" if learned else "plain"] = {
+                "value": len(f_all) * world / (ms / 1e3), "unit": UNIT, "seconds": ms / 1e3,
+                "converged_on_rank0": int((st == _lib.CONVERGED).sum()), "systems_on_rank0": int(len(st)),
+                "iterations_mean": float(res.iterations.float().mean()),
+                "residual_max": float(res.residual.max())}
+            del setup, res
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, wall, nsolves, _ = cpu_sample(args.cpu_sample_bins, 1)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_sample_bins} bin(s) x 11 angles: assemble + SuperLU factor + solves, "
-                         f"{wall:.1f} s on 1 core"}
+        cores = os.cpu_count() or 1
+        pool = CpuPool(1)
+        wall, nsolves, _ = pool.bins([int(b) for b in rank_bins(rec, 0, 1)[:args.cpu_sample_bins]])
+        cpu = {"value": nsolves / wall, "unit": UNIT, "cores": 1, "kind": "port", "host_cores": cores,
+               "cpu_model": cpu_model(),
+               "sample": f"{args.cpu_sample_bins} bin(s) x 11 angles of the breast record: assemble + SuperLU "
+                         f"factor + solves, {wall:.1f} s on 1 core",
+               "config1": config1_cpu(cores)}
 
     if rank == 0:
         line = {
@@ -390,7 +589,9 @@ def run_ours(args):
                                    "(fixed shifted-Laplace, shift 0.15) under plain_krylov",
                        "systems_per_step": SYSTEMS_PER_STEP, "n_slots": N_SLOTS, "grid_zx": [rec.nz, rec.nx],
                        "l2": f"inputs larger than L2: {slots * n * 96 / 1e9:.2f} GB resident Krylov state per GPU",
-                       "parallelism": f"frequency-sharded x{world}"},
+                       "parallelism": f"frequency-sharded x{world}",
+                       "tiles": {"learned": shapes[True][0], "learned_graph_iterations": shapes[True][1],
+                                 "plain": shapes[False][0], "plain_graph_iterations": shapes[False][1]}},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -401,6 +602,8 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clock_info,
             "solves": L["solves"],
+            "tuning": tuning or None,
+            "record": record,
             "plain_krylov": None if P is None else {
                 "value": P["value"], "unit": UNIT, "ms_per_step": P["ms_per_step"], "solves": P["solves"],
                 "learned_speedup": value / P["value"],

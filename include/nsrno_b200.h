@@ -77,7 +77,7 @@ typedef struct NsrTiles {
   int32_t cols_width;        /* columns per column-FFT CTA: 8 or 16            */
   int32_t row_tile;          /* rows per row-FFT CTA: 1..8                     */
   int32_t slot_groups;       /* independent slot groups on graph branches: 1, 2 */
-  int32_t reserved;
+  int32_t stencil_cols;      /* adjacent columns per stencil thread: 1 or 2    */
 } NsrTiles;
 
 /* Krylov parameters of nsr_solve_batched. */

@@ -67,6 +67,78 @@ __device__ __forceinline__ float2 stencil_pts(const Geo& g, const SysScalars& sc
 }
 
 
+// The same stencil with every per-system scalar already in float (set up once
+// per work item), so that no node pays a double-to-float conversion; the PML
+// profile multiplies by 1/n_pml instead of dividing.
+struct SysScalarsF {
+  float kh2, sig, fpow, inv_npml;
+  int lo, hi_z, hi_x;   // interior: lo < i < hi_z, lo < j < hi_x
+};
+
+__device__ __forceinline__ SysScalarsF sys_scalars_f(const Geo& g, const SysScalars& s) {
+  SysScalarsF f;
+  f.kh2 = (float)s.kh2;
+  f.sig = (float)s.sig;
+  f.fpow = (float)s.fpow;
+  f.inv_npml = g.n_pml > 0 ? 1.0f / (float)g.n_pml : 0.0f;
+  f.lo = g.n_pml;
+  f.hi_z = g.nz - 1 - g.n_pml;
+  f.hi_x = g.nx - 1 - g.n_pml;
+  return f;
+}
+
+__device__ __forceinline__ float pml_profile_f(float pos, int n, int n_pml, float inv_npml) {
+  float f = fmaxf((float)n_pml - pos, pos - (float)(n - 1 - n_pml)) * inv_npml;
+  f = fminf(fmaxf(f, 0.0f), 1.0f);
+  return f * f;
+}
+
+template <bool ADJ>
+__device__ __forceinline__ float2 stencil_pts_f(const Geo& g, const SysScalarsF& sf, int i, int j, float a_c,
+                                                float a_e, float a_w, float a_s, float a_n, float b_c, float t_c,
+                                                float2 pc, float2 pe, float2 pw, float2 ps, float2 pn) {
+  const float e = t_c * sf.fpow;
+  const float mb = sf.kh2 * b_c;
+  float2 mass = make_float2(mb * (1.0f - e * e), (ADJ ? -2.0f : 2.0f) * mb * e);
+  if (i > sf.lo && i < sf.hi_z && j > sf.lo && j < sf.hi_x) {
+    float2 y = mass * pc;
+    y = y + (0.5f * (a_c + a_e)) * (pe - pc);
+    y = y + (0.5f * (a_c + a_w)) * (pw - pc);
+    y = y + (0.5f * (a_c + a_s)) * (ps - pc);
+    y = y + (0.5f * (a_c + a_n)) * (pn - pc);
+    return y;
+  }
+  // PML: stretches at the node and the four half nodes (theranostic/wave.py:127-155)
+  const float fi = (float)i, fj = (float)j;
+  const float2 sx = make_float2(1.0f, sf.sig * pml_profile_f(fj, g.nx, g.n_pml, sf.inv_npml));
+  const float2 sz = make_float2(1.0f, sf.sig * pml_profile_f(fi, g.nz, g.n_pml, sf.inv_npml));
+  const float2 sxe = make_float2(1.0f, sf.sig * pml_profile_f(fj + 0.5f, g.nx, g.n_pml, sf.inv_npml));
+  const float2 sxw = make_float2(1.0f, sf.sig * pml_profile_f(fj - 0.5f, g.nx, g.n_pml, sf.inv_npml));
+  const float2 szs = make_float2(1.0f, sf.sig * pml_profile_f(fi + 0.5f, g.nz, g.n_pml, sf.inv_npml));
+  const float2 szn = make_float2(1.0f, sf.sig * pml_profile_f(fi - 0.5f, g.nz, g.n_pml, sf.inv_npml));
+  float2 fe = (0.5f * (a_c + a_e)) * divc(sz, sxe);
+  float2 fw = (0.5f * (a_c + a_w)) * divc(sz, sxw);
+  float2 fs = (0.5f * (a_c + a_s)) * divc(sx, szs);
+  float2 fn = (0.5f * (a_c + a_n)) * divc(sx, szn);
+  // mass * (sx sz): (sx sz) is the stretched cell measure
+  const float2 sxz = sx * sz;
+  mass = mass * (ADJ ? conjc(sxz) : sxz);
+  if (ADJ) { fe = conjc(fe); fw = conjc(fw); fs = conjc(fs); fn = conjc(fn); }
+  float2 y = mass * pc;
+  y = y + fe * (pe - pc);
+  y = y + fw * (pw - pc);
+  y = y + fs * (ps - pc);
+  y = y + fn * (pn - pc);
+  return y;
+}
+
+// Complex conj(a) * b accumulated in float (short partial sums of the FP64
+// inner products).
+__device__ __forceinline__ void dot_acc_f(float& re, float& im, float2 a, float2 b) {
+  re = fmaf(a.x, b.x, fmaf(a.y, b.y, re));
+  im = fmaf(a.x, b.y, fmaf(-a.y, b.x, im));
+}
+
 // ---------------------------------------------------------------------------
 // Preconditioner passes shared by the Krylov solvers.
 // ---------------------------------------------------------------------------

@@ -621,6 +621,7 @@ struct StnLayout {
 };
 
 #define NSR_STN_WAIT_NS 2000000000ull   // a ring wait longer than 2 s is an error
+#define NSR_STN_FLUSH 8                  // rows per float partial sum of the inner products
 
 // Items of one launch and their decoding.
 struct StnItems {
@@ -638,10 +639,12 @@ __host__ __device__ inline StnItems stn_items(int nz, int nx, int tz, int ns) {
   return it;
 }
 
-template <int W, int D, bool ADJ>
-__global__ void __launch_bounds__(W / 2 + 32, W == 512 ? 2 : 3) k_stn(SolveArgs A, int half, StnItems it, int ns) {
+template <int W, int D, int CPT, bool ADJ>
+__global__ void __launch_bounds__(W / CPT + 32, (W / CPT) >= 512 ? 1 : 3)
+    k_stn(SolveArgs A, int half, StnItems it, int ns) {
   typedef StnLayout<W> Ly;
-  constexpr int NC = W / 2;   // consumer threads
+  constexpr int NC = W / CPT;   // consumer threads, CPT adjacent columns each
+  constexpr int FLUSH = NSR_STN_FLUSH * 2 / CPT;   // rows per float partial sum
   extern __shared__ __align__(128) unsigned char ring[];
   __shared__ __align__(8) uint64_t full[D], empty[D];
   __shared__ int abort_word;
@@ -733,16 +736,19 @@ __global__ void __launch_bounds__(W / 2 + 32, W == 512 ? 2 : 3) k_stn(SolveArgs 
     const int z0 = band * it.tz, z1 = min(z0 + it.tz, nz);
     const int nrows = z1 - z0;
     const int c0 = strip * W;
-    const int j = c0 + 2 * tid;
+    const int j = c0 + CPT * tid;
     const bool own = j < nx;
-    const bool has_w = j > 0, has_e = j + 2 < nx;
+    const bool has_w = j > 0, has_e = j + CPT < nx;
     const long long soff = slot * n;
     float2* __restrict__ out = (half == 0 ? A.B.v : A.B.t) + soff;
-    const SysScalars sc = sys_scalars(g, S.freq);
+    const SysScalarsF sf = sys_scalars_f(g, sys_scalars(g, S.freq));
     const float2 sv = f2(S.c_sv);
+    // Inner products: float partial sums over NSR_STN_FLUSH rows (2 NSR_STN_FLUSH
+    // products per thread), accumulated in FP64.
     double acc[NSR_NPART];
+    float accf[NSR_NPART];
 #pragma unroll
-    for (int k = 0; k < NSR_NPART; ++k) acc[k] = 0.0;
+    for (int k = 0; k < NSR_NPART; ++k) { acc[k] = 0.0; accf[k] = 0.0f; }
     const uint32_t q0 = q;   // step of row z0 - 1
     bool ok = !abort_flag;
     // rows z0 - 1 and z0
@@ -756,43 +762,81 @@ __global__ void __launch_bounds__(W / 2 + 32, W == 512 ? 2 : 3) k_stn(SolveArgs 
         const unsigned char* bN = ring + (size_t)(sN % D) * Ly::SLOT;
         const unsigned char* bC = ring + (size_t)(sC % D) * Ly::SLOT;
         const unsigned char* bS = ring + (size_t)(sS % D) * Ly::SLOT;
-        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
         const float2 zero = make_float2(0.f, 0.f);
-        const int ez = (2 * tid + 2) * 8, ea = (2 * tid + 4) * 4;
-        const float4 zc = *reinterpret_cast<const float4*>(bC + Ly::OZ + ez);
-        const float4 zn = i > 0 ? *reinterpret_cast<const float4*>(bN + Ly::OZ + ez) : zero4;
-        const float4 zs = i + 1 < nz ? *reinterpret_cast<const float4*>(bS + Ly::OZ + ez) : zero4;
-        const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
-        const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 16) : zero;
-        const float2 ac = *reinterpret_cast<const float2*>(bC + Ly::OA + ea);
-        const float2 an = i > 0 ? *reinterpret_cast<const float2*>(bN + Ly::OA + ea) : make_float2(1.f, 1.f);
-        const float2 as = i + 1 < nz ? *reinterpret_cast<const float2*>(bS + Ly::OA + ea) : make_float2(1.f, 1.f);
-        const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
-        const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 8) : 1.0f;
-        const float2 bb = *reinterpret_cast<const float2*>(bC + Ly::OB + 8 * tid);
-        const float2 tt = *reinterpret_cast<const float2*>(bC + Ly::OT + 8 * tid);
-        const float4 rk = *reinterpret_cast<const float4*>(bC + Ly::ORH + 16 * tid);
-        const float2 c0v = lo2(zc), c1v = hi2(zc);
-        const float2 av0 = stencil_pts<ADJ>(g, sc, i, j, ac.x, ac.y, aw, as.x, an.x, bb.x, tt.x, c0v, c1v, zw,
-                                            lo2(zs), lo2(zn));
-        const float2 av1 = stencil_pts<ADJ>(g, sc, i, j + 1, ac.y, ae, ac.x, as.y, an.y, bb.y, tt.y, c1v, ze, c0v,
-                                            hi2(zs), hi2(zn));
-        *reinterpret_cast<float4*>(out + (long long)i * nx + j) = pack2(av0, av1);
-        if (half == 0) {
-          dot_acc(acc[0], acc[1], lo2(rk), av0);       // <rhat, v>
-          dot_acc(acc[0], acc[1], hi2(rk), av1);
+        if constexpr (CPT == 2) {
+          const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+          const int ez = (2 * tid + 2) * 8, ea = (2 * tid + 4) * 4;
+          const float4 zc = *reinterpret_cast<const float4*>(bC + Ly::OZ + ez);
+          const float4 zn = i > 0 ? *reinterpret_cast<const float4*>(bN + Ly::OZ + ez) : zero4;
+          const float4 zs = i + 1 < nz ? *reinterpret_cast<const float4*>(bS + Ly::OZ + ez) : zero4;
+          const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
+          const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 16) : zero;
+          const float2 ac = *reinterpret_cast<const float2*>(bC + Ly::OA + ea);
+          const float2 an = i > 0 ? *reinterpret_cast<const float2*>(bN + Ly::OA + ea) : make_float2(1.f, 1.f);
+          const float2 as = i + 1 < nz ? *reinterpret_cast<const float2*>(bS + Ly::OA + ea) : make_float2(1.f, 1.f);
+          const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
+          const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 8) : 1.0f;
+          const float2 bb = *reinterpret_cast<const float2*>(bC + Ly::OB + 8 * tid);
+          const float2 tt = *reinterpret_cast<const float2*>(bC + Ly::OT + 8 * tid);
+          const float4 rk = *reinterpret_cast<const float4*>(bC + Ly::ORH + 16 * tid);
+          const float2 c0v = lo2(zc), c1v = hi2(zc);
+          const float2 av0 = stencil_pts_f<ADJ>(g, sf, i, j, ac.x, ac.y, aw, as.x, an.x, bb.x, tt.x, c0v, c1v, zw,
+                                                lo2(zs), lo2(zn));
+          const float2 av1 = stencil_pts_f<ADJ>(g, sf, i, j + 1, ac.y, ae, ac.x, as.y, an.y, bb.y, tt.y, c1v, ze,
+                                                c0v, hi2(zs), hi2(zn));
+          *reinterpret_cast<float4*>(out + (long long)i * nx + j) = pack2(av0, av1);
+          if (half == 0) {
+            dot_acc_f(accf[0], accf[1], lo2(rk), av0);       // <rhat, v>
+            dot_acc_f(accf[0], accf[1], hi2(rk), av1);
+          } else {
+            const float4 rr = *reinterpret_cast<const float4*>(bC + Ly::OR + 16 * tid);
+            const float4 vv = *reinterpret_cast<const float4*>(bC + Ly::OV + 16 * tid);
+            const float2 s0 = lo2(rr) + sv * lo2(vv), s1 = hi2(rr) + sv * hi2(vv);
+            dot_acc_f(accf[0], accf[1], av0, s0);            // <t, s>
+            dot_acc_f(accf[0], accf[1], av1, s1);
+            accf[2] = fmaf(av0.x, av0.x, fmaf(av0.y, av0.y, fmaf(av1.x, av1.x, fmaf(av1.y, av1.y, accf[2]))));
+            accf[3] = fmaf(s0.x, s0.x, fmaf(s0.y, s0.y, fmaf(s1.x, s1.x, fmaf(s1.y, s1.y, accf[3]))));
+            dot_acc_f(accf[4], accf[5], lo2(rk), av0);       // <rhat, t>
+            dot_acc_f(accf[4], accf[5], hi2(rk), av1);
+            dot_acc_f(accf[6], accf[7], lo2(rk), s0);        // <rhat, s>
+            dot_acc_f(accf[6], accf[7], hi2(rk), s1);
+          }
         } else {
-          const float4 rr = *reinterpret_cast<const float4*>(bC + Ly::OR + 16 * tid);
-          const float4 vv = *reinterpret_cast<const float4*>(bC + Ly::OV + 16 * tid);
-          const float2 s0 = lo2(rr) + sv * lo2(vv), s1 = hi2(rr) + sv * hi2(vv);
-          dot_acc(acc[0], acc[1], av0, s0);            // <t, s>
-          dot_acc(acc[0], acc[1], av1, s1);
-          acc[2] += (double)av0.x * av0.x + (double)av0.y * av0.y + (double)av1.x * av1.x + (double)av1.y * av1.y;
-          acc[3] += (double)s0.x * s0.x + (double)s0.y * s0.y + (double)s1.x * s1.x + (double)s1.y * s1.y;
-          dot_acc(acc[4], acc[5], lo2(rk), av0);       // <rhat, t>
-          dot_acc(acc[4], acc[5], hi2(rk), av1);
-          dot_acc(acc[6], acc[7], lo2(rk), s0);        // <rhat, s>
-          dot_acc(acc[6], acc[7], hi2(rk), s1);
+          const int ez = (tid + 2) * 8, ea = (tid + 4) * 4;
+          const float2 zc = *reinterpret_cast<const float2*>(bC + Ly::OZ + ez);
+          const float2 zn = i > 0 ? *reinterpret_cast<const float2*>(bN + Ly::OZ + ez) : zero;
+          const float2 zs = i + 1 < nz ? *reinterpret_cast<const float2*>(bS + Ly::OZ + ez) : zero;
+          const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
+          const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 8) : zero;
+          const float ac = *reinterpret_cast<const float*>(bC + Ly::OA + ea);
+          const float an = i > 0 ? *reinterpret_cast<const float*>(bN + Ly::OA + ea) : 1.0f;
+          const float as = i + 1 < nz ? *reinterpret_cast<const float*>(bS + Ly::OA + ea) : 1.0f;
+          const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
+          const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 4) : 1.0f;
+          const float bb = *reinterpret_cast<const float*>(bC + Ly::OB + 4 * tid);
+          const float tt = *reinterpret_cast<const float*>(bC + Ly::OT + 4 * tid);
+          const float2 rk = *reinterpret_cast<const float2*>(bC + Ly::ORH + 8 * tid);
+          const float2 av = stencil_pts_f<ADJ>(g, sf, i, j, ac, ae, aw, as, an, bb, tt, zc, ze, zw, zs, zn);
+          out[(long long)i * nx + j] = av;
+          if (half == 0) {
+            dot_acc_f(accf[0], accf[1], rk, av);       // <rhat, v>
+          } else {
+            const float2 rr = *reinterpret_cast<const float2*>(bC + Ly::OR + 8 * tid);
+            const float2 vv = *reinterpret_cast<const float2*>(bC + Ly::OV + 8 * tid);
+            const float2 s0 = rr + sv * vv;
+            dot_acc_f(accf[0], accf[1], av, s0);       // <t, s>
+            accf[2] = fmaf(av.x, av.x, fmaf(av.y, av.y, accf[2]));
+            accf[3] = fmaf(s0.x, s0.x, fmaf(s0.y, s0.y, accf[3]));
+            dot_acc_f(accf[4], accf[5], rk, av);       // <rhat, t>
+            dot_acc_f(accf[6], accf[7], rk, s0);       // <rhat, s>
+          }
+        }
+      }
+      if ((k + 1) % FLUSH == 0 || k + 1 == nrows) {
+#pragma unroll
+        for (int qq = 0; qq < NSR_NPART; ++qq) {
+          if (half == 1 || qq < 2) acc[qq] += (double)accf[qq];
+          accf[qq] = 0.0f;
         }
       }
       // the buffer of row i - 1 is no longer needed
@@ -1049,10 +1093,12 @@ static int stn_items_max(const NsrGrid* g) {
 
 typedef void (*StnKernel)(SolveArgs, int, StnItems, int);
 
-static StnKernel stn_kernel(int w, int d, bool adj) {
-#define NSR_STN_CASE(W_, D_) \
-  if (w == W_ && d == D_) return adj ? k_stn<W_, D_, true> : k_stn<W_, D_, false>;
-  NSR_STN_CASE(256, 4) NSR_STN_CASE(256, 6) NSR_STN_CASE(256, 8) NSR_STN_CASE(512, 4) NSR_STN_CASE(512, 5)
+static StnKernel stn_kernel(int w, int d, int cpt, bool adj) {
+#define NSR_STN_CASE(W_, D_, C_) \
+  if (w == W_ && d == D_ && cpt == C_) return adj ? k_stn<W_, D_, C_, true> : k_stn<W_, D_, C_, false>;
+  NSR_STN_CASE(256, 4, 2) NSR_STN_CASE(256, 6, 2) NSR_STN_CASE(256, 8, 2) NSR_STN_CASE(512, 4, 2)
+  NSR_STN_CASE(512, 5, 2) NSR_STN_CASE(256, 4, 1) NSR_STN_CASE(256, 6, 1) NSR_STN_CASE(256, 8, 1)
+  NSR_STN_CASE(512, 4, 1)
 #undef NSR_STN_CASE
   return nullptr;
 }
@@ -1063,11 +1109,11 @@ static size_t stn_smem(int w, int d) {
 
 // Launch shapes of one call: NsrTiles with zero fields replaced by defaults.
 struct TileChoice {
-  int sw, sd, sr, sctas, tc, rows, groups;
+  int sw, sd, sr, sctas, tc, rows, groups, scpt;
 };
 
 static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileChoice* c) {
-  c->sw = 256; c->sd = 6; c->sr = 16; c->sctas = 0;
+  c->sw = 256; c->sd = 6; c->sr = 32; c->sctas = 0; c->scpt = 1;
   c->tc = nsr_cols_tc(g);
   c->rows = nsr_rows_per_cta(g);
   c->groups = n_slots >= 8 ? 2 : 1;
@@ -1079,8 +1125,9 @@ static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileC
     if (t->cols_width) c->tc = t->cols_width;
     if (t->row_tile) c->rows = t->row_tile;
     if (t->slot_groups) c->groups = t->slot_groups;
+    if (t->stencil_cols) c->scpt = t->stencil_cols;
   }
-  if (!stn_kernel(c->sw, c->sd, false)) return NSR_ERR_ARGUMENT;
+  if (!stn_kernel(c->sw, c->sd, c->scpt, false)) return NSR_ERR_ARGUMENT;
   if (c->sr < NSR_STN_MIN_ROWS || c->sr > 64 || c->sctas < 0 || c->sctas > 8) return NSR_ERR_ARGUMENT;
   if (!(c->tc == 8 || c->tc == 16) || (size_t)g->nz * c->tc * sizeof(float2) > 200 * 1024) return NSR_ERR_ARGUMENT;
   if (c->rows < 1 || c->rows > 8 || sizeof(float2) * (size_t)c->rows * nsr_row_stride(g->nx) > 200 * 1024)
@@ -1252,7 +1299,8 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     const int nb_st = stencil_ctas(grid);
     const bool pairs = grid->nx % 2 == 0;
     const bool use_stn = stn_ok(grid);
-    const StnKernel stn_fn = stn_kernel(T.sw, T.sd, A.adjoint != 0);
+    const StnKernel stn_fn = stn_kernel(T.sw, T.sd, T.scpt, A.adjoint != 0);
+    const int stn_threads = T.sw / T.scpt + 32;
     const size_t stn_sm = stn_smem(T.sw, T.sd);
     int stn_per_sm = T.sctas;
     int n_sms = 1;
@@ -1264,7 +1312,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     if (use_stn) {
       NSR_TRY(cudaFuncSetAttribute((const void*)stn_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stn_sm));
       if (stn_per_sm <= 0) {
-        NSR_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&stn_per_sm, (const void*)stn_fn, T.sw / 2 + 32,
+        NSR_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&stn_per_sm, (const void*)stn_fn, stn_threads,
                                                               stn_sm));
         if (stn_per_sm < 1) { err = NSR_ERR_ARGUMENT; goto cleanup; }
       }
@@ -1326,7 +1374,7 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
         int hv = half, nsv = ns;
         const int gx = si.n_items < stn_per_sm * n_sms ? si.n_items : stn_per_sm * n_sms;
         void* args[] = {&Ag, &hv, &si, &nsv};
-        cudaLaunchKernel((const void*)stn_fn, dim3(gx), dim3(T.sw / 2 + 32), args, stn_sm, sq);
+        cudaLaunchKernel((const void*)stn_fn, dim3(gx), dim3(stn_threads), args, stn_sm, sq);
       } else if (which == 3) {
         if (pairs) {
           if (A.adjoint) k_inv<true><<<g_inv, 256, 0, sq>>>(Ag, half);
