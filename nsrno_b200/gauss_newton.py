@@ -16,6 +16,12 @@ The reference's only tangent is time-domain (nsrno/native_tangent.cu:53-79);
 the frequency-domain one reuses the batched solver with a tangent right-hand
 side.  All fields of a step stay resident on the device (c64 background and
 adjoint fields: 8 bytes per node and system).
+
+On several GPUs (one process per GPU, ``distributed=True``) every rank holds
+the systems of its own frequency bins; the misfit, the gradient and the
+Hessian-vector product are sums over systems, so each is one all-reduce
+(the gradient all-reduce of the reference's DDP inversion,
+nsrno/reconstruct_dense.py:53,97-106), and every rank then takes the same step.
 """
 from __future__ import annotations
 
@@ -71,6 +77,8 @@ class GaussNewton:
     tolerance: float = 1e-6
     n_slots: int = 22
     max_iterations: int = 6000
+    distributed: bool = False         # sum misfit, gradient and H v over the ranks of `group`
+    group: object = None              # torch.distributed process group (None: the default group)
     timings: dict = field(default_factory=dict)
 
     def __post_init__(self):
@@ -132,20 +140,41 @@ class GaussNewton:
         mu = self._solve("adjoint2", rhs=self._receiver_rhs(jv), adjoint=True).fields
         return grad_accum(self.medium, self.f_dev, self.u, mu), jv
 
+    def _sum_planes(self, a, b):
+        """(a, b) summed over the ranks: one all-reduce of the stacked planes."""
+        if not self.distributed:
+            return a, b
+        from .shard import allreduce_gradient
+        t0 = time.perf_counter()
+        both = allreduce_gradient(torch.stack((a, b)).contiguous(), group=self.group)
+        self.timings["allreduce"] = self.timings.get("allreduce", 0.0) + time.perf_counter() - t0
+        return both[0], both[1]
+
+    def _sum_scalar(self, x, like):
+        if not self.distributed:
+            return float(x)
+        import torch.distributed as dist
+        t = torch.tensor([float(x)], dtype=torch.float64, device=like.device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+        return float(t)
+
     def step(self):
         """One step along the steepest-descent direction with the exact Gauss-Newton length."""
         self.timings = {}
         t0 = time.perf_counter()
         misfit = self.forward()
-        gc, gr = self.gradient()
+        gc, gr = self._sum_planes(*self.gradient())
+        misfit = self._sum_scalar(misfit, gc)
         gnorm = float(torch.sqrt((gc ** 2).sum() + (gr ** 2).sum()))
         vc, vr = -gc / gnorm, -gr / gnorm
         (hc, hr), jv = self.hessian_vector(vc, vr)
+        hc, hr = self._sum_planes(hc, hr)
         gv = float((gc * vc).sum() + (gr * vr).sum())
         vhv = float((vc * hc).sum() + (vr * hr).sum())
         alpha = -gv / vhv
+        jv2 = self._sum_scalar((jv.abs() ** 2).sum(), gc)
         total = time.perf_counter() - t0
-        return dict(misfit=misfit, gradient_norm=gnorm, vHv=vhv, jv_norm2=float((jv.abs() ** 2).sum()),
+        return dict(misfit=misfit, gradient_norm=gnorm, vHv=vhv, jv_norm2=jv2,
                     alpha=alpha, predicted_decrease=0.5 * gv * gv / vhv, seconds=total,
                     phase_seconds=dict(self.timings), update=(alpha * vc, alpha * vr))
 
@@ -164,9 +193,22 @@ def main():
     ap.add_argument("--slots", type=int, default=22)
     ap.add_argument("--fixed", action="store_true", help="fixed shifted-Laplace preconditioner")
     a = ap.parse_args()
+    import os
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        # one process per GPU (torchrun); each rank solves its own bins
+        import datetime
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     dev = torch.device("cuda")
     all_bins = breast_bins()
     pick = np.unique(np.linspace(0, len(all_bins) - 1, a.bins).round().astype(int))
+    if world > 1:
+        from .shard import partition_bins
+        pick = pick[partition_bins(all_bins[pick], world)[rank]]
     rec = breast_record(nz=a.nz, nx=a.nx, h=a.h, n_pml=int(round(1.2e-3 / a.h)), bins=all_bins[pick],
                         n_angles=a.angles, rx_pitch=max(1, int(round(2e-4 / a.h))))
     true = perturbed(rec, seed=3)
@@ -181,7 +223,7 @@ def main():
     del setup
     t_obs = time.perf_counter() - t0
     med = Medium(geo, rec.c, rec.rho, rec.alpha, device=dev)
-    gn = GaussNewton(med, f, th, obs.iq, preconditioner=pre, n_slots=a.slots)
+    gn = GaussNewton(med, f, th, obs.iq, preconditioner=pre, n_slots=a.slots, distributed=world > 1)
     torch.cuda.reset_peak_memory_stats()
     out = gn.step()
     out.pop("update")
@@ -200,8 +242,12 @@ def main():
                solves_per_step=4 * len(f), solves_per_second=4 * len(f) / out["seconds"],
                forward_iterations_mean=float(fw.iterations.float().mean()),
                forward_residual_max=float(fw.residual.max()),
-               peak_device_gb=torch.cuda.max_memory_allocated() / 1e9)
-    print(json.dumps(out))
+               peak_device_gb=torch.cuda.max_memory_allocated() / 1e9, ranks=world)
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
