@@ -385,6 +385,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     from nsrno_b200 import Geometry, Medium, Workspace, _lib, solve_batched, tune
+    from nsrno_b200.solver import solve_progress
     from nsrno_b200.learned import LearnedPreconditioner
     from nsrno_b200.media import breast_record
 
@@ -483,7 +484,7 @@ def run_ours(args):
         return dict(value=solves / (ms_max / 1e3), ms_per_step=ms_max / max(1, args.steps), kms=kms, alg=alg,
                     dominant=dominant, achieved=alg[dominant] / (kms[dominant] / 1e3) / 1e9,
                     iteration_achieved=sum(alg.values()) / (iter_ms / 1e3) / 1e9,
-                    launches=int(sum(r.extra["stats"]["launches"] for r in results)),
+                    launches=int(sum(solve_progress(r)[3] for r in results)),
                     solves={"total": int(len(status)), "converged": int((status == _lib.CONVERGED).sum()),
                             "iterations_mean": float(iters.mean()), "iterations_max": int(iters.max()),
                             "residual_max": float(resid.max())})

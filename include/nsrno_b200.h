@@ -9,7 +9,8 @@
  *     complex values are interleaved (re, im) pairs: "c64" = 2 x float,
  *     "c128" = 2 x double;
  *   - work runs on the caller's stream (a cudaStream_t passed as void*);
- *     only nsr_solve_batched synchronises (it polls a completion counter);
+ *     entry points do not synchronise it, except the *_sync variants, the
+ *     dense solve (one small read per restart cycle) and the queries that say so;
  *   - no exceptions cross the ABI; nothing here allocates device memory
  *     except where stated (nsr_solve_batched takes a caller workspace sized by
  *     nsr_solve_workspace_size).
@@ -229,7 +230,22 @@ int nsr_plane_wave_rhs(const NsrGrid* grid, const double* freq_hz, const double*
  * residual, FP64), iterations i32 [S], status i32 [S] (NSR_CONVERGED ...),
  * fields NULL or [S][nz][nx] (c64, or c128 when params->fields_fp64);
  * stats NULL or a host NsrSolveStats.
- * The call synchronises its stream while it polls for completion. */
+ *
+ * nsr_solve_batched does not block: it enqueues the whole solve on the
+ * caller's stream and returns.  The iteration loop runs on the device, as a
+ * CUDA graph whose conditional WHILE node repeats graph_iterations
+ * iterations until every system has finished (or a round budget derived
+ * from max_iterations is spent; systems never finished keep NSR_NOT_RUN).
+ * Inputs, outputs and the workspace must stay valid until the stream passes
+ * the solve.  stats (if given) gets only what is known at enqueue time;
+ * profile_iterations must be 0.  A kernel that gives up on its copy ring
+ * ends the loop; nsr_solve_progress reports it.
+ *
+ * nsr_solve_batched_sync runs the same solve with a host-driven loop: it
+ * relaunches the captured iterations and polls a completion counter, fills
+ * every field of stats (device loop time, per-kernel event timings of the
+ * first profile_iterations iterations), returns NSR_ERR_TIMEOUT for a
+ * kernel that gave up, and returns once the solve has finished. */
 size_t nsr_solve_workspace_size(const NsrGrid* grid, int32_t n_slots);
 int nsr_solve_batched(const NsrGrid* grid, const void* material,
                       const double* freq_hz, const double* angle_rad, int32_t n_systems,
@@ -239,6 +255,25 @@ int nsr_solve_batched(const NsrGrid* grid, const void* material,
                       void* workspace, size_t workspace_bytes,
                       double* iq, double* residual, int32_t* iterations, int32_t* status,
                       void* fields, NsrSolveStats* stats, void* stream);
+int nsr_solve_batched_sync(const NsrGrid* grid, const void* material,
+                           const double* freq_hz, const double* angle_rad, int32_t n_systems,
+                           const float* rhs, const float* x0,
+                           const int32_t* rx_index, int32_t n_rx,
+                           const NsrSolveParams* params,
+                           void* workspace, size_t workspace_bytes,
+                           double* iq, double* residual, int32_t* iterations, int32_t* status,
+                           void* fields, NsrSolveStats* stats, void* stream);
+
+/* Progress of the last solve in `workspace` (n_slots as given to it): systems
+ * finished, device loop rounds run, and 1 if a kernel gave up on its copy
+ * ring.  Synchronises `stream` (reads a few words). */
+int nsr_solve_progress(const NsrGrid* grid, int32_t n_slots, const void* workspace, int32_t* done,
+                       int64_t* rounds, int32_t* error, void* stream);
+/* Byte offset in the workspace of the progress record read by
+ * nsr_solve_progress: int32 words [1] systems finished, [4] error, and the
+ * int64 at word 6 the device loop rounds; a caller may copy these 32 bytes
+ * asynchronously after a non-blocking solve.  0 for invalid arguments. */
+size_t nsr_solve_progress_offset(const NsrGrid* grid, int32_t n_slots);
 
 /* Parameters of nsr_gmres_batched. */
 typedef struct NsrGmresParams {

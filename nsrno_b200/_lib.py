@@ -18,7 +18,9 @@ ERR_TIMEOUT = 1006
 
 EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_material", "nsr_apply",
            "nsr_precondition_workspace_size", "nsr_precondition", "nsr_precondition_noalloc", "nsr_plane_wave_rhs",
-           "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_gmres_workspace_size", "nsr_gmres_batched",
+           "nsr_solve_workspace_size", "nsr_solve_batched", "nsr_solve_batched_sync", "nsr_solve_progress",
+           "nsr_solve_progress_offset",
+           "nsr_gmres_workspace_size", "nsr_gmres_batched",
            "nsr_grad_accum", "nsr_dense_coef_bytes", "nsr_dense_workspace_size", "nsr_dense_apply",
            "nsr_learned_state_bytes", "nsr_learned_setup", "nsr_learned_precondition",
            "nsr_learned_backward_workspace_size", "nsr_learned_map_backward", "nsr_learned_network_backward",
@@ -133,6 +135,11 @@ def load():
     lib.nsr_solve_workspace_size.argtypes = [G, I]
     lib.nsr_solve_batched.argtypes = [G, P, P, P, I, P, P, P, I, ctypes.POINTER(NsrSolveParams),
                                       P, S, P, P, P, P, P, ctypes.POINTER(NsrSolveStats), P]
+    lib.nsr_solve_batched_sync.argtypes = lib.nsr_solve_batched.argtypes
+    lib.nsr_solve_progress.argtypes = [G, I, P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(ctypes.c_int32), P]
+    lib.nsr_solve_progress_offset.restype = S
+    lib.nsr_solve_progress_offset.argtypes = [G, I]
     lib.nsr_grad_accum.argtypes = [G, P, P, I, I, P, P, P, P, P]
     lib.nsr_tangent_rhs.argtypes = [G, P, P, I, I, P, P, P, P, P]
     lib.nsr_band_rf.argtypes = [I, I, I, P, P, P, P]

@@ -1068,7 +1068,22 @@ __global__ void k_solve_init(SolveArgs A, int n_slots) {
     A.B.warm[0] = 0;
     A.B.warm[1] = 0;
     *A.B.error = 0;
+    *reinterpret_cast<unsigned long long*>(A.B.queue + 6) = 0ull;   // device-loop rounds
   }
+}
+
+// Last node of the device-side solve loop (the body of a conditional WHILE
+// graph node): ends the loop once every system has finished, a kernel has
+// reported an error, or the round budget (an upper bound on the rounds a full
+// queue can need) is spent.
+__global__ void k_loop_control(SolveArgs A, cudaGraphConditionalHandle loop, long long max_rounds) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long* rounds = reinterpret_cast<unsigned long long*>(A.B.queue + 6);
+  const unsigned long long r = *rounds + 1;
+  *rounds = r;
+  const int done = *(volatile int*)A.B.done;
+  const int error = *(volatile int*)A.B.error;
+  if (done >= A.n_systems || error || r >= (unsigned long long)max_rounds) cudaGraphSetConditional(loop, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1185,14 +1200,11 @@ static int* pinned_counter() {
   return p;
 }
 
-extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
-                                 const double* freq_hz, const double* angle_rad, int32_t n_systems,
-                                 const float* rhs, const float* x0,
-                                 const int32_t* rx_index, int32_t n_rx,
-                                 const NsrSolveParams* params,
-                                 void* workspace, size_t workspace_bytes,
-                                 double* iq, double* residual, int32_t* iterations, int32_t* status,
-                                 void* fields, NsrSolveStats* stats, void* stream) {
+static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_hz, const double* angle_rad,
+                      int32_t n_systems, const float* rhs, const float* x0, const int32_t* rx_index, int32_t n_rx,
+                      const NsrSolveParams* params, void* workspace, size_t workspace_bytes, double* iq,
+                      double* residual, int32_t* iterations, int32_t* status, void* fields, NsrSolveStats* stats,
+                      void* stream, bool blocking) {
   int err = nsr_check_grid(grid, true);
   if (err) return err;
   if (!params || !coef || n_systems < 0 || n_rx < 0) return NSR_ERR_ARGUMENT;
@@ -1226,8 +1238,10 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
   long long launches = 0;
   int graph_launches = 0;
   if (stats) memset(stats, 0, sizeof(*stats));
-  int* host = pinned_counter();
-  if (!host) return (int)cudaErrorMemoryAllocation;
+  if (!blocking && params->profile_iterations > 0) return NSR_ERR_ARGUMENT;   // event timings need the host
+  int* host = blocking ? pinned_counter() : nullptr;
+  if (blocking && !host) return (int)cudaErrorMemoryAllocation;
+  cudaGraph_t loop_graph = nullptr;
   cudaError_t ce;
 #define NSR_TRY(x) do { ce = (x); if (ce != cudaSuccess) { err = (int)ce; goto cleanup; } } while (0)
   {
@@ -1419,29 +1433,75 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
       launches += (long long)NSR_LAUNCHES_PER_IT * P * n_groups;
     }
 
-    NSR_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    if (n_groups == 2) {
-      NSR_TRY(cudaEventRecord(ev_fork, st));
-      NSR_TRY(cudaStreamWaitEvent(st2, ev_fork, 0));
-    }
-    for (int it = 0; it < K; ++it)
-      for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) {
-        launch(q, 0, st);
-        if (n_groups == 2) launch(q, 1, st2);
-      }
-    if (n_groups == 2) {
-      NSR_TRY(cudaEventRecord(ev_join, st2));
-      NSR_TRY(cudaStreamWaitEvent(st, ev_join, 0));
-    }
-    ce = cudaStreamEndCapture(st, &graph);
-    if (ce != cudaSuccess) { err = (int)ce; goto cleanup; }
-    NSR_TRY(cudaGraphInstantiate(&exec, graph, 0));
-
     // Each system needs at most max_it iterations plus its replacement,
-    // init and emit half-iterations; bound the number of graph launches.
+    // init and emit half-iterations; bound the number of graph rounds.
     const long long per_sys = (long long)params->max_iterations * 2 + 16;
     const long long waves = (n_systems + n_slots - 1) / n_slots + 1;
     const long long max_launch = waves * ((per_sys + K - 1) / K) + 4;
+    // The K iterations of one round, captured from both slot-group streams.
+    auto capture_round = [&]() -> cudaError_t {
+      cudaError_t e = cudaSuccess;
+      if (n_groups == 2) {
+        if ((e = cudaEventRecord(ev_fork, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st2, ev_fork, 0)) != cudaSuccess) return e;
+      }
+      for (int it = 0; it < K; ++it)
+        for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) {
+          launch(q, 0, st);
+          if (n_groups == 2) launch(q, 1, st2);
+        }
+      if (n_groups == 2) {
+        if ((e = cudaEventRecord(ev_join, st2)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st, ev_join, 0)) != cudaSuccess) return e;
+      }
+      return cudaGetLastError();
+    };
+
+    if (!blocking) {
+      // Device-side loop: a conditional WHILE node whose body is one round
+      // followed by k_loop_control, so the whole solve is one graph launch
+      // on the stream and the host returns at once.
+      cudaGraphConditionalHandle handle;
+      NSR_TRY(cudaGraphCreate(&loop_graph, 0));
+      NSR_TRY(cudaGraphConditionalHandleCreate(&handle, loop_graph, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+      cp.conditional.handle = handle;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t while_node;
+      NSR_TRY(cudaGraphAddNode(&while_node, loop_graph, nullptr, 0, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      NSR_TRY(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      ce = capture_round();
+      if (ce == cudaSuccess) {
+        k_loop_control<<<1, 32, 0, st>>>(A, handle, max_launch);
+        ce = cudaGetLastError();
+      }
+      cudaGraph_t captured = nullptr;
+      const cudaError_t ce2 = cudaStreamEndCapture(st, &captured);
+      if (ce == cudaSuccess) ce = ce2;
+      if (ce != cudaSuccess) { err = (int)ce; goto cleanup; }
+      NSR_TRY(cudaGraphInstantiate(&exec, loop_graph, 0));
+      NSR_TRY(cudaGraphLaunch(exec, st));
+      graph_launches = 1;   // the rounds it runs are in the progress record
+      if (stats) {
+        stats->launches = launches;
+        stats->graph_launches = graph_launches;
+      }
+      NSR_TRY(cudaEventRecord(ev_out, st));
+      NSR_TRY(cudaStreamWaitEvent(caller, ev_out, 0));
+      goto cleanup;
+    }
+
+    NSR_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    ce = capture_round();
+    {
+      const cudaError_t ce2 = cudaStreamEndCapture(st, &graph);
+      if (ce == cudaSuccess) ce = ce2;
+    }
+    if (ce != cudaSuccess) { err = (int)ce; goto cleanup; }
+    NSR_TRY(cudaGraphInstantiate(&exec, graph, 0));
+
     long long launched = 0;
     bool drained = false, failed = false;
     int pending = -1;
@@ -1497,10 +1557,15 @@ extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef,
     NSR_TRY(cudaStreamWaitEvent(caller, ev_out, 0));
   }
 cleanup:
-  if (st) cudaStreamSynchronize(st);
-  if (st2) cudaStreamSynchronize(st2);
+  // A non-blocking call that enqueued its loop leaves the work in flight:
+  // graph, streams and events are then released by CUDA once it completes.
+  if (blocking || err) {
+    if (st) cudaStreamSynchronize(st);
+    if (st2) cudaStreamSynchronize(st2);
+  }
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
+  if (loop_graph) cudaGraphDestroy(loop_graph);
   if (ev_in) cudaEventDestroy(ev_in);
   if (ev_out) cudaEventDestroy(ev_out);
   if (ev_poll[0]) cudaEventDestroy(ev_poll[0]);
@@ -1518,4 +1583,47 @@ cleanup:
   if (ev_join) cudaEventDestroy(ev_join);
 #undef NSR_TRY
   return err;
+}
+
+extern "C" int nsr_solve_batched(const NsrGrid* grid, const void* coef, const double* freq_hz,
+                                 const double* angle_rad, int32_t n_systems, const float* rhs, const float* x0,
+                                 const int32_t* rx_index, int32_t n_rx, const NsrSolveParams* params,
+                                 void* workspace, size_t workspace_bytes, double* iq, double* residual,
+                                 int32_t* iterations, int32_t* status, void* fields, NsrSolveStats* stats,
+                                 void* stream) {
+  return solve_impl(grid, coef, freq_hz, angle_rad, n_systems, rhs, x0, rx_index, n_rx, params, workspace,
+                    workspace_bytes, iq, residual, iterations, status, fields, stats, stream, false);
+}
+
+extern "C" int nsr_solve_batched_sync(const NsrGrid* grid, const void* coef, const double* freq_hz,
+                                      const double* angle_rad, int32_t n_systems, const float* rhs,
+                                      const float* x0, const int32_t* rx_index, int32_t n_rx,
+                                      const NsrSolveParams* params, void* workspace, size_t workspace_bytes,
+                                      double* iq, double* residual, int32_t* iterations, int32_t* status,
+                                      void* fields, NsrSolveStats* stats, void* stream) {
+  return solve_impl(grid, coef, freq_hz, angle_rad, n_systems, rhs, x0, rx_index, n_rx, params, workspace,
+                    workspace_bytes, iq, residual, iterations, status, fields, stats, stream, true);
+}
+
+extern "C" size_t nsr_solve_progress_offset(const NsrGrid* grid, int32_t n_slots) {
+  if (nsr_check_grid(grid, true) || n_slots <= 0 || n_slots > 65535) return 0;
+  return layout(grid, n_slots).queue;
+}
+
+extern "C" int nsr_solve_progress(const NsrGrid* grid, int32_t n_slots, const void* workspace, int32_t* done,
+                                  int64_t* rounds, int32_t* error, void* stream) {
+  if (nsr_check_grid(grid, true) || n_slots <= 0 || n_slots > 65535 || !workspace) return NSR_ERR_ARGUMENT;
+  const Layout L = layout(grid, n_slots);
+  int words[8];
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t ce = cudaMemcpyAsync(words, (const char*)workspace + L.queue, sizeof(words), cudaMemcpyDeviceToHost,
+                                   st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  if (ce != cudaSuccess) return (int)ce;
+  unsigned long long r;
+  memcpy(&r, &words[6], sizeof(r));
+  if (done) *done = words[1];
+  if (rounds) *rounds = (int64_t)r;
+  if (error) *error = words[4];
+  return 0;
 }

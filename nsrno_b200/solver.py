@@ -147,7 +147,7 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
                   max_iterations=2000, shift=DEFAULT_SHIFT, replace_every=DEFAULT_REPLACE, n_slots=16,
                   adjoint=False, return_fields=False, rx_index=None, graph_iterations=16,
                   profile_iterations=0, restart_factor=DEFAULT_RESTART, warm_gate=1.0, fields_dtype=torch.complex64,
-                  learned=None, gain_index=None, time_limit=0.0, tiles=None,
+                  learned=None, gain_index=None, time_limit=0.0, tiles=None, blocking=None,
                   workspace: Workspace | None = None, out: BatchResult | None = None) -> BatchResult:
     """Solve every (frequency, angle) system of a record with batched BiCGSTAB.
 
@@ -160,7 +160,12 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
     0: none) bounds each system's solve on the device: a system still running
     then stops at its next true residual with reason ``"timeout"``.
     ``tiles`` (a dict of :class:`nsrno_b200._lib.NsrTiles` fields, e.g. from
-    :func:`nsrno_b200.tune.tuned_tiles`) overrides the launch shapes.
+    :func:`nsrno_b200.tune.tuned_config`) overrides the launch shapes.
+    ``blocking`` (default: only when ``profile_iterations`` > 0) selects the
+    host-polled ``nsr_solve_batched_sync``, which also reports the device loop
+    time and per-kernel timings in ``extra["stats"]``; otherwise the solve is
+    one device-side graph loop enqueued on the current stream
+    (``nsr_solve_batched``) and this call returns before it finishes.
     """
     lib = _lib.load()
     g = medium.geometry
@@ -216,15 +221,40 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
     if tiles_struct is not None:
         params.tiles = ctypes.pointer(tiles_struct)
     stats = _lib.NsrSolveStats()
-    _lib.check(lib.nsr_solve_batched(
+    if blocking is None:
+        blocking = profile_iterations > 0
+    entry = lib.nsr_solve_batched_sync if blocking else lib.nsr_solve_batched
+    _lib.check(entry(
         ctypes.byref(grid), _ptr(medium.material), _ptr(freqs), _ptr(angles), S,
         _ptr(rhs), _ptr(x0), _ptr(rx_index), n_rx, ctypes.byref(params),
         _ptr(ws), ws.numel(), _ptr(out.iq), _ptr(out.residual), _ptr(out.iterations), _ptr(out.status),
         _ptr(out.fields), ctypes.byref(stats), _stream()))
     del keep, tiles_struct
     out.extra["stats"] = stats.as_dict()
+    out.extra["blocking"] = bool(blocking)
     out.extra["n_slots"] = n_slots
+    if not blocking:
+        out.extra["stats"]["loop_ms"] = None
+        # the progress record (finished systems, device loop rounds, error),
+        # copied to pinned memory behind the solve; read it after a sync
+        off = lib.nsr_solve_progress_offset(ctypes.byref(grid), n_slots)
+        words = torch.empty(8, dtype=torch.int32, pin_memory=True)
+        words.copy_(ws[off:off + 32].view(torch.int32), non_blocking=True)
+        groups = int((tiles or {}).get("slot_groups", 0)) or (2 if n_slots >= 8 else 1)
+        per_round = 9 * int(graph_iterations) * (groups if n_slots >= 2 else 1) + 1
+        out.extra["progress_words"] = words
+        out.extra["launches_per_round"] = per_round
     return out
+
+
+def solve_progress(result: BatchResult):
+    """(systems finished, device loop rounds, error flag, kernels launched) of a
+    non-blocking solve, from the progress record copied behind it (call after
+    the stream has passed the solve, e.g. after torch.cuda.synchronize())."""
+    w = result.extra["progress_words"]
+    rounds = int(w[6:8].view(torch.int64)[0])
+    launches = result.extra["stats"]["launches"] + rounds * result.extra["launches_per_round"]
+    return int(w[1]), rounds, int(w[4]), launches
 
 
 def _tiles_struct(tiles):

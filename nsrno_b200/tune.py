@@ -99,7 +99,7 @@ def measure_iteration(medium, freqs, angles, config, learned=None, n_slots=22, i
     try:
         r = solve_batched(medium, freqs, angles, tolerance=1e-30, max_iterations=iterations, n_slots=n_slots,
                           graph_iterations=graph_iterations, learned=learned, tiles=tiles,
-                          shift=DEFAULT_SHIFT if shift is None else shift)
+                          shift=DEFAULT_SHIFT if shift is None else shift, blocking=True)
     except (RuntimeError, ValueError):
         return None
     torch.cuda.synchronize()

@@ -168,11 +168,11 @@ def test_warm_start_gate_discards_bad_initial_fields(cuda):
     cold = solve_batched(med, f[:3], th[:3], tolerance=1e-6)
     rng = np.random.default_rng(4)
     noise = torch.as_tensor((rng.standard_normal((3, rec.nz, rec.nx)) * 1e3).astype(np.complex64), device=cuda)
-    bad = solve_batched(med, f[:3], th[:3], tolerance=1e-6, x0=noise)
+    bad = solve_batched(med, f[:3], th[:3], tolerance=1e-6, x0=noise, blocking=True)
     assert bad.extra["stats"]["warm_rejected"] == 3 and bad.extra["stats"]["warm_accepted"] == 0
     assert torch.equal(bad.iterations, cold.iterations)
     assert torch.equal(bad.iq, cold.iq)
-    ok = solve_batched(med, f[:3], th[:3], tolerance=1e-6, x0=noise, warm_gate=0.0)
+    ok = solve_batched(med, f[:3], th[:3], tolerance=1e-6, x0=noise, warm_gate=0.0, blocking=True)
     assert ok.extra["stats"]["warm_accepted"] == 3 and ok.reasons() == ["converged"] * 3
 
 
@@ -312,3 +312,26 @@ def test_grid_with_prime_factors_matches_lu(cuda):
         for s in range(2):
             ref = H.solve_lu(A, H.plane_wave_rhs(spec, f[s], th[s]))
             assert rel(res.fields[s].cpu().numpy().ravel(), ref) < 1e-5
+
+
+def test_device_loop_equals_host_loop(cuda):
+    """The non-blocking solve (one graph launch whose conditional WHILE node
+    repeats the iterations until the queue is empty) gives bitwise the results
+    of the host-polled loop, and its progress record accounts for every system."""
+    from nsrno_b200 import solve_batched
+    from nsrno_b200.solver import solve_progress
+    rec, med = blob_case(cuda)
+    f, th = rec.systems()
+    host = solve_batched(med, f, th, tolerance=1e-7, n_slots=4, blocking=True)
+    dev = solve_batched(med, f, th, tolerance=1e-7, n_slots=4, blocking=False)
+    torch.cuda.synchronize()
+    assert not dev.extra["blocking"] and host.extra["blocking"]
+    assert torch.equal(dev.iq, host.iq) and torch.equal(dev.iterations, host.iterations)
+    assert torch.equal(dev.status, host.status) and torch.equal(dev.residual, host.residual)
+    done, rounds, error, launches = solve_progress(dev)
+    assert done == len(f) and error == 0 and rounds >= 1
+    assert launches == 3 + rounds * dev.extra["launches_per_round"]
+    # a budget-limited solve still ends: the round budget bounds the device loop
+    cut = solve_batched(med, f[:2], th[:2], tolerance=1e-12, max_iterations=5)
+    torch.cuda.synchronize()
+    assert cut.reasons() == ["iteration_budget"] * 2
