@@ -47,6 +47,7 @@ struct __align__(16) SlotState {
   unsigned long long t_start;   // global timer (ns) when the system started
   double bnorm2, rnorm2, resid, r0norm2;
   double freq, angle;
+  float kh2f, sigf, fpowf, pad_f;   // per-system stencil scalars in float (set when the slot starts)
   double2 rho, alpha, omega, beta;
   // s = r + c_sv v ; r_new = s + c_rt t ; y += c_yp p + c_ys s ; p_new = r_new + c_pp p + c_pv v
   double2 c_sv, c_rt, c_yp, c_ys, c_pp, c_pv;
@@ -258,6 +259,13 @@ __global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
   }
 }
 
+__device__ __forceinline__ void set_float_scalars(const Geo& g, SlotState& S) {
+  const SysScalars sc = sys_scalars(g, S.freq);
+  S.kh2f = (float)sc.kh2;
+  S.sigf = (float)sc.sig;
+  S.fpowf = (float)sc.fpow;
+}
+
 __device__ void pop_next(const SolveArgs& A, SlotState& S) {
   const int nxt = atomicAdd(A.B.queue, 1);
   if (nxt < A.n_systems) {
@@ -267,6 +275,7 @@ __device__ void pop_next(const SolveArgs& A, SlotState& S) {
     S.gidx = A.gain_index ? A.gain_index[nxt] : nxt;
     S.freq = A.freq[nxt];
     S.angle = A.angle ? A.angle[nxt] : 0.0;
+    set_float_scalars(A.g, S);
   } else {
     S.sys = -1;
     S.mode = MODE_EMPTY;
@@ -639,8 +648,17 @@ __host__ __device__ inline StnItems stn_items(int nz, int nx, int tz, int ns) {
   return it;
 }
 
+// Resident CTAs per SM that the shared-memory ring of a k_stn shape allows
+// (at most 4): its register budget follows from it.
+template <int W, int D, int CPT>
+__host__ __device__ constexpr int stn_min_blocks() {
+  constexpr int by_smem = (227 * 1024) / (D * StnLayout<W>::SLOT + 2048);
+  constexpr int cap = (W / CPT + 32) > 256 ? 2 : 4;
+  return by_smem < 1 ? 1 : (by_smem > cap ? cap : by_smem);
+}
+
 template <int W, int D, int CPT, bool ADJ>
-__global__ void __launch_bounds__(W / CPT + 32, (W / CPT) >= 512 ? 1 : 3)
+__global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
     k_stn(SolveArgs A, int half, StnItems it, int ns) {
   typedef StnLayout<W> Ly;
   constexpr int NC = W / CPT;   // consumer threads, CPT adjacent columns each
@@ -741,7 +759,14 @@ __global__ void __launch_bounds__(W / CPT + 32, (W / CPT) >= 512 ? 1 : 3)
     const bool has_w = j > 0, has_e = j + CPT < nx;
     const long long soff = slot * n;
     float2* __restrict__ out = (half == 0 ? A.B.v : A.B.t) + soff;
-    const SysScalarsF sf = sys_scalars_f(g, sys_scalars(g, S.freq));
+    SysScalarsF sf;
+    sf.kh2 = S.kh2f;
+    sf.sig = S.sigf;
+    sf.fpow = S.fpowf;
+    sf.inv_npml = g.n_pml > 0 ? 1.0f / (float)g.n_pml : 0.0f;
+    sf.lo = g.n_pml;
+    sf.hi_z = nz - 1 - g.n_pml;
+    sf.hi_x = nx - 1 - g.n_pml;
     const float2 sv = f2(S.c_sv);
     // Inner products: float partial sums over NSR_STN_FLUSH rows (2 NSR_STN_FLUSH
     // products per thread), accumulated in FP64.
@@ -1055,6 +1080,7 @@ __global__ void k_solve_init(SolveArgs A, int n_slots) {
       st.gidx = A.gain_index ? A.gain_index[s] : s;
       st.freq = A.freq[s];
       st.angle = A.angle ? A.angle[s] : 0.0;
+      set_float_scalars(A.g, st);
     } else {
       st.sys = -1;
       st.mode = MODE_EMPTY;
@@ -1111,9 +1137,8 @@ typedef void (*StnKernel)(SolveArgs, int, StnItems, int);
 static StnKernel stn_kernel(int w, int d, int cpt, bool adj) {
 #define NSR_STN_CASE(W_, D_, C_) \
   if (w == W_ && d == D_ && cpt == C_) return adj ? k_stn<W_, D_, C_, true> : k_stn<W_, D_, C_, false>;
-  NSR_STN_CASE(256, 4, 2) NSR_STN_CASE(256, 6, 2) NSR_STN_CASE(256, 8, 2) NSR_STN_CASE(512, 4, 2)
-  NSR_STN_CASE(512, 5, 2) NSR_STN_CASE(256, 4, 1) NSR_STN_CASE(256, 6, 1) NSR_STN_CASE(256, 8, 1)
-  NSR_STN_CASE(512, 4, 1)
+  NSR_STN_CASE(256, 4, 2) NSR_STN_CASE(256, 5, 2) NSR_STN_CASE(256, 6, 2) NSR_STN_CASE(256, 8, 2)
+  NSR_STN_CASE(512, 4, 2) NSR_STN_CASE(512, 5, 2) NSR_STN_CASE(256, 4, 1) NSR_STN_CASE(256, 6, 1)
 #undef NSR_STN_CASE
   return nullptr;
 }
@@ -1128,7 +1153,7 @@ struct TileChoice {
 };
 
 static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileChoice* c) {
-  c->sw = 256; c->sd = 6; c->sr = 32; c->sctas = 0; c->scpt = 1;
+  c->sw = 256; c->sd = 4; c->sr = 32; c->sctas = 0; c->scpt = 2;
   c->tc = nsr_cols_tc(g);
   c->rows = nsr_rows_per_cta(g);
   c->groups = n_slots >= 8 ? 2 : 1;

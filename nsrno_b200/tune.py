@@ -32,10 +32,10 @@ import numpy as np
 
 # Parameter groups searched in this order; each candidate is a partial NsrTiles
 # dict (plus graph_iterations) merged into the current best.
-STENCIL_SHAPES = ([dict(stencil_width=w, stencil_depth=d, stencil_cols=1, stencil_rows=r)
-                   for (w, d) in ((256, 4), (256, 6), (256, 8), (512, 4)) for r in (16, 32, 64)] +
-                  [dict(stencil_width=w, stencil_depth=d, stencil_cols=2, stencil_rows=r)
-                   for (w, d) in ((256, 4), (256, 6), (256, 8), (512, 4), (512, 5)) for r in (16, 32, 64)])
+STENCIL_SHAPES = ([dict(stencil_width=w, stencil_depth=d, stencil_cols=2, stencil_rows=r)
+                   for (w, d) in ((256, 4), (256, 5), (256, 6), (256, 8), (512, 4), (512, 5))
+                   for r in (16, 32, 64)] +
+                  [dict(stencil_width=256, stencil_depth=d, stencil_cols=1, stencil_rows=32) for d in (4, 6)])
 GROUPS = [
     ("stencil", STENCIL_SHAPES),
     ("stencil_ctas", [dict(stencil_ctas=0), dict(stencil_ctas=1), dict(stencil_ctas=2)]),
@@ -44,7 +44,7 @@ GROUPS = [
     ("slot_groups", [dict(slot_groups=1), dict(slot_groups=2)]),
     ("graph_iterations", [dict(graph_iterations=k) for k in (8, 16, 32)]),
 ]
-DEFAULT = dict(stencil_width=256, stencil_depth=6, stencil_cols=1, stencil_rows=32, stencil_ctas=0, cols_width=0,
+DEFAULT = dict(stencil_width=256, stencil_depth=4, stencil_cols=2, stencil_rows=32, stencil_ctas=0, cols_width=0,
                row_tile=0, slot_groups=0, graph_iterations=16)
 TILE_KEYS = ("stencil_width", "stencil_depth", "stencil_cols", "stencil_rows", "stencil_ctas", "cols_width",
              "row_tile", "slot_groups")

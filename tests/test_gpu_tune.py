@@ -16,8 +16,8 @@ def test_tuned_shapes_solve_the_same_systems(cuda, tmp_path):
     med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=cuda)
     f, th = rec.systems()
     f, th = f[::97][:6], th[::97][:6]
-    groups = [("stencil", [dict(stencil_width=512, stencil_depth=4, stencil_rows=8),
-                           dict(stencil_width=256, stencil_depth=8, stencil_rows=32)]),
+    groups = [("stencil", [dict(stencil_width=512, stencil_depth=4, stencil_cols=2, stencil_rows=8),
+                           dict(stencil_width=256, stencil_depth=6, stencil_cols=1, stencil_rows=32)]),
               ("row_tile", [dict(row_tile=2)]), ("graph_iterations", [dict(graph_iterations=8)])]
     path = tmp_path / "tiles.json"
     first = tune.tuned_config(med, f, th, n_slots=6, path=path, iterations=12, repeats=1, groups=groups)

@@ -12,7 +12,7 @@ def fake_cost(cfg):
     if cfg["stencil_width"] == 512 and cfg["stencil_depth"] == 5:
         return None
     c = 1.0
-    c += {4: 0.3, 6: 0.1, 8: 0.0}[cfg["stencil_depth"]] if cfg["stencil_width"] == 256 else 0.2
+    c += {4: 0.3, 5: 0.2, 6: 0.1, 8: 0.0}[cfg["stencil_depth"]] if cfg["stencil_width"] == 256 else 0.2
     c += {8: 0.05, 16: 0.0, 32: 0.02, 64: 0.03}[cfg["stencil_rows"]]
     c += 0.01 * cfg["stencil_ctas"]
     c += {0: 0.04, 8: 0.0, 16: 0.04}[cfg["cols_width"]]
@@ -42,7 +42,7 @@ def test_rejected_default_is_an_error():
 
 def test_split_drops_zero_fields():
     tiles, k = tune.split({**tune.DEFAULT, "cols_width": 8, "graph_iterations": 32})
-    assert tiles == {"stencil_width": 256, "stencil_depth": 6, "stencil_cols": 1, "stencil_rows": 32,
+    assert tiles == {"stencil_width": 256, "stencil_depth": 4, "stencil_cols": 2, "stencil_rows": 32,
                      "cols_width": 8}
     assert k == 32
 
