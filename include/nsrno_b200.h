@@ -420,6 +420,11 @@ int nsr_true_residual(const NsrGrid* grid, const void* coef, const double* freq_
 
 /* ---- Learned preconditioner: inference -------------------------------- */
 
+/* Arithmetic of the network: FP32, or BF16 weights and activations with FP32
+ * accumulation (the state then holds bfloat16 planes). */
+#define NSR_LEARNED_FP32 0
+#define NSR_LEARNED_BF16 1
+
 /* Bytes of the low-resolution network state of n_freq frequencies. */
 size_t nsr_learned_state_bytes(const NsrGrid* grid, int32_t n_freq);
 
@@ -433,6 +438,12 @@ size_t nsr_learned_state_bytes(const NsrGrid* grid, int32_t n_freq);
 int nsr_learned_setup(const NsrGrid* grid, const float* c, const float* rho, const float* alpha,
                       const double* freq_hz, int32_t n_freq, const float* params, void* state,
                       void* gains, void* stream);
+/* The same with the network's precision (NSR_LEARNED_FP32 / NSR_LEARNED_BF16);
+ * a BF16 state must be passed to the _ex backward entry points with the same
+ * precision. */
+int nsr_learned_setup_ex(const NsrGrid* grid, const float* c, const float* rho, const float* alpha,
+                         const double* freq_hz, int32_t n_freq, const float* params, int32_t precision,
+                         void* state, void* gains, void* stream);
 
 /* y = M x (adjoint = 0) or M^H x (adjoint = 1) of the learned preconditioner
  * for n_systems c64 fields; workspace of nsr_precondition_workspace_size.
@@ -453,12 +464,18 @@ size_t nsr_learned_backward_workspace_size(const NsrGrid* grid, int32_t n_freq);
 int nsr_learned_map_backward(const NsrGrid* grid, const void* state, int32_t n_freq,
                              const float* g_inner, const float* g_outer, float* d_maps,
                              void* workspace, size_t workspace_bytes, void* stream);
+int nsr_learned_map_backward_ex(const NsrGrid* grid, const void* state, int32_t precision, int32_t n_freq,
+                                const float* g_inner, const float* g_outer, float* d_maps,
+                                void* workspace, size_t workspace_bytes, void* stream);
 
 /* Map cotangents -> gradients of the convolution weights and biases, ADDED to
  * d_params[9 .. NSR_LEARNED_PARAMS). */
 int nsr_learned_network_backward(const NsrGrid* grid, const float* params, const void* state,
                                  int32_t n_freq, const float* d_maps, float* d_params,
                                  void* workspace, size_t workspace_bytes, void* stream);
+int nsr_learned_network_backward_ex(const NsrGrid* grid, const float* params, const void* state,
+                                    int32_t precision, int32_t n_freq, const float* d_maps, float* d_params,
+                                    void* workspace, size_t workspace_bytes, void* stream);
 
 size_t nsr_learned_spectral_workspace_size(const NsrGrid* grid, int32_t n_systems);
 

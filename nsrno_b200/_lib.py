@@ -27,9 +27,12 @@ EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_m
            "nsr_learned_spectral_workspace_size", "nsr_learned_spectral_backward", "nsr_learned_adam",
            "nsr_tangent_rhs", "nsr_dense_precondition_workspace_size", "nsr_dense_precondition", "nsr_band_rf",
            "nsr_true_residual_workspace_size", "nsr_true_residual", "nsr_dense_solve_workspace_size",
+           "nsr_learned_setup_ex", "nsr_learned_map_backward_ex", "nsr_learned_network_backward_ex",
            "nsr_dense_solve")
 
 LEARNED_PARAMS = 3645
+LEARNED_FP32, LEARNED_BF16 = 0, 1
+PRECISIONS = {"fp32": LEARNED_FP32, "bf16": LEARNED_BF16}
 
 
 class NsrGrid(ctypes.Structure):
@@ -167,11 +170,14 @@ def load():
     lib.nsr_learned_state_bytes.restype = S
     lib.nsr_learned_state_bytes.argtypes = [G, I]
     lib.nsr_learned_setup.argtypes = [G, P, P, P, P, I, P, P, P, P]
+    lib.nsr_learned_setup_ex.argtypes = [G, P, P, P, P, I, P, I, P, P, P]
     lib.nsr_learned_precondition.argtypes = [G, L, P, I, I, P, P, P, S, P]
     lib.nsr_learned_backward_workspace_size.restype = S
     lib.nsr_learned_backward_workspace_size.argtypes = [G, I]
     lib.nsr_learned_map_backward.argtypes = [G, P, I, P, P, P, P, S, P]
     lib.nsr_learned_network_backward.argtypes = [G, P, P, I, P, P, P, S, P]
+    lib.nsr_learned_map_backward_ex.argtypes = [G, P, I, I, P, P, P, P, S, P]
+    lib.nsr_learned_network_backward_ex.argtypes = [G, P, P, I, I, P, P, P, S, P]
     lib.nsr_learned_spectral_workspace_size.restype = S
     lib.nsr_learned_spectral_workspace_size.argtypes = [G, I]
     lib.nsr_learned_spectral_backward.argtypes = [G, P, P, I, P, P, P, P, S, P]

@@ -13,8 +13,10 @@
 // Sizes: the network runs on (nz/8) x (nx/8) pixels -- 12,288 at 768 x 1024 --
 // with 3,636 weights, about 90 MFLOP per frequency.  It is set up once per
 // frequency and is bound by launch latency, not by the tensor cores or HBM, so
-// the convolutions are plain FP32 CUDA-core loops with the weights staged in
-// shared memory.  What matters for the solve is that the gains are stored once
+// the convolutions are CUDA-core loops with the weights staged in shared
+// memory.  Two precisions share the kernels: FP32, and BF16 (weights rounded
+// to bfloat16, activations stored as bfloat16, every product accumulated in
+// FP32; the master weights and their gradients stay FP32).  What matters for the solve is that the gains are stored once
 // per frequency as two complex64 planes (16 B per node) that the Krylov kernels
 // read next to the vectors they already stream.
 //
@@ -31,6 +33,7 @@
 #include "nsr_internal.cuh"
 #include "nsr_device.cuh"
 
+#include <cuda_bf16.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -54,6 +57,19 @@ static_assert(LP_NPARAM == NSR_LEARNED_PARAMS, "parameter count");
 #define LP_PLANES 41
 
 namespace {
+
+// Activation storage of the network: float, or bfloat16 (the BF16 network:
+// weights rounded to bfloat16 and activations stored in bfloat16, every
+// product accumulated in float).
+__device__ __forceinline__ float ld(const float* p) { return *p; }
+__device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void stv(float* p, float v) { *p = v; }
+__device__ __forceinline__ void stv(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+template <typename T> __device__ __forceinline__ float wround(float w);
+template <> __device__ __forceinline__ float wround<float>(float w) { return w; }
+template <> __device__ __forceinline__ float wround<__nv_bfloat16>(float w) {
+  return __bfloat162float(__float2bfloat16_rn(w));
+}
 
 inline int lp_h(const NsrGrid* g) { return g->nz / 8; }
 inline int lp_w(const NsrGrid* g) { return g->nx / 8; }
@@ -81,13 +97,14 @@ __device__ __forceinline__ float lerp_weight(const Lerp& L, int p) {
   return (L.i0 == p ? 1.0f - L.l1 : 0.0f) + (L.i1 == p ? L.l1 : 0.0f);
 }
 
-__device__ __forceinline__ void node_maps(const float* __restrict__ maps, int hw, int w8, const Lerp& lz,
+template <typename T>
+__device__ __forceinline__ void node_maps(const T* __restrict__ maps, int hw, int w8, const Lerp& lz,
                                           const Lerp& lx, float m[4]) {
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const float* M = maps + c * hw;
-    const float top = (1.0f - lx.l1) * M[lz.i0 * w8 + lx.i0] + lx.l1 * M[lz.i0 * w8 + lx.i1];
-    const float bot = (1.0f - lx.l1) * M[lz.i1 * w8 + lx.i0] + lx.l1 * M[lz.i1 * w8 + lx.i1];
+    const T* M = maps + c * hw;
+    const float top = (1.0f - lx.l1) * ld(M + lz.i0 * w8 + lx.i0) + lx.l1 * ld(M + lz.i0 * w8 + lx.i1);
+    const float bot = (1.0f - lx.l1) * ld(M + lz.i1 * w8 + lx.i0) + lx.l1 * ld(M + lz.i1 * w8 + lx.i1);
     m[c] = (1.0f - lz.l1) * top + lz.l1 * bot;
   }
 }
@@ -97,9 +114,10 @@ __device__ __forceinline__ void node_maps(const float* __restrict__ maps, int hw
 // ---------------------------------------------------------------------------
 // Set-up: context and pooling, convolutions, gains.
 // ---------------------------------------------------------------------------
+template <typename T>
 __global__ void k_lp_pool(int nz, int nx, int h8, int w8, const float* __restrict__ c, const float* __restrict__ rho,
                           const float* __restrict__ alpha, const double* __restrict__ freq, int n_freq,
-                          float* __restrict__ state) {
+                          T* __restrict__ state) {
   const int hw = h8 * w8;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= hw) return;
@@ -113,30 +131,30 @@ __global__ void k_lp_pool(int nz, int nx, int h8, int w8, const float* __restric
       s2 += log1p((double)alpha[k]);
     }
   for (int f = 0; f < n_freq; ++f) {
-    float* st = state + (long long)f * LP_PLANES * hw + LP_POOL * hw;
-    st[p] = (float)(s0 / 64.0);
-    st[hw + p] = (float)(s1 / 64.0);
-    st[2 * hw + p] = (float)(s2 / 64.0);
-    st[3 * hw + p] = (float)(freq[f] / 6e6 - 1.0);
-    st[4 * hw + p] = 1.0f;
+    T* sp = state + (long long)f * LP_PLANES * hw + LP_POOL * hw;
+    stv(sp + p, (float)(s0 / 64.0));
+    stv(sp + hw + p, (float)(s1 / 64.0));
+    stv(sp + 2 * hw + p, (float)(s2 / 64.0));
+    stv(sp + 3 * hw + p, (float)(freq[f] / 6e6 - 1.0));
+    stv(sp + 4 * hw + p, 1.0f);
   }
 }
 
 // 3x3 cross-correlation, zero padding 1, one thread per pixel and all COUT outputs.
-template <int CIN, int COUT, bool TANH>
+template <typename T, int CIN, int COUT, bool TANH>
 __global__ void __launch_bounds__(128) k_lp_conv(int h8, int w8, const float* __restrict__ wt,
-                                                 const float* __restrict__ bias, float* __restrict__ state,
+                                                 const float* __restrict__ bias, T* __restrict__ state,
                                                  int in_plane, int out_plane) {
   __shared__ float sw[COUT * CIN * 9];
   __shared__ float sb[COUT];
-  for (int k = threadIdx.x; k < COUT * CIN * 9; k += blockDim.x) sw[k] = wt[k];
-  for (int k = threadIdx.x; k < COUT; k += blockDim.x) sb[k] = bias[k];
+  for (int k = threadIdx.x; k < COUT * CIN * 9; k += blockDim.x) sw[k] = wround<T>(wt[k]);
+  for (int k = threadIdx.x; k < COUT; k += blockDim.x) sb[k] = wround<T>(bias[k]);
   __syncthreads();
   const int hw = h8 * w8;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= hw) return;
-  const float* in = state + (long long)blockIdx.y * LP_PLANES * hw + in_plane * hw;
-  float* out = state + (long long)blockIdx.y * LP_PLANES * hw + out_plane * hw;
+  const T* in = state + (long long)blockIdx.y * LP_PLANES * hw + in_plane * hw;
+  T* out = state + (long long)blockIdx.y * LP_PLANES * hw + out_plane * hw;
   const int y = p / w8, x = p - y * w8;
   float acc[COUT];
 #pragma unroll
@@ -150,22 +168,23 @@ __global__ void __launch_bounds__(128) k_lp_conv(int h8, int w8, const float* __
       for (int kx = 0; kx < 3; ++kx) {
         const int xx = x + kx - 1;
         if (xx < 0 || xx >= w8) continue;
-        const float v = in[ci * hw + yy * w8 + xx];
+        const float v = ld(in + ci * hw + yy * w8 + xx);
 #pragma unroll
         for (int co = 0; co < COUT; ++co) acc[co] += sw[((co * CIN + ci) * 3 + ky) * 3 + kx] * v;
       }
     }
 #pragma unroll
-  for (int co = 0; co < COUT; ++co) out[co * hw + p] = TANH ? tanhf(acc[co]) : acc[co];
+  for (int co = 0; co < COUT; ++co) stv(out + co * hw + p, TANH ? tanhf(acc[co]) : acc[co]);
 }
 
 // inner = (1 + tanh(m0)/2) exp(-i tanh(m1)/2), outer likewise from m2, m3.
-__global__ void k_lp_gains(int nz, int nx, int h8, int w8, const float* __restrict__ state,
+template <typename T>
+__global__ void k_lp_gains(int nz, int nx, int h8, int w8, const T* __restrict__ state,
                            float2* __restrict__ gains) {
   const long long n = (long long)nz * nx;
   const int hw = h8 * w8;
   const int f = blockIdx.y;
-  const float* maps = state + (long long)f * LP_PLANES * hw + LP_MAPS * hw;
+  const T* maps = state + (long long)f * LP_PLANES * hw + LP_MAPS * hw;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(k / nx), j = (int)(k - (long long)i * nx);
     float m[4];
@@ -185,28 +204,45 @@ extern "C" size_t nsr_learned_state_bytes(const NsrGrid* grid, int32_t n_freq) {
   return nsr_align(sizeof(float) * (size_t)LP_PLANES * lp_h(grid) * lp_w(grid) * n_freq);
 }
 
-extern "C" int nsr_learned_setup(const NsrGrid* grid, const float* c, const float* rho, const float* alpha,
-                                 const double* freq_hz, int32_t n_freq, const float* params, void* state,
-                                 void* gains, void* stream) {
-  int err = nsr_check_grid(grid, false);
-  if (err) return err;
-  if (!c || !rho || !alpha || !freq_hz || !params || !state || n_freq < 0 || n_freq > 65535) return NSR_ERR_ARGUMENT;
-  if (n_freq == 0) return 0;
-  cudaStream_t st = (cudaStream_t)stream;
+template <typename T>
+static void learned_setup_t(const NsrGrid* grid, const float* c, const float* rho, const float* alpha,
+                            const double* freq_hz, int n_freq, const float* params, T* state, void* gains,
+                            cudaStream_t st) {
   const int h8 = lp_h(grid), w8 = lp_w(grid), hw = h8 * w8;
   const int pb = (hw + 127) / 128;
-  k_lp_pool<<<pb, 128, 0, st>>>(grid->nz, grid->nx, h8, w8, c, rho, alpha, freq_hz, n_freq, (float*)state);
+  k_lp_pool<T><<<pb, 128, 0, st>>>(grid->nz, grid->nx, h8, w8, c, rho, alpha, freq_hz, n_freq, state);
   const dim3 gconv(pb, n_freq);
-  k_lp_conv<5, 16, true><<<gconv, 128, 0, st>>>(h8, w8, params + LP_W1, params + LP_B1, (float*)state, LP_POOL, LP_A1);
-  k_lp_conv<16, 16, true><<<gconv, 128, 0, st>>>(h8, w8, params + LP_W2, params + LP_B2, (float*)state, LP_A1, LP_A2);
-  k_lp_conv<16, 4, false><<<gconv, 128, 0, st>>>(h8, w8, params + LP_W3, params + LP_B3, (float*)state, LP_A2, LP_MAPS);
+  k_lp_conv<T, 5, 16, true><<<gconv, 128, 0, st>>>(h8, w8, params + LP_W1, params + LP_B1, state, LP_POOL, LP_A1);
+  k_lp_conv<T, 16, 16, true><<<gconv, 128, 0, st>>>(h8, w8, params + LP_W2, params + LP_B2, state, LP_A1, LP_A2);
+  k_lp_conv<T, 16, 4, false><<<gconv, 128, 0, st>>>(h8, w8, params + LP_W3, params + LP_B3, state, LP_A2, LP_MAPS);
   if (gains) {
     const long long n = (long long)grid->nz * grid->nx;
     int bx = (int)((n + 255) / 256);
     if (bx > 1184) bx = 1184;
-    k_lp_gains<<<dim3(bx, n_freq), 256, 0, st>>>(grid->nz, grid->nx, h8, w8, (const float*)state, (float2*)gains);
+    k_lp_gains<T><<<dim3(bx, n_freq), 256, 0, st>>>(grid->nz, grid->nx, h8, w8, state, (float2*)gains);
   }
+}
+
+extern "C" int nsr_learned_setup_ex(const NsrGrid* grid, const float* c, const float* rho, const float* alpha,
+                                    const double* freq_hz, int32_t n_freq, const float* params, int32_t precision,
+                                    void* state, void* gains, void* stream) {
+  int err = nsr_check_grid(grid, false);
+  if (err) return err;
+  if (!c || !rho || !alpha || !freq_hz || !params || !state || n_freq < 0 || n_freq > 65535) return NSR_ERR_ARGUMENT;
+  if (precision != NSR_LEARNED_FP32 && precision != NSR_LEARNED_BF16) return NSR_ERR_ARGUMENT;
+  if (n_freq == 0) return 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == NSR_LEARNED_BF16)
+    learned_setup_t(grid, c, rho, alpha, freq_hz, n_freq, params, (__nv_bfloat16*)state, gains, st);
+  else
+    learned_setup_t(grid, c, rho, alpha, freq_hz, n_freq, params, (float*)state, gains, st);
   return last_error();
+}
+
+extern "C" int nsr_learned_setup(const NsrGrid* grid, const float* c, const float* rho, const float* alpha,
+                                 const double* freq_hz, int32_t n_freq, const float* params, void* state,
+                                 void* gains, void* stream) {
+  return nsr_learned_setup_ex(grid, c, rho, alpha, freq_hz, n_freq, params, NSR_LEARNED_FP32, state, gains, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -338,13 +374,14 @@ extern "C" int nsr_learned_precondition(const NsrGrid* grid, const NsrLearned* l
 // d m0 = (1 - t0^2) Re(conj(Gi) e^{-i phi1}), d m1 = (1 - t1^2) Im(conj(Gi) inner),
 // likewise m2, m3 with the outer gain; Gi = dL/d conj(inner) (the cotangent
 // convention dL = 2 Re sum conj(G) d(gain)).
-__global__ void k_lp_dmaps(int nz, int nx, int h8, int w8, const float* __restrict__ state,
+template <typename T>
+__global__ void k_lp_dmaps(int nz, int nx, int h8, int w8, const T* __restrict__ state,
                            const float2* __restrict__ g_inner, const float2* __restrict__ g_outer,
                            float* __restrict__ dm) {
   const long long n = (long long)nz * nx;
   const int hw = h8 * w8;
   const int f = blockIdx.y;
-  const float* maps = state + (long long)f * LP_PLANES * hw + LP_MAPS * hw;
+  const T* maps = state + (long long)f * LP_PLANES * hw + LP_MAPS * hw;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(k / nx), j = (int)(k - (long long)i * nx);
     float m[4];
@@ -406,12 +443,13 @@ extern "C" size_t nsr_learned_backward_workspace_size(const NsrGrid* grid, int32
   return nsr_align(sizeof(float) * (a > b ? a : b) * n_freq);
 }
 
-extern "C" int nsr_learned_map_backward(const NsrGrid* grid, const void* state, int32_t n_freq, const float* g_inner,
-                                        const float* g_outer, float* d_maps, void* workspace,
-                                        size_t workspace_bytes, void* stream) {
+extern "C" int nsr_learned_map_backward_ex(const NsrGrid* grid, const void* state, int32_t precision, int32_t n_freq,
+                                           const float* g_inner, const float* g_outer, float* d_maps,
+                                           void* workspace, size_t workspace_bytes, void* stream) {
   int err = nsr_check_grid(grid, false);
   if (err) return err;
   if (!state || !g_inner || !g_outer || !d_maps || !workspace || n_freq < 0 || n_freq > 65535) return NSR_ERR_ARGUMENT;
+  if (precision != NSR_LEARNED_FP32 && precision != NSR_LEARNED_BF16) return NSR_ERR_ARGUMENT;
   if (n_freq == 0) return 0;
   if (workspace_bytes < nsr_learned_backward_workspace_size(grid, n_freq)) return NSR_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
@@ -420,23 +458,35 @@ extern "C" int nsr_learned_map_backward(const NsrGrid* grid, const void* state, 
   int bx = (int)((n + 255) / 256);
   if (bx > 1184) bx = 1184;
   float* dm = (float*)workspace;
-  k_lp_dmaps<<<dim3(bx, n_freq), 256, 0, st>>>(grid->nz, grid->nx, h8, w8, (const float*)state,
-                                              (const float2*)g_inner, (const float2*)g_outer, dm);
+  if (precision == NSR_LEARNED_BF16)
+    k_lp_dmaps<__nv_bfloat16><<<dim3(bx, n_freq), 256, 0, st>>>(grid->nz, grid->nx, h8, w8,
+                                                                (const __nv_bfloat16*)state, (const float2*)g_inner,
+                                                                (const float2*)g_outer, dm);
+  else
+    k_lp_dmaps<float><<<dim3(bx, n_freq), 256, 0, st>>>(grid->nz, grid->nx, h8, w8, (const float*)state,
+                                                        (const float2*)g_inner, (const float2*)g_outer, dm);
   k_lp_upsample_adjoint<<<dim3((4 * hw + 127) / 128, n_freq), 128, 0, st>>>(grid->nz, grid->nx, h8, w8, dm, d_maps);
   return last_error();
+}
+
+extern "C" int nsr_learned_map_backward(const NsrGrid* grid, const void* state, int32_t n_freq, const float* g_inner,
+                                        const float* g_outer, float* d_maps, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+  return nsr_learned_map_backward_ex(grid, state, NSR_LEARNED_FP32, n_freq, g_inner, g_outer, d_maps, workspace,
+                                     workspace_bytes, stream);
 }
 
 // ---------------------------------------------------------------------------
 // Training: backward through the three convolutions.
 // ---------------------------------------------------------------------------
 // d_in[ci] = (sum_co sum_k W[co][ci][k] dz[co][p - k]) * (1 - a[ci]^2)
-template <int CIN, int COUT>
+template <typename T, int CIN, int COUT>
 __global__ void __launch_bounds__(128) k_lp_conv_bwd_data(int h8, int w8, const float* __restrict__ wt,
                                                           const float* __restrict__ dz, int dz_stride,
-                                                          const float* __restrict__ state, int act_plane,
+                                                          const T* __restrict__ state, int act_plane,
                                                           float* __restrict__ din, int din_stride) {
   __shared__ float sw[COUT * CIN * 9];
-  for (int k = threadIdx.x; k < COUT * CIN * 9; k += blockDim.x) sw[k] = wt[k];
+  for (int k = threadIdx.x; k < COUT * CIN * 9; k += blockDim.x) sw[k] = wround<T>(wt[k]);
   __syncthreads();
   const int hw = h8 * w8;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -444,7 +494,7 @@ __global__ void __launch_bounds__(128) k_lp_conv_bwd_data(int h8, int w8, const 
   const int f = blockIdx.y;
   const int y = p / w8, x = p - y * w8;
   const float* g = dz + (long long)f * dz_stride;
-  const float* act = state + (long long)f * LP_PLANES * hw + act_plane * hw;
+  const T* act = state + (long long)f * LP_PLANES * hw + act_plane * hw;
   float acc[CIN];
 #pragma unroll
   for (int ci = 0; ci < CIN; ++ci) acc[ci] = 0.0f;
@@ -465,16 +515,16 @@ __global__ void __launch_bounds__(128) k_lp_conv_bwd_data(int h8, int w8, const 
   float* out = din + (long long)f * din_stride;
 #pragma unroll
   for (int ci = 0; ci < CIN; ++ci) {
-    const float a = act[ci * hw + p];
+    const float a = ld(act + ci * hw + p);
     out[ci * hw + p] = acc[ci] * (1.0f - a * a);
   }
 }
 
 // dW[co][ci][k] += sum_{f,p} dz[co][p] in[ci][p + k];  db[co] += sum dz[co][p].
 // One CTA per (co, ci); a fixed-order block reduction keeps it deterministic.
-template <int CIN, int COUT>
+template <typename T, int CIN, int COUT>
 __global__ void __launch_bounds__(256) k_lp_conv_bwd_weight(int h8, int w8, int n_freq, const float* __restrict__ dz,
-                                                            int dz_stride, const float* __restrict__ state,
+                                                            int dz_stride, const T* __restrict__ state,
                                                             int in_plane, float* __restrict__ dw,
                                                             float* __restrict__ db) {
   const int co = blockIdx.x / CIN, ci = blockIdx.x - co * CIN;
@@ -484,7 +534,7 @@ __global__ void __launch_bounds__(256) k_lp_conv_bwd_weight(int h8, int w8, int 
   for (int q = 0; q < 10; ++q) acc[q] = 0.0;
   for (int f = 0; f < n_freq; ++f) {
     const float* g = dz + (long long)f * dz_stride + co * hw;
-    const float* in = state + (long long)f * LP_PLANES * hw + (in_plane + ci) * hw;
+    const T* in = state + (long long)f * LP_PLANES * hw + (in_plane + ci) * hw;
     for (int p = threadIdx.x; p < hw; p += blockDim.x) {
       const int y = p / w8, x = p - y * w8;
       const float gv = g[p];
@@ -495,7 +545,7 @@ __global__ void __launch_bounds__(256) k_lp_conv_bwd_weight(int h8, int w8, int 
 #pragma unroll
         for (int kx = 0; kx < 3; ++kx) {
           const int xx = x + kx - 1;
-          if (yy >= 0 && yy < h8 && xx >= 0 && xx < w8) acc[ky * 3 + kx] += (double)gv * in[yy * w8 + xx];
+          if (yy >= 0 && yy < h8 && xx >= 0 && xx < w8) acc[ky * 3 + kx] += (double)gv * ld(in + yy * w8 + xx);
         }
       }
     }
@@ -516,30 +566,48 @@ __global__ void __launch_bounds__(256) k_lp_conv_bwd_weight(int h8, int w8, int 
   }
 }
 
-extern "C" int nsr_learned_network_backward(const NsrGrid* grid, const float* params, const void* state,
-                                            int32_t n_freq, const float* d_maps, float* d_params, void* workspace,
-                                            size_t workspace_bytes, void* stream) {
+template <typename T>
+static void network_backward_t(int h8, int w8, int n_freq, const float* params, const T* S, const float* d_maps,
+                               float* d_params, float* dz2, float* dz1, cudaStream_t st) {
+  const int hw = h8 * w8;
+  const dim3 gp((hw + 127) / 128, n_freq);
+  // layer 3 (no activation): dz3 = d_maps
+  k_lp_conv_bwd_weight<T, 16, 4><<<64, 256, 0, st>>>(h8, w8, n_freq, d_maps, 4 * hw, S, LP_A2, d_params + LP_W3,
+                                                      d_params + LP_B3);
+  k_lp_conv_bwd_data<T, 16, 4><<<gp, 128, 0, st>>>(h8, w8, params + LP_W3, d_maps, 4 * hw, S, LP_A2, dz2, 16 * hw);
+  k_lp_conv_bwd_weight<T, 16, 16><<<256, 256, 0, st>>>(h8, w8, n_freq, dz2, 16 * hw, S, LP_A1, d_params + LP_W2,
+                                                        d_params + LP_B2);
+  k_lp_conv_bwd_data<T, 16, 16><<<gp, 128, 0, st>>>(h8, w8, params + LP_W2, dz2, 16 * hw, S, LP_A1, dz1, 16 * hw);
+  k_lp_conv_bwd_weight<T, 5, 16><<<80, 256, 0, st>>>(h8, w8, n_freq, dz1, 16 * hw, S, LP_POOL, d_params + LP_W1,
+                                                      d_params + LP_B1);
+}
+
+extern "C" int nsr_learned_network_backward_ex(const NsrGrid* grid, const float* params, const void* state,
+                                               int32_t precision, int32_t n_freq, const float* d_maps,
+                                               float* d_params, void* workspace, size_t workspace_bytes,
+                                               void* stream) {
   int err = nsr_check_grid(grid, false);
   if (err) return err;
   if (!params || !state || !d_maps || !d_params || !workspace || n_freq < 0 || n_freq > 65535) return NSR_ERR_ARGUMENT;
+  if (precision != NSR_LEARNED_FP32 && precision != NSR_LEARNED_BF16) return NSR_ERR_ARGUMENT;
   if (n_freq == 0) return 0;
   if (workspace_bytes < nsr_learned_backward_workspace_size(grid, n_freq)) return NSR_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   const int h8 = lp_h(grid), w8 = lp_w(grid), hw = h8 * w8;
-  const float* S = (const float*)state;
   float* dz2 = (float*)workspace;              // [f][16][hw]
   float* dz1 = dz2 + (size_t)16 * hw * n_freq; // [f][16][hw]
-  const dim3 gp((hw + 127) / 128, n_freq);
-  // layer 3 (no activation): dz3 = d_maps
-  k_lp_conv_bwd_weight<16, 4><<<64, 256, 0, st>>>(h8, w8, n_freq, d_maps, 4 * hw, S, LP_A2, d_params + LP_W3,
-                                                   d_params + LP_B3);
-  k_lp_conv_bwd_data<16, 4><<<gp, 128, 0, st>>>(h8, w8, params + LP_W3, d_maps, 4 * hw, S, LP_A2, dz2, 16 * hw);
-  k_lp_conv_bwd_weight<16, 16><<<256, 256, 0, st>>>(h8, w8, n_freq, dz2, 16 * hw, S, LP_A1, d_params + LP_W2,
-                                                    d_params + LP_B2);
-  k_lp_conv_bwd_data<16, 16><<<gp, 128, 0, st>>>(h8, w8, params + LP_W2, dz2, 16 * hw, S, LP_A1, dz1, 16 * hw);
-  k_lp_conv_bwd_weight<5, 16><<<80, 256, 0, st>>>(h8, w8, n_freq, dz1, 16 * hw, S, LP_POOL, d_params + LP_W1,
-                                                  d_params + LP_B1);
+  if (precision == NSR_LEARNED_BF16)
+    network_backward_t(h8, w8, n_freq, params, (const __nv_bfloat16*)state, d_maps, d_params, dz2, dz1, st);
+  else
+    network_backward_t(h8, w8, n_freq, params, (const float*)state, d_maps, d_params, dz2, dz1, st);
   return last_error();
+}
+
+extern "C" int nsr_learned_network_backward(const NsrGrid* grid, const float* params, const void* state,
+                                            int32_t n_freq, const float* d_maps, float* d_params, void* workspace,
+                                            size_t workspace_bytes, void* stream) {
+  return nsr_learned_network_backward_ex(grid, params, state, NSR_LEARNED_FP32, n_freq, d_maps, d_params, workspace,
+                                         workspace_bytes, stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -68,6 +68,7 @@ class LearnedSetup:
     freqs: torch.Tensor       # float64 [F] (device)
     state: torch.Tensor       # network activations (device bytes)
     gains: torch.Tensor       # complex64 [F, 2, nz, nx]: inner, outer
+    precision: int = 0        # _lib.LEARNED_FP32 or LEARNED_BF16 (the state's planes)
 
     @property
     def n_gain(self):
@@ -90,20 +91,27 @@ class LearnedSetup:
 class LearnedPreconditioner:
     """Parameters of the learned preconditioner on one device."""
 
-    def __init__(self, params=None, device=None):
+    def __init__(self, params=None, device=None, precision="fp32"):
+        """``precision``: ``"fp32"`` or ``"bf16"`` -- the network's weights and
+        activations in bfloat16 with every product accumulated in FP32 (the
+        parameters themselves, their gradients and Adam stay FP32)."""
         device = torch.device(device or "cuda")
         p = initial_parameters() if params is None else torch.as_tensor(params, dtype=torch.float32).reshape(-1)
         if p.numel() != N_PARAMS:
             raise ValueError(f"expected {N_PARAMS} parameters, got {p.numel()}")
+        if precision not in _lib.PRECISIONS:
+            raise ValueError("precision must be 'fp32' or 'bf16'")
         self.params = p.to(device).contiguous()
+        self.precision = precision
         self.meta = {}
 
     @classmethod
-    def load(cls, path=WEIGHTS, device=None):
+    def load(cls, path=WEIGHTS, device=None, precision=None):
+        """Committed weights; ``precision`` defaults to the one they were trained in."""
         with np.load(path) as z:
-            obj = cls(z["params"], device=device)
-            if "meta" in z.files:
-                obj.meta = json.loads(str(z["meta"]))
+            meta = json.loads(str(z["meta"])) if "meta" in z.files else {}
+            obj = cls(z["params"], device=device, precision=precision or meta.get("precision", "fp32"))
+            obj.meta = meta
         return obj
 
     def save(self, path, **meta):
@@ -130,10 +138,11 @@ class LearnedPreconditioner:
             raise ValueError("unsupported grid for the learned preconditioner")
         state = torch.empty(nbytes, dtype=torch.uint8, device=medium.device)
         gains = torch.empty((F, 2, g.nz, g.nx), dtype=torch.complex64, device=medium.device)
-        _lib.check(lib.nsr_learned_setup(ctypes.byref(medium._grid), _ptr(medium.c), _ptr(medium.rho),
-                                         _ptr(medium.alpha), _ptr(freqs), F, _ptr(self.params), _ptr(state),
-                                         _ptr(gains), _stream()))
-        return LearnedSetup(self.params, freqs, state, gains)
+        prec = _lib.PRECISIONS[getattr(self, "precision", "fp32")]
+        _lib.check(lib.nsr_learned_setup_ex(ctypes.byref(medium._grid), _ptr(medium.c), _ptr(medium.rho),
+                                            _ptr(medium.alpha), _ptr(freqs), F, _ptr(self.params), prec,
+                                            _ptr(state), _ptr(gains), _stream()))
+        return LearnedSetup(self.params, freqs, state, gains, prec)
 
 
 def learned_precondition(medium: Medium, setup: LearnedSetup | None, x: torch.Tensor, freqs, adjoint=False,
@@ -225,7 +234,7 @@ def make_batch(medium: Medium, freqs, angles, with_target=True, tolerance=1e-6):
     return Batch(medium, freqs, angles, rhs, rx, target)
 
 
-def loss_and_grad(params: torch.Tensor, batch: Batch, steps: int, channel_weight=1.0):
+def loss_and_grad(params: torch.Tensor, batch: Batch, steps: int, channel_weight=1.0, precision="fp32"):
     """Loss and exact gradient w.r.t. all parameters (hand-written backward kernels).
 
     Loss (mean over the batch's systems) after ``steps`` minimal-residual
@@ -240,6 +249,7 @@ def loss_and_grad(params: torch.Tensor, batch: Batch, steps: int, channel_weight
     S = int(batch.freqs.numel())
     pre = LearnedPreconditioner.__new__(LearnedPreconditioner)
     pre.params = params
+    pre.precision = precision
     setup = pre.setup(med, batch.freqs)
     inner, outer = setup.gains[:, 0], setup.gains[:, 1]
     core = lambda v, adj=False: learned_precondition(med, None, v, batch.freqs, adjoint=adj, params=params)
@@ -292,10 +302,11 @@ def loss_and_grad(params: torch.Tensor, batch: Batch, steps: int, channel_weight
     bw = torch.empty(bw_bytes, dtype=torch.uint8, device=params.device)
     g = med.geometry
     d_maps = torch.empty((S, 4, g.nz // 8, g.nx // 8), dtype=torch.float32, device=params.device)
-    _lib.check(lib.nsr_learned_map_backward(grid, _ptr(setup.state), S, _ptr(g_in.contiguous()),
-                                            _ptr(g_out.contiguous()), _ptr(d_maps), _ptr(bw), bw_bytes, _stream()))
-    _lib.check(lib.nsr_learned_network_backward(grid, _ptr(params), _ptr(setup.state), S, _ptr(d_maps), _ptr(grad),
-                                                _ptr(bw), bw_bytes, _stream()))
+    _lib.check(lib.nsr_learned_map_backward_ex(grid, _ptr(setup.state), setup.precision, S, _ptr(g_in.contiguous()),
+                                               _ptr(g_out.contiguous()), _ptr(d_maps), _ptr(bw), bw_bytes,
+                                               _stream()))
+    _lib.check(lib.nsr_learned_network_backward_ex(grid, _ptr(params), _ptr(setup.state), setup.precision, S,
+                                                   _ptr(d_maps), _ptr(grad), _ptr(bw), bw_bytes, _stream()))
     return float(loss_sys.mean()), grad, [float(v) for v in loss_sys]
 
 
@@ -329,7 +340,7 @@ def training_media(n_media, nz, nx, seed0=100, device=None):
 
 
 def train(steps=4000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media=16, channel_weight=1.0, seed=0,
-          device=None, log=print, params=None):
+          device=None, log=print, params=None, precision="fp32"):
     """Train the learned preconditioner on seeded breast-like media (GPU).
 
     Each step draws one training medium and ``batch`` (frequency, angle)
@@ -342,7 +353,7 @@ def train(steps=4000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media
     rng = np.random.default_rng(seed)
     media = training_media(n_media, nz, nx, device=device)
     bins = breast_bins()
-    net = LearnedPreconditioner(params, device=device)
+    net = LearnedPreconditioner(params, device=device, precision=precision)
     opt = Adam(net.params, lr=lr)
     history = []
     started = time.perf_counter()
@@ -351,7 +362,7 @@ def train(steps=4000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media
         f = rng.choice(bins, size=batch, replace=False)
         th = np.deg2rad(rng.uniform(-25.0, 25.0, size=batch))
         bt = make_batch(med, f, th, with_target=channel_weight > 0)
-        loss, grad, _ = loss_and_grad(net.params, bt, krylov_steps, channel_weight)
+        loss, grad, _ = loss_and_grad(net.params, bt, krylov_steps, channel_weight, precision=precision)
         if not math.isfinite(loss) or not bool(torch.isfinite(grad).all()):
             raise RuntimeError("non-finite training loss or gradient")
         cur = lr / 10 + 0.5 * (lr - lr / 10) * (1 + math.cos(math.pi * step / max(steps, 1)))
@@ -363,7 +374,7 @@ def train(steps=4000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media
                             "seconds": round(time.perf_counter() - started, 1)}))
     net.meta = dict(steps=steps, grid=[nz, nx], batch=batch, krylov_steps=krylov_steps, lr=lr, n_media=n_media,
                     channel_weight=channel_weight, seed=seed, final_loss=float(np.mean(history[-50:])),
-                    seconds=time.perf_counter() - started)
+                    seconds=time.perf_counter() - started, precision=precision)
     return net, history
 
 
@@ -377,10 +388,16 @@ def main():
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--media", type=int, default=16)
     ap.add_argument("--channel-weight", type=float, default=1.0)
+    ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
+    ap.add_argument("--init", type=Path, default=None, help="start from these weights (fine-tuning)")
     ap.add_argument("--out", type=Path, default=WEIGHTS)
     a = ap.parse_args()
+    init = None
+    if a.init is not None:
+        with np.load(a.init) as z:
+            init = z["params"]
     net, _ = train(steps=a.steps, nz=a.nz, nx=a.nx, batch=a.batch, krylov_steps=a.krylov_steps, lr=a.lr,
-                   n_media=a.media, channel_weight=a.channel_weight)
+                   n_media=a.media, channel_weight=a.channel_weight, params=init, precision=a.precision)
     net.save(a.out)
     print(json.dumps({"saved": str(a.out), **net.meta}))
 
