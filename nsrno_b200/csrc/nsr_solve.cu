@@ -295,16 +295,25 @@ __device__ void finish_system(const SolveArgs& A, SlotState& S, int reason, doub
   A.residual[S.sys] = rel;
   A.iterations[S.sys] = S.iters;
   A.status[S.sys] = reason;
+  if (A.fields) {
+    // counted as done once the emit pass has written its field
+    S.mode = MODE_EMIT;
+    return;
+  }
   __threadfence();
   atomicAdd(A.B.done, 1);
-  if (A.fields) S.mode = MODE_EMIT;
-  else pop_next(A, S);
+  pop_next(A, S);
 }
 
 // Scalar recurrence of one slot, run by thread 0 of the slot's last CTA.
 __device__ void finalize(const SolveArgs& A, SlotState& S, int mode, const double* sum) {
   const double tol2 = A.tol2;
-  if (mode == MODE_EMIT) { pop_next(A, S); return; }
+  if (mode == MODE_EMIT) {
+    __threadfence();
+    atomicAdd(A.B.done, 1);
+    pop_next(A, S);
+    return;
+  }
   if (mode == MODE_INIT) {
     S.bnorm2 = sum[0];
     S.rnorm2 = sum[1];

@@ -323,12 +323,17 @@ def test_device_loop_equals_host_loop(cuda):
     from nsrno_b200.solver import solve_progress
     rec, med = blob_case(cuda)
     f, th = rec.systems()
-    host = solve_batched(med, f, th, tolerance=1e-7, n_slots=4, blocking=True)
-    dev = solve_batched(med, f, th, tolerance=1e-7, n_slots=4, blocking=False)
-    torch.cuda.synchronize()
-    assert not dev.extra["blocking"] and host.extra["blocking"]
-    assert torch.equal(dev.iq, host.iq) and torch.equal(dev.iterations, host.iterations)
-    assert torch.equal(dev.status, host.status) and torch.equal(dev.residual, host.residual)
+    for k in (16, 7, 1):   # loop rounds of several lengths: a system may finish on any iteration of a round
+        host = solve_batched(med, f, th, tolerance=1e-7, n_slots=4, blocking=True, return_fields=True,
+                             graph_iterations=k)
+        dev = solve_batched(med, f, th, tolerance=1e-7, n_slots=4, blocking=False, return_fields=True,
+                            graph_iterations=k)
+        torch.cuda.synchronize()
+        assert not dev.extra["blocking"] and host.extra["blocking"]
+        assert torch.equal(dev.iq, host.iq) and torch.equal(dev.iterations, host.iterations)
+        assert torch.equal(dev.status, host.status) and torch.equal(dev.residual, host.residual)
+        # every field was emitted before the device loop ended
+        assert torch.equal(dev.fields, host.fields)
     done, rounds, error, launches = solve_progress(dev)
     assert done == len(f) and error == 0 and rounds >= 1
     assert launches == 3 + rounds * dev.extra["launches_per_round"]
