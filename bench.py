@@ -412,7 +412,7 @@ def run_ours(args):
             if learned is False and args.no_plain:
                 continue
             r = tune.tuned_config(med, f_s, a_s, learned=sample_setup if learned else None, n_slots=N_SLOTS,
-                                  refresh=args.retune)
+                                  refresh=args.retune, iterations=32, repeats=3)
             shapes[learned] = tune.split(r["config"])
             tuning["learned" if learned else "plain"] = {
                 "config": r["config"], "cached": r["cached"], "us_per_system_iteration": 1e6 * r["cost_s"],
