@@ -341,6 +341,17 @@ int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, double scal_re
                     int32_t n_fields, int32_t adjoint, int32_t precision, const void* x, void* y,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* Cotangents of the dense operator's medium-dependent coefficient planes for
+ * L = -Re sum_f conj(lam_f) . mask . A(m)(mask u_f): g_ax, g_az double [H][W]
+ * (dL/d ax, dL/d az) and g_mass double [2][H][W] (dL/d Re mass, dL/d Im
+ * mass), over n_fields c128 fields u, lam [n][H][W]; the chain rule through
+ * the coefficient construction turns them into dL/d(c, rho).  Replaces the
+ * operator part of the autograd in ImplicitChannels.backward
+ * (nsrno/dense_wave.py:250-255). */
+int nsr_dense_grad(const NsrDenseGrid* grid, const double* coef, double scal_re, double scal_im,
+                   int32_t n_fields, const double* u, const double* lam, double* g_ax, double* g_az,
+                   double* g_mass, void* stream);
+
 /* Tangent (Born) right-hand side rhs = -dA[dm] u of n_systems background
  * fields u for the material direction dm = (dlogc, dlogrho) (double [nz][nx],
  * shared by all systems), in SI units like the solver's rhs: solving

@@ -28,6 +28,7 @@ EXPORTS = ("nsr_version", "nsr_error_string", "nsr_material_bytes", "nsr_setup_m
            "nsr_tangent_rhs", "nsr_dense_precondition_workspace_size", "nsr_dense_precondition", "nsr_band_rf",
            "nsr_true_residual_workspace_size", "nsr_true_residual", "nsr_dense_solve_workspace_size",
            "nsr_learned_setup_ex", "nsr_learned_map_backward_ex", "nsr_learned_network_backward_ex",
+           "nsr_dense_grad",
            "nsr_dense_solve")
 
 LEARNED_PARAMS = 3645
@@ -162,6 +163,7 @@ def load():
     lib.nsr_dense_precondition_workspace_size.restype = S
     lib.nsr_dense_precondition_workspace_size.argtypes = [DG, I]
     lib.nsr_dense_precondition.argtypes = [DG, D, D, I, I, P, P, P, S, P]
+    lib.nsr_dense_grad.argtypes = [DG, P, D, D, I, P, P, P, P, P, P]
     lib.nsr_dense_solve_workspace_size.restype = S
     lib.nsr_dense_solve_workspace_size.argtypes = [DG, I, I]
     lib.nsr_dense_solve.argtypes = [DG, P, ctypes.POINTER(NsrDenseSolveParams), I, P, P, P,

@@ -223,6 +223,96 @@ extern "C" int nsr_dense_apply(const NsrDenseGrid* grid, const double* coef, dou
 }
 
 // ---------------------------------------------------------------------------
+// Implicit gradient of the dense operator: cotangents of its coefficient
+// planes for the bilinear form
+//   L = -Re sum_f sum_n conj(lam_f[n]) mask[n] (A(m) (mask u_f))[n]
+// that ImplicitChannels.backward differentiates (nsrno/dense_wave.py:250-255).
+// A depends on the medium only through ax, az (the face coefficients) and the
+// mass term, and L is linear in each, so
+//   dL/dax[k]   = -Re sum_f svx[j] gx_f[k] Qx_f[k],   gx = D_x(mask u) / dx,
+//   Qx = Div^T(mu lx) + gvx Div^T(mu rx),   mu = conj(lam) mask scal,
+//   (Div^T v)[k] = (1/dx) sum_q a_q (v[k-q] - v[k+1+q]),
+// likewise along z, and with w = conj(lam) mask u:
+//   dL/dRe(mass) = -Re w,  dL/dIm(mass) = Im w.
+// One thread per node sums the fields in order (deterministic).
+// ---------------------------------------------------------------------------
+__global__ void k_dense_grad(DenseGeo g, const double* __restrict__ coef, const double2* __restrict__ u,
+                             const double2* __restrict__ lam, int nf, double* __restrict__ g_ax,
+                             double* __restrict__ g_az, double* __restrict__ g_mass) {
+  const DenseCoef dc = dense_unpack(coef, g.H, g.W);
+  const long long n = (long long)g.H * g.W;
+  const double inv_dx = 1.0 / g.dx;
+  const double2 zero = make_double2(0.0, 0.0);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k / g.W), j = (int)(k - (long long)i * g.W);
+    double sax = 0.0, saz = 0.0, smr = 0.0, smi = 0.0;
+    for (int f = 0; f < nf; ++f) {
+      const double2* uf = u + (long long)f * n;
+      const double2* lf = lam + (long long)f * n;
+      // masked field and mu = conj(lam) mask scal at (i2, j2); zero outside the grid
+      auto U = [&](int i2, int j2) -> double2 {
+        if (i2 < 0 || i2 >= g.H || j2 < 0 || j2 >= g.W || !dense_inside(g, i2, j2)) return zero;
+        return uf[(long long)i2 * g.W + j2];
+      };
+      auto MU = [&](int i2, int j2) -> double2 {
+        if (i2 < 0 || i2 >= g.H || j2 < 0 || j2 >= g.W || !dense_inside(g, i2, j2)) return zero;
+        return conjc(lf[(long long)i2 * g.W + j2]) * g.scal;
+      };
+      double2 gx = zero, gz = zero, qxl = zero, qxr = zero, qzl = zero, qzr = zero;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double a = c_dense_a[q];
+        gx = gx + a * (U(i, j + 1 + q) - U(i, j - q));
+        gz = gz + a * (U(i + 1 + q, j) - U(i - q, j));
+        const int jw = j - q, je = j + 1 + q, in_ = i - q, is = i + 1 + q;
+        const double2 mw = MU(i, jw), me = MU(i, je), mn = MU(in_, j), ms = MU(is, j);
+        const double2 lxw = jw >= 0 ? dc.lx[jw] : zero, lxe = je < g.W ? dc.lx[je] : zero;
+        const double2 rxw = jw >= 0 ? dc.rx[jw] : zero, rxe = je < g.W ? dc.rx[je] : zero;
+        const double2 lzn = in_ >= 0 ? dc.lz[in_] : zero, lzs = is < g.H ? dc.lz[is] : zero;
+        const double2 rzn = in_ >= 0 ? dc.rz[in_] : zero, rzs = is < g.H ? dc.rz[is] : zero;
+        qxl = qxl + a * (mw * lxw - me * lxe);
+        qxr = qxr + a * (mw * rxw - me * rxe);
+        qzl = qzl + a * (mn * lzn - ms * lzs);
+        qzr = qzr + a * (mn * rzn - ms * rzs);
+      }
+      const double2 Qx = inv_dx * (qxl + dc.gvx[j] * qxr);
+      const double2 Qz = inv_dx * (qzl + dc.gvz[i] * qzr);
+      sax -= (dc.svx[j] * (inv_dx * gx) * Qx).x;
+      saz -= (dc.svz[i] * (inv_dx * gz) * Qz).x;
+      if (dense_inside(g, i, j)) {
+        const double2 w = conjc(lf[k]) * uf[k];
+        smr -= w.x;
+        smi += w.y;
+      }
+    }
+    g_ax[k] = sax;
+    g_az[k] = saz;
+    g_mass[k] = smr;
+    g_mass[n + k] = smi;
+  }
+}
+
+extern "C" int nsr_dense_grad(const NsrDenseGrid* grid, const double* coef, double scal_re, double scal_im,
+                              int32_t n_fields, const double* u, const double* lam, double* g_ax, double* g_az,
+                              double* g_mass, void* stream) {
+  if (!grid || !coef || !u || !lam || !g_ax || !g_az || !g_mass || n_fields < 0 || n_fields > 65535)
+    return NSR_ERR_ARGUMENT;
+  if (grid->H < 3 || grid->W < 3 || grid->h < 1 || grid->w < 1 || grid->pz < 0 || grid->px < 0 ||
+      grid->pz + grid->h > grid->H || grid->px + grid->w > grid->W || !(grid->dx > 0))
+    return NSR_ERR_ARGUMENT;
+  DenseGeo g;
+  g.H = grid->H; g.W = grid->W; g.pz = grid->pz; g.px = grid->px; g.h = grid->h; g.w = grid->w; g.dx = grid->dx;
+  g.scal = make_double2(scal_re, scal_im);
+  const long long n = (long long)g.H * g.W;
+  int bx = (int)((n + 255) / 256);
+  if (bx > 4096) bx = 4096;
+  k_dense_grad<<<bx, 256, 0, (cudaStream_t)stream>>>(g, coef, (const double2*)u, (const double2*)lam, n_fields,
+                                                     g_ax, g_az, g_mass);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
+// ---------------------------------------------------------------------------
 // Fixed preconditioner of the dense path (nsrno/conditioned_wave.py:90-92,
 // nsrno/dense_wave.py:194-196):
 //   M r = mask * IFFT((1 + lap/k0^2 - i shift)^-1 FFT(r)),

@@ -50,7 +50,12 @@ class DenseGeometry:
         self.dt = float(self.spec["native_dt_s"])
         self.pml = int(self.spec["pml"])
         self.face = round(-self.spec["z0_m"] / self.dx) + self.pz
-        self.rx_cols = np.round((np.arange(192) * 0.0002 - 0.0191 - self.spec["x0_m"]) / self.dx).astype(np.int64) + self.px
+        # 192 receivers at 0.2 mm from x = -19.1 mm (nsrno/conditioned_wave.py:30); a spec may
+        # describe another array with rx_count, rx_pitch_m and rx_first_m
+        count = int(self.spec.get("rx_count", 192))
+        pitch = float(self.spec.get("rx_pitch_m", 0.0002))
+        first = float(self.spec.get("rx_first_m", -0.0191))
+        self.rx_cols = np.round((np.arange(count) * pitch + first - self.spec["x0_m"]) / self.dx).astype(np.int64) + self.px
         cols = np.arange(self.W) - self.px
         rows = np.arange(self.H) - self.pz
         self.arx = 1.0 - self.dt * _damping(cols, self.w, self.pml, 0.0, self.dx)
@@ -72,6 +77,58 @@ class DenseGeometry:
     def pad_field(self, p):
         return torch.nn.functional.pad(p, (self.px, self.W - self.w - self.px, self.pz, self.H - self.h - self.pz))
 
+    def pad_material_t(self, m):
+        """:meth:`pad_material` in torch (differentiable): ``m [k, h, w]`` -> ``[k, H, W]``."""
+        F = torch.nn.functional
+        p = self.pml
+        inner = m[:, p:-p, p:-p]
+        m = F.pad(inner[None], (p, p, p, p), mode="replicate")
+        return F.pad(m, (self.px, self.W - self.w - self.px, self.pz, self.H - self.h - self.pz),
+                     mode="replicate")[0]
+
+    def mask_t(self, device):
+        mask = torch.zeros((self.H, self.W), dtype=torch.float64, device=device)
+        mask[self.pz:self.pz + self.h, self.px:self.px + self.w] = 1.0
+        return mask
+
+
+def medium_terms(g: DenseGeometry, medium, alpha, frequency):
+    """The medium-dependent terms of the dense operator at one frequency, in
+    torch float64 (differentiable w.r.t. ``medium [2, h, w] = (c, rho)``):
+    padded c and rho, a = rho0/rho, the face coefficients ax, az (harmonic
+    means with the periodic neighbour, zero outside the mask) and the
+    two-relaxation mass term (nsrno/conditioned_wave.py:53-69)."""
+    c, rho = g.pad_material_t(medium).unbind(0)
+    al = g.pad_material_t(alpha[None])[0]
+    mask = g.mask_t(medium.device)
+    f = float(frequency)
+    D = cmath.exp(2j * math.pi * f * g.dt)
+    q = 1.0 / D
+    a = RHO0 / rho
+    a_east = torch.roll(a, -1, dims=1)
+    a_south = torch.roll(a, -1, dims=0)
+    ax = 2.0 * a * a_east / (a + a_east) * mask
+    az = 2.0 * a * a_south / (a + a_south) * mask
+    eta0, eta1 = (al * c / C0 * v for v in g.spec["eta_per_unit_alpha"])
+    amp = (1.0 + 0.5 * (eta0 + eta1)) ** 2
+    taus = g.spec["taus_s"]
+    relax = eta0 / (amp * (1.0 + taus[0] * (D - 1.0) / g.dt)) + eta1 / (amp * (1.0 + taus[1] * (D - 1.0) / g.dt))
+    modulus = amp * (1.0 - relax) / (1.0 - (1.0 - q) * relax)
+    mass = a * (C0 / c) ** 2 / modulus
+    return dict(c=c, rho=rho, alpha=al, a=a, ax=ax, az=az, mass=mass, mask=mask, D=D, q=q)
+
+
+def source_term(g: DenseGeometry, terms, line):
+    """Pressure source of lines ``[n, w]`` on the array row (nsrno/conditioned_wave.py:82-88),
+    differentiable through ``terms`` (a and the source speed)."""
+    zi, xi = g.spec["source_c_lookup_zx"]
+    source_c = terms["c"][zi + g.pz, xi + g.px]
+    dtype = torch.complex128 if line.dtype in (torch.complex128, torch.float64) else torch.complex64
+    profile = torch.zeros((line.shape[0], g.H, g.W), dtype=dtype, device=line.device)
+    profile[:, g.face, g.px:g.px + line.shape[-1]] = line.to(dtype)
+    scale = C0 ** 2 * 2 * g.dt / (g.dx * (terms["D"] - 1.0))
+    return profile * (terms["a"] * scale / source_c).to(dtype)
+
 
 class DenseSystem:
     """One medium ``[2, h, w] = (c, rho)`` with attenuation ``alpha [h, w]`` at one frequency."""
@@ -80,30 +137,18 @@ class DenseSystem:
         g = geometry
         self.g = g
         self.frequency = float(frequency)
-        medium = np.asarray(torch.as_tensor(medium).detach().cpu(), dtype=np.float64)
-        alpha = np.asarray(torch.as_tensor(alpha).detach().cpu(), dtype=np.float64)
-        if medium.shape != (2, g.h, g.w) or alpha.shape != (g.h, g.w):
+        medium = torch.as_tensor(medium).detach().to(device=device, dtype=torch.float64)
+        alpha = torch.as_tensor(alpha).detach().to(device=device, dtype=torch.float64)
+        if tuple(medium.shape) != (2, g.h, g.w) or tuple(alpha.shape) != (g.h, g.w):
             raise ValueError("Expected native [2,z,x] medium and [z,x] alpha")
-        c, rho = g.pad_material(medium)
-        al = g.pad_material(alpha)
-        mask = np.zeros((g.H, g.W))
-        mask[g.pz:g.pz + g.h, g.px:g.px + g.w] = 1.0
-        a = RHO0 / rho
-        D = cmath.exp(2j * math.pi * self.frequency * g.dt)
-        q = 1.0 / D
+        with torch.no_grad():
+            terms = medium_terms(g, medium, alpha, self.frequency)
+        self.terms = terms
+        D, q = terms["D"], terms["q"]
         k0 = 2.0 * math.sin(math.pi * self.frequency * g.dt) / (g.dt * C0)
-        # harmonic means on the faces n+1/2 (periodic neighbour, zero outside the mask)
-        a_east = np.roll(a, -1, axis=1)
-        a_south = np.roll(a, -1, axis=0)
-        ax = 2.0 * a * a_east / (a + a_east) * mask
-        az = 2.0 * a * a_south / (a + a_south) * mask
-        # two-relaxation modulus (conditioned_wave.py:62-66)
-        eta0, eta1 = (al * c / C0 * v for v in g.spec["eta_per_unit_alpha"])
-        amp = (1.0 + 0.5 * (eta0 + eta1)) ** 2
-        taus = g.spec["taus_s"]
-        relax = eta0 / (amp * (1.0 + taus[0] * (D - 1.0) / g.dt)) + eta1 / (amp * (1.0 + taus[1] * (D - 1.0) / g.dt))
-        modulus = amp * (1.0 - relax) / (1.0 - (1.0 - q) * relax)
-        mass = a * (C0 / c) ** 2 / modulus
+        ax = terms["ax"].cpu().numpy()
+        az = terms["az"].cpu().numpy()
+        mass = terms["mass"].cpu().numpy()
 
         def profiles(av, ar):
             sv = (D - 1.0) / (D - av)
@@ -124,7 +169,7 @@ class DenseSystem:
             raise RuntimeError("dense coefficient layout mismatch")
         self.D, self.q, self.k0 = D, q, k0
         self.scal = (D - 1.0) / D / k0 ** 2
-        self.c, self.rho, self.alpha = c, rho, al
+        self.c, self.rho, self.alpha = (terms[k].cpu().numpy() for k in ("c", "rho", "alpha"))
 
     def _run(self, p, adjoint):
         g = self.g
@@ -193,20 +238,12 @@ class DenseSystem:
     def source(self, line):
         """Pressure source of a line on the array row (conditioned_wave.py:82-88):
         ``line [n, w]`` padded into row ``face``, times ``a c0^2 2 dt / (c_src dx (D - 1))``."""
-        g = self.g
         line = torch.as_tensor(line)
         squeeze = line.dim() == 1
         if squeeze:
             line = line[None]
-        dev = line.device
-        zi, xi = g.spec["source_c_lookup_zx"]
-        source_c = float(self.c[zi + g.pz, xi + g.px])
-        a = torch.as_tensor(RHO0 / self.rho, device=dev)
-        dtype = torch.complex128 if line.dtype in (torch.complex128, torch.float64) else torch.complex64
-        profile = torch.zeros((line.shape[0], g.H, g.W), dtype=dtype, device=dev)
-        profile[:, g.face, g.px:g.px + line.shape[-1]] = line.to(dtype)
-        scale = C0 ** 2 * 2 * g.dt / (source_c * g.dx * (self.D - 1.0))
-        out = profile * (a.to(dtype) * scale)
+        terms = {k: (v.to(line.device) if torch.is_tensor(v) else v) for k, v in self.terms.items()}
+        out = source_term(self.g, terms, line)
         return out[0] if squeeze else out
 
 
@@ -300,3 +337,147 @@ def save_reference(directory, fields):
     d.mkdir(parents=True, exist_ok=True)
     for a in range(fields.shape[0]):
         np.save(d / f"a{a:02d}.npy", fields[a].cpu().numpy())
+
+
+# ---------------------------------------------------------------------------
+# Implicit gradient and the converged, differentiable channels of the dense
+# path (nsrno/dense_wave.py:227-259, nsrno/dense_surrogate.py:19-28).
+# ---------------------------------------------------------------------------
+def material_gradient(system: DenseSystem, medium, alpha, u_total, lam, line):
+    """d/d(medium) of ``-Re sum conj(lam) mask [A(m)(mask u_total) - S(m) line]``,
+    the scalar ImplicitChannels.backward differentiates (nsrno/dense_wave.py:250-255).
+
+    The operator part goes through ``nsr_dense_grad`` (cotangents of the face
+    coefficients and of the mass term, a contraction of the forward and adjoint
+    fields on the device); the chain rule from those planes, and the source
+    term, back to ``medium [2, h, w] = (c, rho)`` is torch autograd of
+    :func:`medium_terms` (elementwise work on single planes)."""
+    g = system.g
+    lib = _lib.load()
+    dev = system.coef.device
+    u_total = torch.as_tensor(u_total).to(dev, torch.complex128).contiguous()
+    lam = torch.as_tensor(lam).to(dev, torch.complex128).contiguous()
+    if u_total.dim() == 2:
+        u_total, lam = u_total[None], lam[None]
+    n = u_total.shape[0]
+    g_ax = torch.empty((g.H, g.W), dtype=torch.float64, device=dev)
+    g_az = torch.empty_like(g_ax)
+    g_mass = torch.empty((2, g.H, g.W), dtype=torch.float64, device=dev)
+    _lib.check(lib.nsr_dense_grad(ctypes.byref(g.struct), ctypes.c_void_p(system.coef.data_ptr()),
+                                  float(system.scal.real), float(system.scal.imag), n,
+                                  ctypes.c_void_p(u_total.data_ptr()), ctypes.c_void_p(lam.data_ptr()),
+                                  ctypes.c_void_p(g_ax.data_ptr()), ctypes.c_void_p(g_az.data_ptr()),
+                                  ctypes.c_void_p(g_mass.data_ptr()),
+                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    with torch.enable_grad():
+        m = torch.as_tensor(medium).detach().to(dev, torch.float64).requires_grad_(True)
+        al = torch.as_tensor(alpha).detach().to(dev, torch.float64)
+        t = medium_terms(g, m, al, system.frequency)
+        surrogate = ((t["ax"] * g_ax).sum() + (t["az"] * g_az).sum() + (t["mass"].real * g_mass[0]).sum() +
+                     (t["mass"].imag * g_mass[1]).sum())
+        line = torch.as_tensor(line).to(dev)
+        src = source_term(g, t, line.reshape(n, -1).to(torch.complex128))
+        surrogate = surrogate + (lam.conj() * t["mask"] * src).real.sum()
+        return torch.autograd.grad(surrogate, m)[0]
+
+
+class DenseAcquisition:
+    """The ``data`` of the dense path (the role of nsrno/dense_wave.py:15-57's
+    DenseData): geometry, the source line of every (bin, angle), and the
+    homogeneous-medium reference field of every (bin, angle), computed on
+    first use by :func:`homogeneous_reference` and cached (the reference
+    reads them from ``reference/a{angle:02d}.npy``)."""
+
+    def __init__(self, geometry: DenseGeometry, bins, lines, references=None, device="cuda", tolerance=1e-8):
+        self.geometry = geometry
+        self.bins = [int(b) for b in bins]
+        self.lines = torch.as_tensor(lines).to(device, torch.complex128)   # [bins, angles, w]
+        self.device = torch.device(device)
+        self.tolerance = tolerance
+        self._refs = {}
+        if references is not None:     # [angles, bins, h, w], the on-disk layout
+            refs = torch.as_tensor(references)
+            for k, b in enumerate(self.bins):
+                self._refs[b] = g_pad(geometry, refs[:, k].to(self.device, torch.complex128))
+
+    @staticmethod
+    def frequency(frequency_bin):
+        return frequency_bin * 40e6 / 2401
+
+    def line(self, frequency_bin, angles):
+        return self.lines[self.bins.index(frequency_bin)][list(angles)]
+
+    def reference(self, frequency_bin, angles):
+        if frequency_bin not in self._refs:
+            lines = self.lines[self.bins.index(frequency_bin)][None]
+            fields = homogeneous_reference(self.geometry, [self.frequency(frequency_bin)], lines,
+                                           tolerance=self.tolerance, device=self.device)
+            self._refs[frequency_bin] = g_pad(self.geometry, fields[:, 0].to(torch.complex128))
+        return self._refs[frequency_bin][list(angles)]
+
+
+def g_pad(geometry, native):
+    """Native fields ``[n, h, w]`` on the padded grid."""
+    return geometry.pad_field(native)
+
+
+class DenseImplicitChannels(torch.autograd.Function):
+    """Converged channels of the dense operator with the implicit adjoint gradient
+    (ImplicitChannels, nsrno/dense_wave.py:227-256): the forward solves the
+    scattered field of the assembled right-hand side (homogeneous-reference
+    subtraction), the backward one adjoint solve and :func:`material_gradient`."""
+
+    @staticmethod
+    def forward(ctx, medium, alpha, data, frequency_bin, angles, tolerance):
+        from .solver import receiver_response
+        g = data.geometry
+        f = data.frequency(frequency_bin)
+        system = DenseSystem(g, medium.detach(), alpha.detach(), f, device=data.device)
+        reference = homogeneous_system(g, f, device=data.device)
+        line = data.line(frequency_bin, angles)
+        pref = data.reference(frequency_bin, angles)
+        rhs = assemble(system, reference, line, pref)
+        u, info = solve(system, rhs, tolerance=tolerance)
+        if info["reason"] != "converged":
+            raise RuntimeError("Forward failed to converge: " + str(info))
+        ctx.system, ctx.line, ctx.tolerance = system, line, tolerance
+        ctx.save_for_backward(medium, alpha, u, pref)
+        resp = receiver_response(f)
+        return (u[:, g.face, torch.as_tensor(g.rx_cols, device=u.device)] * resp).to(torch.complex128)
+
+    @staticmethod
+    def backward(ctx, gradient):
+        from .solver import receiver_response
+        medium, alpha, u, pref = ctx.saved_tensors
+        system = ctx.system
+        g = system.g
+        with torch.no_grad():
+            rhs = torch.zeros_like(u)
+            rhs[:, g.face, torch.as_tensor(g.rx_cols, device=u.device)] = \
+                (gradient * receiver_response(system.frequency)).to(rhs.dtype)
+            lam, info = solve(system, rhs, adjoint=True, tolerance=ctx.tolerance)
+            if info["reason"] != "converged":
+                raise RuntimeError("Adjoint failed to converge: " + str(info))
+        derivative = material_gradient(system, medium, alpha, u + pref, lam, ctx.line)
+        return derivative.to(medium.dtype), None, None, None, None, None
+
+
+def dense_implicit_channels(medium, alpha, data: DenseAcquisition, frequency_bin, angles, tolerance=1e-5):
+    """Differentiable converged receiver channels ``[A, 192]`` of the dense operator."""
+    return DenseImplicitChannels.apply(medium, alpha, data, frequency_bin, list(angles), tolerance)
+
+
+class DenseSurrogate(torch.nn.Module):
+    """Drop-in for ``DenseSurrogate.forward`` (nsrno/dense_surrogate.py:19-28) on the
+    8th-order dense operator: native ``medium [2, h, w]`` and ``alpha`` -> channels
+    ``[A, 192]``, differentiable through the implicit adjoint."""
+
+    def __init__(self, data: DenseAcquisition):
+        super().__init__()
+        self.data = data
+
+    def forward(self, medium, alpha, frequency_bin, angles=None, tolerance=1e-5):
+        if frequency_bin not in self.data.bins:
+            raise ValueError("Frequency outside cached dense band")
+        angles = list(range(self.data.lines.shape[1])) if angles is None else list(angles)
+        return dense_implicit_channels(medium, alpha, self.data, frequency_bin, angles, tolerance)

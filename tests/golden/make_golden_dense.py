@@ -12,8 +12,10 @@ native (masked) region -- outside it both operators are the identity.
 The probe is ``default_rng(PROBE_SEED)`` normal real + 1j normal imag, [H, W].
 Also stored, at the first frequency: the fixed preconditioner of the probe,
 the acquisition right-hand side ``S(line) - S0(line) - A p_ref + A0 p_ref`` of
-seeded lines and masked reference fields, the source term alone, and a
-GMRES solve converged to 1e-10.
+seeded lines and masked reference fields, the source term alone, a GMRES
+solve converged to 1e-10, and the implicit gradient of ImplicitChannels'
+backward for seeded forward and adjoint fields (the same lines and reference
+fields).
 """
 from __future__ import annotations
 
@@ -25,6 +27,7 @@ import numpy as np
 
 PROBE_SEED = 20261203
 ASSEMBLY_SEED = 77
+GRADIENT_SEED = 4242
 SPEC = {"medium_shape": [32, 40], "dx_m": 5e-5, "x0_m": -0.001, "z0_m": -0.0002, "native_dt_s": 2.5e-9,
         "pml": 6, "eta_per_unit_alpha": [0.012, 0.021], "taus_s": [2.0e-8, 1.5e-7],
         "source_c_lookup_zx": [10, 20]}
@@ -86,6 +89,18 @@ def main(reference_root):
     assert reason == "converged", trace[-1]
     out["solve_rhs"] = b.numpy()
     out["solve_x"] = x.numpy()
+    # The implicit gradient of ImplicitChannels.backward (nsrno/dense_wave.py:250-255)
+    # for seeded fields: d/d(medium) of -Re sum conj(lam) mask (A(m)(mask (u + pref)) - S(m) line).
+    grng = np.random.default_rng(GRADIENT_SEED)
+    shape = (2, g.H, g.W)
+    u = torch.tensor(grng.standard_normal(shape) + 1j * grng.standard_normal(shape))
+    lam = torch.tensor(grng.standard_normal(shape) + 1j * grng.standard_normal(shape))
+    material = medium.clone().requires_grad_(True)
+    physical = ConditionedFrequencySystem(g, material, torch.tensor(alpha), FREQS[0])
+    residual = physical(g.mask * (u + pref)) - source_rhs(physical, line)
+    scalar = -(lam.conj() * g.mask * residual).real.sum()
+    out.update(grad_u=u.numpy(), grad_lam=lam.numpy(),
+               grad_medium=torch.autograd.grad(scalar, material)[0].numpy())
     path = Path(__file__).resolve().parent / "reference_dense.npz"
     np.savez_compressed(path, **out)
     print(path, {k: np.shape(v) for k, v in out.items()})
