@@ -79,6 +79,10 @@ typedef struct NsrTiles {
   int32_t row_tile;          /* rows per row-FFT CTA: 1..8                     */
   int32_t slot_groups;       /* independent slot groups on graph branches: 1, 2 */
   int32_t stencil_cols;      /* adjacent columns per stencil thread: 1 or 2    */
+  int32_t cols_staged;       /* 1: column transform staged wholly through shared
+                                memory; 0: first and last stages fused into the
+                                global load and store (sizes 256..2048 of 2^a 3^b) */
+  int32_t reserved[3];
 } NsrTiles;
 
 /* Krylov parameters of nsr_solve_batched. */

@@ -597,6 +597,100 @@ __device__ __forceinline__ void ct_cols_fused(float2* s, const float2* __restric
   if constexpr (LAST > 0) ct_inverse<N, LAST - 1, true, 1, TC, false>(s, TC, tws);
 }
 
+// Inverse stages S down to STOP (inclusive).
+template <int N, int S, int STOP, bool LF, int LS, int ES, bool PAD>
+__device__ __forceinline__ void ct_inverse_downto(float2* s, int nl, const float2* __restrict__ tws) {
+  if constexpr (S >= STOP) {
+    constexpr RadixList RL = nsr_radix_list(N);
+    constexpr int R = RL.r[S];
+    constexpr int L = nsr_stage_len(N, S);
+    ct_stage<N, R, L, true, LF, LS, ES, PAD>(s, nl, tws);
+    __syncthreads();
+    ct_inverse_downto<N, S - 1, STOP, LF, LS, ES, PAD>(s, nl, tws);
+  }
+}
+
+// The column pass of a TC-column tile of a field in global memory (row stride
+// nx), with the first forward stage computed straight from the global loads
+// and the last inverse stage written straight to global memory: the tile
+// crosses shared memory two times fewer than load-transform-store.  Columns
+// at or beyond `ncol` read as zero and are not written.  `mul(l, k)` as in
+// ct_cols_fused.  Needs at least two stages (every specialised size has).
+template <int N, int TC, typename MUL>
+__device__ __forceinline__ void ct_cols_direct(float2* s, const float2* __restrict__ tws, float2* __restrict__ g,
+                                               int nx, int ncol, MUL mul) {
+  constexpr RadixList RL = nsr_radix_list(N);
+  constexpr int LAST = RL.nst - 1;
+  static_assert(LAST >= 1, "two stages at least");
+  constexpr int R0 = RL.r[0];
+  constexpr int M0 = N / R0;
+  const float2* __restrict__ tw0 = tws + nsr_twiddle_offset(N, N);
+  // stage 0 forward: global -> registers -> shared
+  for (int b = threadIdx.x; b < TC * M0; b += blockDim.x) {
+    const int l = b % TC, j = b / TC;
+    float2 v[R0];
+#pragma unroll
+    for (int q = 0; q < R0; ++q)
+      v[q] = l < ncol ? g[(long long)(j + q * M0) * nx + l] : make_float2(0.f, 0.f);
+    small_dft<R0, false>(v);
+#pragma unroll
+    for (int k = 1; k < R0; ++k) v[k] = v[k] * __ldg(tw0 + (k - 1) * M0 + j);
+#pragma unroll
+    for (int q = 0; q < R0; ++q) s[l + (j + q * M0) * TC] = v[q];
+  }
+  __syncthreads();
+  if constexpr (LAST > 1) ct_forward_upto<N, 1, LAST, true, 1, TC, false>(s, TC, tws);
+  // last forward stage, multiply, first inverse stage (unit twiddles, m == 1)
+  constexpr int R = RL.r[LAST];
+  constexpr int per_line = N / R;
+  for (int b = threadIdx.x; b < TC * per_line; b += blockDim.x) {
+    const int l = b % TC, o = b / TC;
+    float2* base = s + l + o * R * TC;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = base[q * TC];
+    small_dft<R, false>(v);
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = v[q] * mul(l, o * R + q);
+    small_dft<R, true>(v);
+#pragma unroll
+    for (int q = 0; q < R; ++q) base[q * TC] = v[q];
+  }
+  __syncthreads();
+  if constexpr (LAST > 1) ct_inverse_downto<N, LAST - 1, 1, true, 1, TC, false>(s, TC, tws);
+  // stage 0 inverse: shared -> registers -> global
+  for (int b = threadIdx.x; b < TC * M0; b += blockDim.x) {
+    const int l = b % TC, j = b / TC;
+    float2 v[R0];
+#pragma unroll
+    for (int q = 0; q < R0; ++q) v[q] = s[l + (j + q * M0) * TC];
+#pragma unroll
+    for (int k = 1; k < R0; ++k) v[k] = v[k] * conjc(__ldg(tw0 + (k - 1) * M0 + j));
+    small_dft<R0, true>(v);
+    if (l < ncol) {
+#pragma unroll
+      for (int q = 0; q < R0; ++q) g[(long long)(j + q * M0) * nx + l] = v[q];
+    }
+  }
+}
+
+// Column pass of a tile straight between global and shared memory for the
+// specialised sizes; returns false for other sizes.
+template <int TC, typename MUL>
+__device__ __forceinline__ bool fft_cols_direct(float2* s, const FftPlan& P, float2* __restrict__ g, int nx,
+                                                int ncol, MUL mul) {
+  switch (P.n) {
+    case 256: ct_cols_direct<256, TC>(s, P.tws, g, nx, ncol, mul); return true;
+    case 384: ct_cols_direct<384, TC>(s, P.tws, g, nx, ncol, mul); return true;
+    case 512: ct_cols_direct<512, TC>(s, P.tws, g, nx, ncol, mul); return true;
+    case 768: ct_cols_direct<768, TC>(s, P.tws, g, nx, ncol, mul); return true;
+    case 1024: ct_cols_direct<1024, TC>(s, P.tws, g, nx, ncol, mul); return true;
+    case 1536: ct_cols_direct<1536, TC>(s, P.tws, g, nx, ncol, mul); return true;
+    case 2048: ct_cols_direct<2048, TC>(s, P.tws, g, nx, ncol, mul); return true;
+    default: return false;
+  }
+}
+
 // Column pass with the fused middle stage for the specialised sizes; other
 // sizes run the separate transforms and multiply.  Returns false for those
 // other sizes, which the caller then handles itself.

@@ -216,6 +216,22 @@ __device__ __forceinline__ void cols_pass_with(float2* sm, const Geo& g, const P
   }
 }
 
+// The same pass with the first forward and the last inverse stage fused into
+// the global load and store (the specialised sizes of nsr_row_padded only);
+// STAGED selects cols_pass_with instead (every size: load, every stage in
+// shared memory, store).
+template <int TC, bool STAGED, typename MUL>
+__device__ __forceinline__ void cols_pass_direct(float2* sm, const Geo& g, const PrecTables& tab,
+                                                 float2* __restrict__ ws, int c0, MUL mul) {
+  if constexpr (STAGED) {
+    cols_pass_with<TC>(sm, g, tab, ws, c0, mul);
+  } else {
+    const int ncol = min(TC, g.nx - c0);
+    auto m = [&](int c, int z) -> float2 { return c < ncol ? mul(c, z) : make_float2(0.f, 0.f); };
+    fft_cols_direct<TC>(sm, tab.pz, ws + c0, g.nx, ncol, m);
+  }
+}
+
 // Fixed shifted-Laplace multiplier 1 / (n (-4 (s2z + s2x) + (k0 h)^2 (1 + i shift))).
 template <int TC>
 __device__ __forceinline__ void cols_pass_fixed(float2* sm, const Geo& g, const PrecTables& tab,

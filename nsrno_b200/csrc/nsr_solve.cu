@@ -215,18 +215,33 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
 // ---------------------------------------------------------------------------
 // cols: column FFT, preconditioner multiply, inverse column FFT (in place).
 // ---------------------------------------------------------------------------
-template <int TC, bool LEARNED>
+template <int TC, bool LEARNED, bool STAGED>
 __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
   const int slot = A.slot0 + blockIdx.y;
   const int mode = A.B.slots[slot].mode;
   if (!cols_active(mode, half)) return;
   const long long n = (long long)A.g.nz * A.g.nx;
-  if (LEARNED)
-    cols_pass_plane<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.sym + slot * n, A.adjoint, blockIdx.x * TC);
-  else
-    cols_pass_fixed<TC>(sm, A.g, A.tab, A.B.w + slot * n, A.B.slots[slot].freq, A.shift, A.adjoint,
-                        blockIdx.x * TC);
+  const int c0 = blockIdx.x * TC;
+  const Geo& g = A.g;
+  const int adjoint = A.adjoint;
+  if (LEARNED) {
+    const float2* __restrict__ symp = A.B.sym + slot * n;
+    cols_pass_direct<TC, STAGED>(sm, g, A.tab, A.B.w + slot * n, c0, [&](int c, int z) -> float2 {
+      const float2 mul = symp[(long long)z * g.nx + c0 + c];
+      return adjoint ? conjc(mul) : mul;
+    });
+  } else {
+    const SysScalars s = sys_scalars(g, A.B.slots[slot].freq);
+    const float inv_n = 1.0f / (float)n;
+    const float2 shiftc = make_float2((float)s.kh2, (float)(s.kh2 * A.shift));
+    const PrecTables& tab = A.tab;
+    cols_pass_direct<TC, STAGED>(sm, g, tab, A.B.w + slot * n, c0, [&](int c, int z) -> float2 {
+      const float sym = -4.0f * (tab.s2z[z] + tab.s2x[c0 + c]);
+      const float2 mul = divc(make_float2(inv_n, 0.f), make_float2(sym + shiftc.x, shiftc.y));
+      return adjoint ? conjc(mul) : mul;
+    });
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1158,11 +1173,11 @@ static size_t stn_smem(int w, int d) {
 
 // Launch shapes of one call: NsrTiles with zero fields replaced by defaults.
 struct TileChoice {
-  int sw, sd, sr, sctas, tc, rows, groups, scpt;
+  int sw, sd, sr, sctas, tc, rows, groups, scpt, cols_staged;
 };
 
 static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileChoice* c) {
-  c->sw = 256; c->sd = 4; c->sr = 32; c->sctas = 0; c->scpt = 2;
+  c->sw = 256; c->sd = 4; c->sr = 32; c->sctas = 0; c->scpt = 2; c->cols_staged = 0;
   c->tc = nsr_cols_tc(g);
   c->rows = nsr_rows_per_cta(g);
   c->groups = n_slots >= 8 ? 2 : 1;
@@ -1175,6 +1190,7 @@ static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileC
     if (t->row_tile) c->rows = t->row_tile;
     if (t->slot_groups) c->groups = t->slot_groups;
     if (t->stencil_cols) c->scpt = t->stencil_cols;
+    c->cols_staged = t->cols_staged != 0;
   }
   if (!stn_kernel(c->sw, c->sd, c->scpt, false)) return NSR_ERR_ARGUMENT;
   if (c->sr < NSR_STN_MIN_ROWS || c->sr > 64 || c->sctas < 0 || c->sctas > 8) return NSR_ERR_ARGUMENT;
@@ -1366,10 +1382,17 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
       }
     }
     NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_cols<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_cols<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_cols<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_cols<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+    // column kernel: transform tile width, learned or fixed multiplier, direct
+    // (specialised sizes) or staged through shared memory
+    typedef void (*ColsKernel)(SolveArgs, int);
+    const bool generic_cols = !nsr_row_padded(grid->nz) || T.cols_staged;
+    ColsKernel cols_fn = nullptr;
+#define NSR_COLS_PICK(TC_, L_) \
+    if (A.tc == TC_ && (A.lp != nullptr) == L_) cols_fn = generic_cols ? k_cols<TC_, L_, true> : k_cols<TC_, L_, false>;
+    NSR_COLS_PICK(16, false) NSR_COLS_PICK(8, false) NSR_COLS_PICK(16, true) NSR_COLS_PICK(8, true)
+#undef NSR_COLS_PICK
+    if (!cols_fn) { err = NSR_ERR_ARGUMENT; goto cleanup; }
+    NSR_TRY(cudaFuncSetAttribute((const void*)cols_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
     NSR_TRY(cudaFuncSetAttribute(k_rinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
 
     k_solve_init<<<64, 256, 0, st>>>(A, n_slots);
@@ -1402,13 +1425,9 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
       if (which == 0) {
         k_fwd<<<g_fwd, 256, fwd_smem, sq>>>(Ag, half);
       } else if (which == 1) {
-        if (A.lp) {
-          if (A.tc == 16) k_cols<16, true><<<g_col, 512, col_smem, sq>>>(Ag, half);
-          else k_cols<8, true><<<g_col, 512, col_smem, sq>>>(Ag, half);
-        } else {
-          if (A.tc == 16) k_cols<16, false><<<g_col, 512, col_smem, sq>>>(Ag, half);
-          else k_cols<8, false><<<g_col, 512, col_smem, sq>>>(Ag, half);
-        }
+        int hv = half;
+        void* args[] = {&Ag, &hv};
+        cudaLaunchKernel((const void*)cols_fn, g_col, dim3(512), args, col_smem, sq);
       } else if (which == 2) {
         if (A.adjoint) k_res<true><<<g_res, 256, 0, sq>>>(Ag);
         else k_res<false><<<g_res, 256, 0, sq>>>(Ag);

@@ -40,14 +40,15 @@ GROUPS = [
     ("stencil", STENCIL_SHAPES),
     ("stencil_ctas", [dict(stencil_ctas=0), dict(stencil_ctas=1), dict(stencil_ctas=2)]),
     ("cols_width", [dict(cols_width=8), dict(cols_width=16)]),
+    ("cols_staged", [dict(cols_staged=1), dict(cols_staged=0)]),
     ("row_tile", [dict(row_tile=r) for r in (2, 4, 8)]),
     ("slot_groups", [dict(slot_groups=1), dict(slot_groups=2)]),
     ("graph_iterations", [dict(graph_iterations=k) for k in (8, 16, 32)]),
 ]
 DEFAULT = dict(stencil_width=256, stencil_depth=4, stencil_cols=2, stencil_rows=32, stencil_ctas=0, cols_width=0,
-               row_tile=0, slot_groups=0, graph_iterations=16)
+               cols_staged=0, row_tile=0, slot_groups=0, graph_iterations=16)
 TILE_KEYS = ("stencil_width", "stencil_depth", "stencil_cols", "stencil_rows", "stencil_ctas", "cols_width",
-             "row_tile", "slot_groups")
+             "cols_staged", "row_tile", "slot_groups")
 
 
 def search(measure, groups=GROUPS, start=None, repeats=1):

@@ -16,6 +16,7 @@ def fake_cost(cfg):
     c += {8: 0.05, 16: 0.0, 32: 0.02, 64: 0.03}[cfg["stencil_rows"]]
     c += 0.01 * cfg["stencil_ctas"]
     c += {0: 0.04, 8: 0.0, 16: 0.04}[cfg["cols_width"]]
+    c += {0: 0.0, 1: 0.01}[cfg["cols_staged"]]
     c += {0: 0.03, 2: 0.05, 4: 0.0, 8: 0.02}[cfg["row_tile"]]
     c += {0: 0.0, 1: 0.07, 2: 0.0}[cfg["slot_groups"]]
     c += {8: 0.02, 16: 0.01, 32: 0.0}[cfg["graph_iterations"]]
