@@ -82,6 +82,8 @@ def parse():
     p.add_argument("--retune", action="store_true", help="tune even when a cached choice exists")
     p.add_argument("--record", action="store_true", help="also run the plain arm over the whole record")
     p.add_argument("--no-record", action="store_true", help="skip the whole-record run")
+    p.add_argument("--host-loop", action="store_true",
+                   help="host-polled solve loop (every kernel a separate launch, for a profiler's launch list)")
     p.add_argument("--plain-only", action="store_true",
                    help="run only the plain-Krylov arm (for profiling it); prints a short line, not the bench line")
     return p.parse_args()
@@ -430,7 +432,7 @@ def run_ours(args):
         tiles, k = shapes[learned]
         return solve_batched(medium, f, a, tolerance=TOL, max_iterations=MAX_ITERS, n_slots=N_SLOTS,
                              profile_iterations=profile, workspace=ws, learned=setup, tiles=tiles,
-                             graph_iterations=k)
+                             graph_iterations=k, blocking=True if args.host_loop else None)
 
     def barrier():
         if world > 1:

@@ -82,7 +82,11 @@ typedef struct NsrTiles {
   int32_t cols_staged;       /* 1: column transform staged wholly through shared
                                 memory; 0: first and last stages fused into the
                                 global load and store (sizes 256..2048 of 2^a 3^b) */
-  int32_t reserved[3];
+  int32_t rows_staged;       /* 1: row transforms staged wholly through shared
+                                memory; 0: first and last stages between
+                                registers and global memory (widths 256..2048
+                                of 2^a 3^b)                                    */
+  int32_t reserved[2];
 } NsrTiles;
 
 /* Krylov parameters of nsr_solve_batched. */

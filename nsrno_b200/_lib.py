@@ -53,10 +53,10 @@ class NsrTiles(ctypes.Structure):
                 ("stencil_rows", ctypes.c_int32), ("stencil_ctas", ctypes.c_int32),
                 ("cols_width", ctypes.c_int32), ("row_tile", ctypes.c_int32),
                 ("slot_groups", ctypes.c_int32), ("stencil_cols", ctypes.c_int32), ("cols_staged", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 3)]
+                ("rows_staged", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
 
     FIELDS = ("stencil_width", "stencil_depth", "stencil_rows", "stencil_ctas", "cols_width", "row_tile",
-              "slot_groups", "stencil_cols", "cols_staged")
+              "slot_groups", "stencil_cols", "cols_staged", "rows_staged")
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k in self.FIELDS}

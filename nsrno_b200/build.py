@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
@@ -48,15 +49,20 @@ def build(force=False, verbose=False):
     objdir.mkdir(exist_ok=True)
     common = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--extended-lambda",
                      f"-I{ROOT / 'include'}", f"-I{CSRC}"]
-    objects = []
+    jobs = []
     for src in sources():
         obj = objdir / (src.stem + ".o")
         cmd = [nvcc, *common, "-c", str(src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objects.append(str(obj))
+        jobs.append((cmd, str(obj)))
+    # one nvcc per translation unit, side by side
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(workers) as pool:
+        for done in [pool.submit(subprocess.run, cmd, check=True) for cmd, _ in jobs]:
+            done.result()
+    objects = [obj for _, obj in jobs]
     tmp = LIBRARY.with_suffix(".so.tmp")
     subprocess.run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objects], check=True)
     os.replace(tmp, LIBRARY)

@@ -691,6 +691,141 @@ __device__ __forceinline__ bool fft_cols_direct(float2* s, const FftPlan& P, flo
   }
 }
 
+// Row transforms of the specialised sizes straight between global memory and
+// padded shared-memory rows (element k of a row at k + k/16, row stride
+// N + N/16).  The tile is nl rows of N points, contiguous in global memory
+// (flat index k = row * N + column).  Every specialised size ends its forward
+// transform with a radix-16 stage on contiguous groups of 16 with unit
+// twiddles, which is the inverse transform's first stage: that stage goes
+// straight between registers and global memory as eight 16-byte accesses per
+// group.  The other end of the transform, stage 0 (radix R0, elements
+// j + q N/R0 of a row), is coalesced across threads:
+//  * forward: `in(std::integral_constant<int, R0>{}, k0, step, v)` fills v[q]
+//    with the value to transform at flat index k0 + q step (q < R0), doing
+//    whatever elementwise work produces it; stage 0 runs on those registers,
+//    the middle stages in shared memory, the last stage writes `g`;
+//  * inverse: the first stage reads `g`, the middle stages run in shared
+//    memory, and `out(k, v)` receives each output of stage 0 (flat index k)
+//    and stores it.
+// Two shared-memory round trips fewer than load, transform, store.
+template <int R>
+struct RadixTag { static constexpr int value = R; };
+
+template <int N, typename IN>
+__device__ __forceinline__ void ct_rows_forward_direct(float2* s, int nl, const float2* __restrict__ tws,
+                                                       float2* __restrict__ g, IN in) {
+  constexpr RadixList RL = nsr_radix_list(N);
+  constexpr int LAST = RL.nst - 1;
+  static_assert(LAST >= 1 && RL.r[LAST] == 16, "specialised sizes end with a radix-16 stage");
+  constexpr int LS = N + N / 16;
+  constexpr int R0 = RL.r[0], M0 = N / R0;
+  const float2* __restrict__ tw0 = tws + nsr_twiddle_offset(N, N);
+  for (int b = threadIdx.x; b < nl * M0; b += blockDim.x) {
+    const int l = b / M0, j = b - l * M0;
+    float2 v[R0];
+    in(RadixTag<R0>{}, l * N + j, M0, v);
+    small_dft<R0, false>(v);
+#pragma unroll
+    for (int k = 1; k < R0; ++k) v[k] = v[k] * __ldg(tw0 + (k - 1) * M0 + j);
+    float2* d = s + l * LS;
+#pragma unroll
+    for (int q = 0; q < R0; ++q) {
+      const int e = j + q * M0;
+      d[e + (e >> 4)] = v[q];
+    }
+  }
+  __syncthreads();
+  if constexpr (LAST > 1) ct_forward_upto<N, 1, LAST, false, LS, 1, true>(s, nl, tws);
+  constexpr int G = N / 16;
+  for (int b = threadIdx.x; b < nl * G; b += blockDim.x) {
+    const int l = b / G, o = b - l * G;
+    const float2* src = s + l * LS + o * 17;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = src[q];
+    small_dft<16, false>(v);
+    float4* dst = reinterpret_cast<float4*>(g + (long long)l * N + o * 16);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) dst[q] = make_float4(v[2 * q].x, v[2 * q].y, v[2 * q + 1].x, v[2 * q + 1].y);
+  }
+}
+
+template <int N, typename OUT>
+__device__ __forceinline__ void ct_rows_inverse_direct(float2* s, int nl, const float2* __restrict__ tws,
+                                                       const float2* g, OUT out) {
+  constexpr RadixList RL = nsr_radix_list(N);
+  constexpr int LAST = RL.nst - 1;
+  static_assert(LAST >= 1 && RL.r[LAST] == 16, "specialised sizes end with a radix-16 stage");
+  constexpr int LS = N + N / 16;
+  constexpr int G = N / 16;
+  for (int b = threadIdx.x; b < nl * G; b += blockDim.x) {
+    const int l = b / G, o = b - l * G;
+    const float4* src = reinterpret_cast<const float4*>(g + (long long)l * N + o * 16);
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 t = src[q];
+      v[2 * q] = make_float2(t.x, t.y);
+      v[2 * q + 1] = make_float2(t.z, t.w);
+    }
+    small_dft<16, true>(v);
+    float2* d = s + l * LS + o * 17;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) d[q] = v[q];
+  }
+  __syncthreads();
+  if constexpr (LAST > 1) ct_inverse_downto<N, LAST - 1, 1, false, LS, 1, true>(s, nl, tws);
+  constexpr int R0 = RL.r[0], M0 = N / R0;
+  const float2* __restrict__ tw0 = tws + nsr_twiddle_offset(N, N);
+  for (int b = threadIdx.x; b < nl * M0; b += blockDim.x) {
+    const int l = b / M0, j = b - l * M0;
+    const float2* src = s + l * LS;
+    float2 v[R0];
+#pragma unroll
+    for (int q = 0; q < R0; ++q) {
+      const int e = j + q * M0;
+      v[q] = src[e + (e >> 4)];
+    }
+#pragma unroll
+    for (int k = 1; k < R0; ++k) v[k] = v[k] * conjc(__ldg(tw0 + (k - 1) * M0 + j));
+    small_dft<R0, true>(v);
+#pragma unroll
+    for (int q = 0; q < R0; ++q) out(l * N + j + q * M0, v[q]);
+  }
+}
+
+// Dispatch of the direct row transforms over the specialised sizes; false for
+// any other size (the caller then stages the tile itself).
+template <typename IN>
+__device__ __forceinline__ bool fft_rows_forward_direct(float2* s, int nl, const FftPlan& P, float2* __restrict__ g,
+                                                        IN in) {
+  switch (P.n) {
+    case 256: ct_rows_forward_direct<256>(s, nl, P.tws, g, in); return true;
+    case 384: ct_rows_forward_direct<384>(s, nl, P.tws, g, in); return true;
+    case 512: ct_rows_forward_direct<512>(s, nl, P.tws, g, in); return true;
+    case 768: ct_rows_forward_direct<768>(s, nl, P.tws, g, in); return true;
+    case 1024: ct_rows_forward_direct<1024>(s, nl, P.tws, g, in); return true;
+    case 1536: ct_rows_forward_direct<1536>(s, nl, P.tws, g, in); return true;
+    case 2048: ct_rows_forward_direct<2048>(s, nl, P.tws, g, in); return true;
+    default: return false;
+  }
+}
+
+template <typename OUT>
+__device__ __forceinline__ bool fft_rows_inverse_direct(float2* s, int nl, const FftPlan& P, const float2* g,
+                                                        OUT out) {
+  switch (P.n) {
+    case 256: ct_rows_inverse_direct<256>(s, nl, P.tws, g, out); return true;
+    case 384: ct_rows_inverse_direct<384>(s, nl, P.tws, g, out); return true;
+    case 512: ct_rows_inverse_direct<512>(s, nl, P.tws, g, out); return true;
+    case 768: ct_rows_inverse_direct<768>(s, nl, P.tws, g, out); return true;
+    case 1024: ct_rows_inverse_direct<1024>(s, nl, P.tws, g, out); return true;
+    case 1536: ct_rows_inverse_direct<1536>(s, nl, P.tws, g, out); return true;
+    case 2048: ct_rows_inverse_direct<2048>(s, nl, P.tws, g, out); return true;
+    default: return false;
+  }
+}
+
 // Column pass with the fused middle stage for the specialised sizes; other
 // sizes run the separate transforms and multiply.  Returns false for those
 // other sizes, which the caller then handles itself.

@@ -119,9 +119,65 @@ __device__ __forceinline__ float2 f2(double2 a) { return make_float2((float)a.x,
 __device__ __forceinline__ bool finite2(double2 a) { return isfinite(a.x) && isfinite(a.y); }
 __device__ __forceinline__ double abs2(double2 a) { return a.x * a.x + a.y * a.y; }
 
+// The staged row pass of k_fwd: the updated tile is written to padded shared
+// rows, transformed there and copied to w.
+__device__ __forceinline__ void fwd_staged(const SolveArgs& A, const SlotState& S, const GainPair& G, float2* sm,
+                                           int mode, int nr, long long off, long long goff, int cnt, float2 sv,
+                                           float2 rt, float2 yp, float2 ys, float2 pp, float2 pv) {
+  const Geo& g = A.g;
+  float2 *r = A.B.r + off, *p = A.B.p + off, *v = A.B.v + off, *t = A.B.t + off, *y = A.B.y + off;
+  // The tile's rows are contiguous in HBM, so one flat index k = l*nx + c runs
+  // over them.  The padded row layout puts (l, c) at l*(nx + nx/16) + c + c/16,
+  // which equals k + k/16 because every padded width is a multiple of 16.
+  const bool pad = nsr_row_padded(g.nx);
+  float2* __restrict__ rr_ = r;
+  float2* __restrict__ pp_ = p;
+  float2* __restrict__ yy_ = y;
+  const float2* __restrict__ vv_ = v;
+  const float2* __restrict__ tt_ = t;
+  if (mode == MODE_ITER_A) {
+    const bool restart = S.restart != 0;
+    float2* __restrict__ rh = A.B.rh + off;
+#pragma unroll 4
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 rk = rr_[k], vk = vv_[k], tk = tt_[k], pk = pp_[k], yk = yy_[k];
+      const float2 s1 = rk + sv * vk;
+      const float2 rn = s1 + rt * tk;
+      const float2 yn = yk + yp * pk + ys * s1;
+      const float2 pn = rn + pp * pk + pv * vk;
+      rr_[k] = rn; pp_[k] = pn; yy_[k] = yn;
+      if (restart) rh[k] = rn;
+      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, pn) : pn;
+    }
+  } else if (mode == MODE_ITER_B) {
+#pragma unroll 8
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 s1 = rr_[k] + sv * vv_[k];
+      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, s1) : s1;
+    }
+  } else {  // MODE_RES: apply the pending update to y, transform y, clear it
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      const float2 s1 = rr_[k] + sv * vv_[k];
+      const float2 yn = yy_[k] + yp * pp_[k] + ys * s1;
+      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, yn) : yn;
+      yy_[k] = make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+  fft_rows<false>(sm, nr, A.tab.px);
+  float2* __restrict__ w = A.B.w + off;
+#pragma unroll 8
+  for (int k = threadIdx.x; k < cnt; k += blockDim.x) w[k] = sm[pad ? k + (k >> 4) : k];
+}
+
 // ---------------------------------------------------------------------------
-// fwd: elementwise update + forward row FFT into w.
+// fwd: elementwise update + forward row FFT into w.  DIRECT (row widths
+// 256 ... 2048 of the form 2^a 3^b): the update runs inside the transform's
+// first stage and its last stage writes w straight from registers
+// (ct_rows_forward_direct); otherwise the updated tile is staged in shared
+// memory first.
 // ---------------------------------------------------------------------------
+template <bool DIRECT>
 __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
   const int slot = A.slot0 + blockIdx.y;
@@ -168,48 +224,68 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   const float2 sv = f2(S.c_sv), rt = f2(S.c_rt), yp = f2(S.c_yp), ys = f2(S.c_ys), pp = f2(S.c_pp), pv = f2(S.c_pv);
   const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
   const long long goff = (long long)z0 * g.nx;   // node index of this tile's first element
-  // The tile's rows are contiguous in HBM, so one flat index k = l*nx + c runs
-  // over them.  The padded row layout puts (l, c) at l*(nx + nx/16) + c + c/16,
-  // which equals k + k/16 because every padded width is a multiple of 16.
-  const bool pad = nsr_row_padded(g.nx);
   float2* __restrict__ rr_ = r;
   float2* __restrict__ pp_ = p;
   float2* __restrict__ yy_ = y;
   const float2* __restrict__ vv_ = v;
   const float2* __restrict__ tt_ = t;
-  if (mode == MODE_ITER_A) {
+  if constexpr (DIRECT) {
     const bool restart = S.restart != 0;
     float2* __restrict__ rh = A.B.rh + off;
-#pragma unroll 4
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-      const float2 rk = rr_[k], vk = vv_[k], tk = tt_[k], pk = pp_[k], yk = yy_[k];
-      const float2 s1 = rk + sv * vk;
-      const float2 rn = s1 + rt * tk;
-      const float2 yn = yk + yp * pk + ys * s1;
-      const float2 pn = rn + pp * pk + pv * vk;
-      rr_[k] = rn; pp_[k] = pn; yy_[k] = yn;
-      if (restart) rh[k] = rn;
-      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, pn) : pn;
-    }
-  } else if (mode == MODE_ITER_B) {
-#pragma unroll 8
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-      const float2 s1 = rr_[k] + sv * vv_[k];
-      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, s1) : s1;
-    }
-  } else {  // MODE_RES: apply the pending update to y, transform y, clear it
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-      const float2 s1 = rr_[k] + sv * vv_[k];
-      const float2 yn = yy_[k] + yp * pp_[k] + ys * s1;
-      sm[pad ? k + (k >> 4) : k] = G.pre ? gain_mul(G.pre, goff + k, G.conj, yn) : yn;
-      yy_[k] = make_float2(0.f, 0.f);
-    }
+    // Values of one stage-0 butterfly: elements k0 + q*step, q < R.  The
+    // loads of up to four elements are issued together (two for the radix-8
+    // and radix-16 first stages, whose results already hold 16-32 registers).
+    auto in = [&](auto tag, int k0, int step, float2* out) {
+      constexpr int R = decltype(tag)::value;
+      constexpr int CH = R <= 4 ? R : 2;
+      if (mode == MODE_ITER_A) {
+#pragma unroll
+        for (int c = 0; c < R; c += CH) {
+          float2 rk[CH], vk[CH], tk[CH], pk[CH], yk[CH];
+#pragma unroll
+          for (int q = 0; q < CH; ++q) {
+            const int k = k0 + (c + q) * step;
+            rk[q] = rr_[k]; vk[q] = vv_[k]; tk[q] = tt_[k]; pk[q] = pp_[k]; yk[q] = yy_[k];
+          }
+#pragma unroll
+          for (int q = 0; q < CH; ++q) {
+            const int k = k0 + (c + q) * step;
+            const float2 s1 = rk[q] + sv * vk[q];
+            const float2 rn = s1 + rt * tk[q];
+            const float2 yn = yk[q] + yp * pk[q] + ys * s1;
+            const float2 pn = rn + pp * pk[q] + pv * vk[q];
+            rr_[k] = rn; pp_[k] = pn; yy_[k] = yn;
+            if (restart) rh[k] = rn;
+            out[c + q] = pn;
+          }
+        }
+      } else if (mode == MODE_ITER_B) {
+        float2 rk[R], vk[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int k = k0 + q * step;
+          rk[q] = rr_[k]; vk[q] = vv_[k];
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) out[q] = rk[q] + sv * vk[q];
+      } else {  // MODE_RES: apply the pending update to y, transform y, clear it
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int k = k0 + q * step;
+          const float2 s1 = rr_[k] + sv * vv_[k];
+          out[q] = yy_[k] + yp * pp_[k] + ys * s1;
+          yy_[k] = make_float2(0.f, 0.f);
+        }
+      }
+      if (G.pre) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) out[q] = gain_mul(G.pre, goff + k0 + q * step, G.conj, out[q]);
+      }
+    };
+    fft_rows_forward_direct(sm, nr, A.tab.px, A.B.w + off, in);
+  } else {
+    fwd_staged(A, S, G, sm, mode, nr, off, goff, cnt, sv, rt, yp, ys, pp, pv);
   }
-  __syncthreads();
-  fft_rows<false>(sm, nr, A.tab.px);
-  float2* __restrict__ w = A.B.w + off;
-#pragma unroll 8
-  for (int k = threadIdx.x; k < cnt; k += blockDim.x) w[k] = sm[pad ? k + (k >> 4) : k];
 }
 
 // ---------------------------------------------------------------------------
@@ -246,8 +322,11 @@ __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
 
 // ---------------------------------------------------------------------------
 // rinv: inverse row FFT in place on w, times the outer gain of the learned
-// preconditioner; afterwards w holds z = M^-1 (input of the half).
+// preconditioner; afterwards w holds z = M^-1 (input of the half).  DIRECT:
+// the transform's first stage reads w and its last stage writes it, with the
+// gain, straight from registers (ct_rows_inverse_direct).
 // ---------------------------------------------------------------------------
+template <bool DIRECT>
 __global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
   const int slot = A.slot0 + blockIdx.y;
@@ -258,7 +337,14 @@ __global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
   const int z0 = blockIdx.x * A.rows;
   const int nr = min(A.rows, g.nz - z0);
   const long long goff = (long long)z0 * g.nx;
-  float2* __restrict__ w = A.B.w + slot * n + goff;
+  float2* w = A.B.w + slot * n + goff;
+  const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
+  if constexpr (DIRECT) {
+    fft_rows_inverse_direct(sm, nr, A.tab.px, w, [&](int k, float2 v) {
+      w[k] = G.post ? gain_mul(G.post, goff + k, G.conj, v) : v;
+    });
+    return;
+  }
   const bool pad = nsr_row_padded(g.nx);   // flat index k + k/16, as in k_fwd
   const int cnt = nr * g.nx;
 #pragma unroll 8
@@ -266,7 +352,6 @@ __global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
   __syncthreads();
   fft_rows<true>(sm, nr, A.tab.px);
   __syncthreads();
-  const GainPair G = gain_pair(A.gains, S.gidx, n, A.adjoint);
 #pragma unroll 8
   for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
     const float2 v = sm[pad ? k + (k >> 4) : k];
@@ -1173,11 +1258,11 @@ static size_t stn_smem(int w, int d) {
 
 // Launch shapes of one call: NsrTiles with zero fields replaced by defaults.
 struct TileChoice {
-  int sw, sd, sr, sctas, tc, rows, groups, scpt, cols_staged;
+  int sw, sd, sr, sctas, tc, rows, groups, scpt, cols_staged, rows_staged;
 };
 
 static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileChoice* c) {
-  c->sw = 256; c->sd = 4; c->sr = 32; c->sctas = 0; c->scpt = 2; c->cols_staged = 0;
+  c->sw = 256; c->sd = 4; c->sr = 64; c->sctas = 0; c->scpt = 2; c->cols_staged = 0; c->rows_staged = 0;
   c->tc = nsr_cols_tc(g);
   c->rows = nsr_rows_per_cta(g);
   c->groups = n_slots >= 8 ? 2 : 1;
@@ -1191,6 +1276,7 @@ static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileC
     if (t->slot_groups) c->groups = t->slot_groups;
     if (t->stencil_cols) c->scpt = t->stencil_cols;
     c->cols_staged = t->cols_staged != 0;
+    c->rows_staged = t->rows_staged != 0;
   }
   if (!stn_kernel(c->sw, c->sd, c->scpt, false)) return NSR_ERR_ARGUMENT;
   if (c->sr < NSR_STN_MIN_ROWS || c->sr > 64 || c->sctas < 0 || c->sctas > 8) return NSR_ERR_ARGUMENT;
@@ -1381,7 +1467,12 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
         if (stn_per_sm < 1) { err = NSR_ERR_ARGUMENT; goto cleanup; }
       }
     }
-    NSR_TRY(cudaFuncSetAttribute(k_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
+    // row kernels: direct (specialised widths) or staged through shared memory
+    const bool direct_rows = nsr_row_padded(grid->nx) && !T.rows_staged;
+    typedef void (*RowKernel)(SolveArgs, int);
+    const RowKernel fwd_fn = direct_rows ? k_fwd<true> : k_fwd<false>;
+    const RowKernel rinv_fn = direct_rows ? k_rinv<true> : k_rinv<false>;
+    NSR_TRY(cudaFuncSetAttribute((const void*)fwd_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
     // column kernel: transform tile width, learned or fixed multiplier, direct
     // (specialised sizes) or staged through shared memory
     typedef void (*ColsKernel)(SolveArgs, int);
@@ -1393,7 +1484,7 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
 #undef NSR_COLS_PICK
     if (!cols_fn) { err = NSR_ERR_ARGUMENT; goto cleanup; }
     NSR_TRY(cudaFuncSetAttribute((const void*)cols_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
-    NSR_TRY(cudaFuncSetAttribute(k_rinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
+    NSR_TRY(cudaFuncSetAttribute((const void*)rinv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem));
 
     k_solve_init<<<64, 256, 0, st>>>(A, n_slots);
     NSR_TRY(cudaGetLastError());
@@ -1423,7 +1514,9 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
       const dim3 g_inv(nb_st, ns);
       const dim3 g_res(nb_res, ns);
       if (which == 0) {
-        k_fwd<<<g_fwd, 256, fwd_smem, sq>>>(Ag, half);
+        int hv = half;
+        void* args[] = {&Ag, &hv};
+        cudaLaunchKernel((const void*)fwd_fn, g_fwd, dim3(256), args, fwd_smem, sq);
       } else if (which == 1) {
         int hv = half;
         void* args[] = {&Ag, &hv};
@@ -1451,7 +1544,9 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
           else k_inv1<false><<<g_inv, 256, 0, sq>>>(Ag, half);
         }
       } else {
-        k_rinv<<<g_fwd, 256, fwd_smem, sq>>>(Ag, half);
+        int hv = half;
+        void* args[] = {&Ag, &hv};
+        cudaLaunchKernel((const void*)rinv_fn, g_fwd, dim3(256), args, fwd_smem, sq);
       }
     };
 

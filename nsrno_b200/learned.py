@@ -378,6 +378,30 @@ def train(steps=4000, nz=256, nx=384, batch=4, krylov_steps=48, lr=3e-3, n_media
     return net, history
 
 
+def evaluate(path=WEIGHTS, precision=None, systems=220, seed=2, tolerance=1e-6, device=None):
+    """BiCGSTAB iterations of the learned preconditioner on a held-out medium:
+    the 1024 (x) x 768 (z) breast record of ``seed`` (seed 2 is the benchmark
+    medium; training uses seeds 100 and up), ``systems`` (frequency, angle)
+    systems spread evenly over its band, solved from zero to the FP64 true
+    relative residual ``tolerance``.  Returns a dict with the mean and largest
+    iteration counts and the number converged."""
+    from .media import breast_record
+    from .solver import solve_batched
+    device = torch.device(device or "cuda")
+    rec = breast_record(seed=seed)
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=device)
+    net = LearnedPreconditioner.load(path, device=device, precision=precision)
+    f, a = rec.systems()
+    pick = np.linspace(0, len(f) - 1, min(systems, len(f))).round().astype(int)
+    f, a = f[pick], a[pick]
+    setup = net.setup(med, np.unique(f))
+    r = solve_batched(med, f, a, tolerance=tolerance, learned=setup)
+    it = r.iterations.cpu().numpy()
+    return {"weights": str(path), "precision": net.precision, "systems": int(len(f)),
+            "converged": int(sum(x == "converged" for x in r.reasons())),
+            "iterations_mean": float(it.mean()), "iterations_max": int(it.max())}
+
+
 def main():
     ap = argparse.ArgumentParser(description="Train the learned preconditioner on the GPU")
     ap.add_argument("--steps", type=int, default=4000)
@@ -391,7 +415,13 @@ def main():
     ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
     ap.add_argument("--init", type=Path, default=None, help="start from these weights (fine-tuning)")
     ap.add_argument("--out", type=Path, default=WEIGHTS)
+    ap.add_argument("--evaluate", type=Path, default=None,
+                    help="no training: report the iterations these weights take on the held-out benchmark medium")
+    ap.add_argument("--systems", type=int, default=220, help="systems of the evaluation")
     a = ap.parse_args()
+    if a.evaluate is not None:
+        print(json.dumps(evaluate(a.evaluate, precision=a.precision, systems=a.systems)))
+        return
     init = None
     if a.init is not None:
         with np.load(a.init) as z:

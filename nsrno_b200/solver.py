@@ -250,7 +250,12 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
 def solve_progress(result: BatchResult):
     """(systems finished, device loop rounds, error flag, kernels launched) of a
     non-blocking solve, from the progress record copied behind it (call after
-    the stream has passed the solve, e.g. after torch.cuda.synchronize())."""
+    the stream has passed the solve, e.g. after torch.cuda.synchronize()).
+    For a blocking solve the host already counted everything: (systems,
+    graph launches, 0, kernels launched)."""
+    if result.extra.get("blocking"):
+        st = result.extra["stats"]
+        return int(result.status.numel()), int(st.get("graph_launches", 0)), 0, int(st["launches"])
     w = result.extra["progress_words"]
     rounds = int(w[6:8].view(torch.int64)[0])
     launches = result.extra["stats"]["launches"] + rounds * result.extra["launches_per_round"]

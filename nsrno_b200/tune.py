@@ -4,7 +4,9 @@ The batched BiCGSTAB (``nsr_solve_batched``) runs nine launches per
 iteration whose shapes are free parameters (:class:`nsrno_b200._lib.NsrTiles`):
 the stencil's work item (columns ``stencil_width``, rows ``stencil_rows``),
 its copy-ring depth ``stencil_depth`` and resident CTAs per SM, the
-column-transform tile ``cols_width``, the row-transform tile ``row_tile``, the
+column-transform tile ``cols_width``, the row-transform tile ``row_tile``,
+whether the column and row transforms run their end stages between registers
+and global memory (``cols_staged``, ``rows_staged``), the
 number of slot groups on graph branches, plus the CUDA-graph length
 ``graph_iterations``.  The best choice depends on the grid, the GPU and the
 preconditioner, so it is measured: :func:`tune` times a fixed number of
@@ -41,14 +43,15 @@ GROUPS = [
     ("stencil_ctas", [dict(stencil_ctas=0), dict(stencil_ctas=1), dict(stencil_ctas=2)]),
     ("cols_width", [dict(cols_width=8), dict(cols_width=16)]),
     ("cols_staged", [dict(cols_staged=1), dict(cols_staged=0)]),
+    ("rows_staged", [dict(rows_staged=1), dict(rows_staged=0)]),
     ("row_tile", [dict(row_tile=r) for r in (2, 4, 8)]),
     ("slot_groups", [dict(slot_groups=1), dict(slot_groups=2)]),
     ("graph_iterations", [dict(graph_iterations=k) for k in (8, 16, 32)]),
 ]
-DEFAULT = dict(stencil_width=256, stencil_depth=4, stencil_cols=2, stencil_rows=32, stencil_ctas=0, cols_width=0,
-               cols_staged=0, row_tile=0, slot_groups=0, graph_iterations=16)
+DEFAULT = dict(stencil_width=256, stencil_depth=4, stencil_cols=2, stencil_rows=64, stencil_ctas=0, cols_width=0,
+               cols_staged=0, rows_staged=0, row_tile=0, slot_groups=0, graph_iterations=16)
 TILE_KEYS = ("stencil_width", "stencil_depth", "stencil_cols", "stencil_rows", "stencil_ctas", "cols_width",
-             "cols_staged", "row_tile", "slot_groups")
+             "cols_staged", "rows_staged", "row_tile", "slot_groups")
 
 
 def search(measure, groups=GROUPS, start=None, repeats=1):

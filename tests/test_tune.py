@@ -17,6 +17,7 @@ def fake_cost(cfg):
     c += 0.01 * cfg["stencil_ctas"]
     c += {0: 0.04, 8: 0.0, 16: 0.04}[cfg["cols_width"]]
     c += {0: 0.0, 1: 0.01}[cfg["cols_staged"]]
+    c += {0: 0.0, 1: 0.02}[cfg["rows_staged"]]
     c += {0: 0.03, 2: 0.05, 4: 0.0, 8: 0.02}[cfg["row_tile"]]
     c += {0: 0.0, 1: 0.07, 2: 0.0}[cfg["slot_groups"]]
     c += {8: 0.02, 16: 0.01, 32: 0.0}[cfg["graph_iterations"]]
@@ -43,7 +44,7 @@ def test_rejected_default_is_an_error():
 
 def test_split_drops_zero_fields():
     tiles, k = tune.split({**tune.DEFAULT, "cols_width": 8, "graph_iterations": 32})
-    assert tiles == {"stencil_width": 256, "stencil_depth": 4, "stencil_cols": 2, "stencil_rows": 32,
+    assert tiles == {"stencil_width": 256, "stencil_depth": 4, "stencil_cols": 2, "stencil_rows": 64,
                      "cols_width": 8}
     assert k == 32
 
