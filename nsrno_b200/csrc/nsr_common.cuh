@@ -625,18 +625,32 @@ __device__ __forceinline__ void ct_cols_direct(float2* s, const float2* __restri
   constexpr int R0 = RL.r[0];
   constexpr int M0 = N / R0;
   const float2* __restrict__ tw0 = tws + nsr_twiddle_offset(N, N);
-  // stage 0 forward: global -> registers -> shared
-  for (int b = threadIdx.x; b < TC * M0; b += blockDim.x) {
-    const int l = b % TC, j = b / TC;
-    float2 v[R0];
+  // stage 0 forward: global -> registers -> shared, U butterflies per thread
+  // with their loads issued together (radix 2: 8 loads in flight, 3 and 4: 6-8)
+  constexpr int U = R0 <= 2 ? 4 : (R0 <= 4 ? 2 : 1);
+  const int nb0 = TC * M0;
+  for (int b0 = threadIdx.x; b0 < nb0; b0 += U * blockDim.x) {
+    float2 v[U][R0];
 #pragma unroll
-    for (int q = 0; q < R0; ++q)
-      v[q] = l < ncol ? g[(long long)(j + q * M0) * nx + l] : make_float2(0.f, 0.f);
-    small_dft<R0, false>(v);
+    for (int u = 0; u < U; ++u) {
+      const int b = b0 + u * blockDim.x;
+      const int l = b % TC, j = b / TC;
+      const bool live = b < nb0 && l < ncol;
 #pragma unroll
-    for (int k = 1; k < R0; ++k) v[k] = v[k] * __ldg(tw0 + (k - 1) * M0 + j);
+      for (int q = 0; q < R0; ++q) v[u][q] = live ? g[(long long)(j + q * M0) * nx + l] : make_float2(0.f, 0.f);
+    }
 #pragma unroll
-    for (int q = 0; q < R0; ++q) s[l + (j + q * M0) * TC] = v[q];
+    for (int u = 0; u < U; ++u) {
+      const int b = b0 + u * blockDim.x;
+      if (b < nb0) {
+        const int l = b % TC, j = b / TC;
+        small_dft<R0, false>(v[u]);
+#pragma unroll
+        for (int k = 1; k < R0; ++k) v[u][k] = v[u][k] * __ldg(tw0 + (k - 1) * M0 + j);
+#pragma unroll
+        for (int q = 0; q < R0; ++q) s[l + (j + q * M0) * TC] = v[u][q];
+      }
+    }
   }
   __syncthreads();
   if constexpr (LAST > 1) ct_forward_upto<N, 1, LAST, true, 1, TC, false>(s, TC, tws);

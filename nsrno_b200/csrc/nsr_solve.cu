@@ -28,6 +28,7 @@
 
 #include <stdio.h>
 #include <stdlib.h>
+#include <type_traits>
 #include <string.h>
 
 enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES = 4, MODE_EMIT = 5 };
@@ -180,13 +181,13 @@ __device__ __forceinline__ void fwd_staged(const SolveArgs& A, const SlotState& 
 template <bool DIRECT>
 __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
-  const int slot = A.slot0 + blockIdx.y;
+  const int slot = A.slot0 + blockIdx.x;
   const SlotState& S = A.B.slots[slot];
   const int mode = S.mode;
   if (!fwd_active(mode, half)) return;
   const Geo& g = A.g;
   const long long n = (long long)g.nz * g.nx;
-  const int z0 = blockIdx.x * A.rows;
+  const int z0 = blockIdx.y * A.rows;
   const int nr = min(A.rows, g.nz - z0);
   const long long off = slot * n + (long long)z0 * g.nx;
   const int cnt = nr * g.nx;
@@ -294,11 +295,11 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
 template <int TC, bool LEARNED, bool STAGED>
 __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
-  const int slot = A.slot0 + blockIdx.y;
+  const int slot = A.slot0 + blockIdx.x;
   const int mode = A.B.slots[slot].mode;
   if (!cols_active(mode, half)) return;
   const long long n = (long long)A.g.nz * A.g.nx;
-  const int c0 = blockIdx.x * TC;
+  const int c0 = blockIdx.y * TC;
   const Geo& g = A.g;
   const int adjoint = A.adjoint;
   if (LEARNED) {
@@ -329,12 +330,12 @@ __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
 template <bool DIRECT>
 __global__ void __launch_bounds__(256, 4) k_rinv(SolveArgs A, int half) {
   extern __shared__ float2 sm[];
-  const int slot = A.slot0 + blockIdx.y;
+  const int slot = A.slot0 + blockIdx.x;
   const SlotState& S = A.B.slots[slot];
   if (!cols_active(S.mode, half)) return;
   const Geo& g = A.g;
   const long long n = (long long)g.nz * g.nx;
-  const int z0 = blockIdx.x * A.rows;
+  const int z0 = blockIdx.y * A.rows;
   const int nr = min(A.rows, g.nz - z0);
   const long long goff = (long long)z0 * g.nx;
   float2* w = A.B.w + slot * n + goff;
@@ -741,7 +742,10 @@ struct StnLayout {
 #define NSR_STN_WAIT_NS 2000000000ull   // a ring wait longer than 2 s is an error
 #define NSR_STN_FLUSH 8                  // rows per float partial sum of the inner products
 
-// Items of one launch and their decoding.
+// Items of one launch and their decoding.  Item i is band-strip i / ns of
+// slot i % ns: the slots run fastest, so the CTAs in flight at any time work
+// on the same few bands of every slot, and the medium's coefficient rows
+// (read by every slot) come from L2 after the first slot's copy.
 struct StnItems {
   int tz, nbands, nstrips, per_slot, n_items;
 };
@@ -761,7 +765,8 @@ __host__ __device__ inline StnItems stn_items(int nz, int nx, int tz, int ns) {
 // (at most 4): its register budget follows from it.
 template <int W, int D, int CPT>
 __host__ __device__ constexpr int stn_min_blocks() {
-  constexpr int by_smem = (227 * 1024) / (D * StnLayout<W>::SLOT + 2048);
+  // ring, barriers and block sums (2 KB), FP64 accumulators of the consumers
+  constexpr int by_smem = (227 * 1024) / (D * StnLayout<W>::SLOT + 2048 + 8 * NSR_NPART * (W / CPT));
   constexpr int cap = (W / CPT + 32) > 256 ? 2 : 4;
   return by_smem < 1 ? 1 : (by_smem > cap ? cap : by_smem);
 }
@@ -778,6 +783,10 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
   volatile int& abort_flag = abort_word;
   __shared__ double wsum[NC / 32][NSR_NPART];
   __shared__ double tot[NSR_NPART];
+  // Each consumer's FP64 accumulators live in shared memory (column tid): in
+  // registers they pushed the 96-register budget of four CTAs per SM into
+  // spills inside the row loop.
+  __shared__ double accs[NSR_NPART][NC];
   __shared__ int am_last;
   const Geo& g = A.g;
   const int nz = g.nz, nx = g.nx;
@@ -798,7 +807,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
     if (threadIdx.x != NC) return;
     uint32_t q = 0;   // row step counter (ring entry q % D, phase q / D)
     for (int item = blockIdx.x; item < it.n_items && !abort_flag; item += gridDim.x) {
-      const int sl = item / it.per_slot, rem = item - sl * it.per_slot;
+      const int rem = item / ns, sl = item - rem * ns;
       const int band = rem / it.nstrips, strip = rem - band * it.nstrips;
       const int slot = A.slot0 + sl;
       if (A.B.slots[slot].mode != want) continue;
@@ -855,7 +864,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   uint32_t q = 0;
   for (int item = blockIdx.x; item < it.n_items; item += gridDim.x) {
-    const int sl = item / it.per_slot, rem = item - sl * it.per_slot;
+    const int rem = item / ns, sl = item - rem * ns;
     const int band = rem / it.nstrips, strip = rem - band * it.nstrips;
     const int slot = A.slot0 + sl;
     SlotState& S = A.B.slots[slot];
@@ -879,35 +888,47 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
     const float2 sv = f2(S.c_sv);
     // Inner products: float partial sums over NSR_STN_FLUSH rows (2 NSR_STN_FLUSH
     // products per thread), accumulated in FP64.
-    double acc[NSR_NPART];
     float accf[NSR_NPART];
 #pragma unroll
-    for (int k = 0; k < NSR_NPART; ++k) { acc[k] = 0.0; accf[k] = 0.0f; }
+    for (int k = 0; k < NSR_NPART; ++k) { accs[k][tid] = 0.0; accf[k] = 0.0f; }
     const uint32_t q0 = q;   // step of row z0 - 1
     bool ok = !abort_flag;
     // rows z0 - 1 and z0
     for (uint32_t s = q0; s < q0 + 2 && ok; ++s) ok = mbar_wait(&full[s % D], (s / D) & 1, &abort_word, NSR_STN_WAIT_NS);
+    // Ring entries of rows i - 1, i, i + 1 (advanced incrementally) and the
+    // column's z and a of rows i - 1 and i, carried from row to row so that
+    // each row reads only its south neighbours from the ring.
+    int eN = q0 % D, eC = (eN + 1 == D) ? 0 : eN + 1;
+    const int ez = (CPT * tid + 2) * 8, ea = (CPT * tid + 4) * 4;
+    typedef typename std::conditional<CPT == 2, float4, float2>::type ZT;
+    typedef typename std::conditional<CPT == 2, float2, float>::type AT;
+    auto zload = [&](int e) -> ZT { return *reinterpret_cast<const ZT*>(ring + (size_t)e * Ly::SLOT + Ly::OZ + ez); };
+    auto aload = [&](int e) -> AT { return *reinterpret_cast<const AT*>(ring + (size_t)e * Ly::SLOT + Ly::OA + ea); };
+    ZT zN = ZT{}, zC = ZT{};
+    AT aN, aC = AT{};
+    if constexpr (CPT == 2) aN = make_float2(1.f, 1.f); else aN = 1.0f;   // no density contrast outside
+    if (ok) {
+      if (z0 > 0) { zN = zload(eN); aN = aload(eN); }
+      zC = zload(eC); aC = aload(eC);
+    }
     for (int k = 0; k < nrows; ++k) {
       const int i = z0 + k;
-      const uint32_t sN = q0 + k, sC = sN + 1, sS = sN + 2;
-      if (ok) ok = mbar_wait(&full[sS % D], (sS / D) & 1, &abort_word, NSR_STN_WAIT_NS);
+      const uint32_t sS = q0 + k + 2;
+      const int eS = (eC + 1 == D) ? 0 : eC + 1;
+      if (ok) ok = mbar_wait(&full[eS], (sS / D) & 1, &abort_word, NSR_STN_WAIT_NS);
       if (!ok) abort_flag = 1;
+      ZT zS = ZT{};
+      AT aS;
+      if constexpr (CPT == 2) aS = make_float2(1.f, 1.f); else aS = 1.0f;
+      if (ok && i + 1 < nz) { zS = zload(eS); aS = aload(eS); }
       if (ok && own) {
-        const unsigned char* bN = ring + (size_t)(sN % D) * Ly::SLOT;
-        const unsigned char* bC = ring + (size_t)(sC % D) * Ly::SLOT;
-        const unsigned char* bS = ring + (size_t)(sS % D) * Ly::SLOT;
+        const unsigned char* bC = ring + (size_t)eC * Ly::SLOT;
         const float2 zero = make_float2(0.f, 0.f);
         if constexpr (CPT == 2) {
-          const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-          const int ez = (2 * tid + 2) * 8, ea = (2 * tid + 4) * 4;
-          const float4 zc = *reinterpret_cast<const float4*>(bC + Ly::OZ + ez);
-          const float4 zn = i > 0 ? *reinterpret_cast<const float4*>(bN + Ly::OZ + ez) : zero4;
-          const float4 zs = i + 1 < nz ? *reinterpret_cast<const float4*>(bS + Ly::OZ + ez) : zero4;
+          const float4 zc = zC, zn = zN, zs = zS;
           const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
           const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 16) : zero;
-          const float2 ac = *reinterpret_cast<const float2*>(bC + Ly::OA + ea);
-          const float2 an = i > 0 ? *reinterpret_cast<const float2*>(bN + Ly::OA + ea) : make_float2(1.f, 1.f);
-          const float2 as = i + 1 < nz ? *reinterpret_cast<const float2*>(bS + Ly::OA + ea) : make_float2(1.f, 1.f);
+          const float2 ac = aC, an = aN, as = aS;
           const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
           const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 8) : 1.0f;
           const float2 bb = *reinterpret_cast<const float2*>(bC + Ly::OB + 8 * tid);
@@ -936,15 +957,10 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
             dot_acc_f(accf[6], accf[7], hi2(rk), s1);
           }
         } else {
-          const int ez = (tid + 2) * 8, ea = (tid + 4) * 4;
-          const float2 zc = *reinterpret_cast<const float2*>(bC + Ly::OZ + ez);
-          const float2 zn = i > 0 ? *reinterpret_cast<const float2*>(bN + Ly::OZ + ez) : zero;
-          const float2 zs = i + 1 < nz ? *reinterpret_cast<const float2*>(bS + Ly::OZ + ez) : zero;
+          const float2 zc = zC, zn = zN, zs = zS;
           const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
           const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 8) : zero;
-          const float ac = *reinterpret_cast<const float*>(bC + Ly::OA + ea);
-          const float an = i > 0 ? *reinterpret_cast<const float*>(bN + Ly::OA + ea) : 1.0f;
-          const float as = i + 1 < nz ? *reinterpret_cast<const float*>(bS + Ly::OA + ea) : 1.0f;
+          const float ac = aC, an = aN, as = aS;
           const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
           const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 4) : 1.0f;
           const float bb = *reinterpret_cast<const float*>(bC + Ly::OB + 4 * tid);
@@ -966,29 +982,32 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
           }
         }
       }
+      zN = zC; zC = zS; aN = aC; aC = aS;
       if ((k + 1) % FLUSH == 0 || k + 1 == nrows) {
 #pragma unroll
         for (int qq = 0; qq < NSR_NPART; ++qq) {
-          if (half == 1 || qq < 2) acc[qq] += (double)accf[qq];
+          if (half == 1 || qq < 2) accs[qq][tid] += (double)accf[qq];
           accf[qq] = 0.0f;
         }
       }
       // the buffer of row i - 1 is no longer needed
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[sN % D]);
+      if (lane == 0) mbar_arrive(&empty[eN]);
+      eN = eC;
+      eC = eS;
     }
     // rows z1 - 1 and z1
     __syncwarp();
     if (lane == 0) {
-      mbar_arrive(&empty[(q0 + nrows) % D]);
-      mbar_arrive(&empty[(q0 + nrows + 1) % D]);
+      mbar_arrive(&empty[eN]);
+      mbar_arrive(&empty[eC]);
     }
     q = q0 + nrows + 2;
 
     // Block sum of the partials (consumer threads only), then the arrival.
 #pragma unroll
     for (int k = 0; k < NSR_NPART; ++k) {
-      const double s = warp_sum(acc[k]);
+      const double s = warp_sum(accs[k][tid]);
       if (lane == 0) wsum[wid][k] = s;
     }
     named_sync(1, NC);
@@ -1509,8 +1528,11 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
       SolveArgs Ag = A;
       Ag.slot0 = g_first[grp];
       const int ns = g_count[grp];
-      const dim3 g_fwd((grid->nz + A.rows - 1) / A.rows, ns);
-      const dim3 g_col((grid->nx + A.tc - 1) / A.tc, ns);
+      // Slots run fastest: the CTAs of one tile of every slot run together, so a
+      // gain plane that several slots share (systems of one frequency) is read
+      // once from HBM and then from L2.
+      const dim3 g_fwd(ns, (grid->nz + A.rows - 1) / A.rows);
+      const dim3 g_col(ns, (grid->nx + A.tc - 1) / A.tc);
       const dim3 g_inv(nb_st, ns);
       const dim3 g_res(nb_res, ns);
       if (which == 0) {
