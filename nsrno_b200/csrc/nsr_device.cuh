@@ -93,14 +93,16 @@ __device__ __forceinline__ float pml_profile_f(float pos, int n, int n_pml, floa
   return f * f;
 }
 
+// `inside`: node (i, j) lies off the PML (sf.lo < i < sf.hi_z and
+// sf.lo < j < sf.hi_x), tested by the caller once per row and column.
 template <bool ADJ>
-__device__ __forceinline__ float2 stencil_pts_f(const Geo& g, const SysScalarsF& sf, int i, int j, float a_c,
-                                                float a_e, float a_w, float a_s, float a_n, float b_c, float t_c,
-                                                float2 pc, float2 pe, float2 pw, float2 ps, float2 pn) {
+__device__ __forceinline__ float2 stencil_pts_f(const Geo& g, const SysScalarsF& sf, bool inside, int i, int j,
+                                                float a_c, float a_e, float a_w, float a_s, float a_n, float b_c,
+                                                float t_c, float2 pc, float2 pe, float2 pw, float2 ps, float2 pn) {
   const float e = t_c * sf.fpow;
   const float mb = sf.kh2 * b_c;
   float2 mass = make_float2(mb * (1.0f - e * e), (ADJ ? -2.0f : 2.0f) * mb * e);
-  if (i > sf.lo && i < sf.hi_z && j > sf.lo && j < sf.hi_x) {
+  if (inside) {
     float2 y = mass * pc;
     y = y + (0.5f * (a_c + a_e)) * (pe - pc);
     y = y + (0.5f * (a_c + a_w)) * (pw - pc);

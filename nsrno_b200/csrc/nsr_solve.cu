@@ -911,8 +911,17 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
       if (z0 > 0) { zN = zload(eN); aN = aload(eN); }
       zC = zload(eC); aC = aload(eC);
     }
-    for (int k = 0; k < nrows; ++k) {
+    // Interior test (no PML stretch) per column, once per item; per row below.
+    const bool col_in0 = j > sf.lo && j < sf.hi_x, col_in1 = j + CPT - 1 > sf.lo && j + CPT - 1 < sf.hi_x;
+    // Rows in groups of FLUSH, unrolled: the window moves and the group's
+    // float partial sums cost no instructions inside a group.
+    for (int k0 = 0; k0 < nrows; k0 += FLUSH) {
+#pragma unroll
+    for (int kk = 0; kk < FLUSH; ++kk) {
+      const int k = k0 + kk;
+      if (k >= nrows) break;
       const int i = z0 + k;
+      const bool row_in = i > sf.lo && i < sf.hi_z;
       const uint32_t sS = q0 + k + 2;
       const int eS = (eC + 1 == D) ? 0 : eC + 1;
       if (ok) ok = mbar_wait(&full[eS], (sS / D) & 1, &abort_word, NSR_STN_WAIT_NS);
@@ -935,10 +944,10 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
           const float2 tt = *reinterpret_cast<const float2*>(bC + Ly::OT + 8 * tid);
           const float4 rk = *reinterpret_cast<const float4*>(bC + Ly::ORH + 16 * tid);
           const float2 c0v = lo2(zc), c1v = hi2(zc);
-          const float2 av0 = stencil_pts_f<ADJ>(g, sf, i, j, ac.x, ac.y, aw, as.x, an.x, bb.x, tt.x, c0v, c1v, zw,
-                                                lo2(zs), lo2(zn));
-          const float2 av1 = stencil_pts_f<ADJ>(g, sf, i, j + 1, ac.y, ae, ac.x, as.y, an.y, bb.y, tt.y, c1v, ze,
-                                                c0v, hi2(zs), hi2(zn));
+          const float2 av0 = stencil_pts_f<ADJ>(g, sf, row_in && col_in0, i, j, ac.x, ac.y, aw, as.x, an.x, bb.x,
+                                                tt.x, c0v, c1v, zw, lo2(zs), lo2(zn));
+          const float2 av1 = stencil_pts_f<ADJ>(g, sf, row_in && col_in1, i, j + 1, ac.y, ae, ac.x, as.y, an.y, bb.y,
+                                                tt.y, c1v, ze, c0v, hi2(zs), hi2(zn));
           *reinterpret_cast<float4*>(out + (long long)i * nx + j) = pack2(av0, av1);
           if (half == 0) {
             dot_acc_f(accf[0], accf[1], lo2(rk), av0);       // <rhat, v>
@@ -966,7 +975,8 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
           const float bb = *reinterpret_cast<const float*>(bC + Ly::OB + 4 * tid);
           const float tt = *reinterpret_cast<const float*>(bC + Ly::OT + 4 * tid);
           const float2 rk = *reinterpret_cast<const float2*>(bC + Ly::ORH + 8 * tid);
-          const float2 av = stencil_pts_f<ADJ>(g, sf, i, j, ac, ae, aw, as, an, bb, tt, zc, ze, zw, zs, zn);
+          const float2 av = stencil_pts_f<ADJ>(g, sf, row_in && col_in0, i, j, ac, ae, aw, as, an, bb, tt, zc, ze, zw,
+                                               zs, zn);
           out[(long long)i * nx + j] = av;
           if (half == 0) {
             dot_acc_f(accf[0], accf[1], rk, av);       // <rhat, v>
@@ -983,18 +993,17 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
         }
       }
       zN = zC; zC = zS; aN = aC; aC = aS;
-      if ((k + 1) % FLUSH == 0 || k + 1 == nrows) {
-#pragma unroll
-        for (int qq = 0; qq < NSR_NPART; ++qq) {
-          if (half == 1 || qq < 2) accs[qq][tid] += (double)accf[qq];
-          accf[qq] = 0.0f;
-        }
-      }
       // the buffer of row i - 1 is no longer needed
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[eN]);
       eN = eC;
       eC = eS;
+    }
+#pragma unroll
+    for (int qq = 0; qq < NSR_NPART; ++qq) {
+      if (half == 1 || qq < 2) accs[qq][tid] += (double)accf[qq];
+      accf[qq] = 0.0f;
+    }
     }
     // rows z1 - 1 and z1
     __syncwarp();
