@@ -911,15 +911,14 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
       if (z0 > 0) { zN = zload(eN); aN = aload(eN); }
       zC = zload(eC); aC = aload(eC);
     }
+    // A row's buffer is read while the row is the south neighbour (its z and
+    // a, into registers) and while it is the centre; after that it goes back
+    // to the producer.  Row z0 - 1 is only ever a north neighbour.
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[eN]);
     // Interior test (no PML stretch) per column, once per item; per row below.
     const bool col_in0 = j > sf.lo && j < sf.hi_x, col_in1 = j + CPT - 1 > sf.lo && j + CPT - 1 < sf.hi_x;
-    // Rows in groups of FLUSH, unrolled: the window moves and the group's
-    // float partial sums cost no instructions inside a group.
-    for (int k0 = 0; k0 < nrows; k0 += FLUSH) {
-#pragma unroll
-    for (int kk = 0; kk < FLUSH; ++kk) {
-      const int k = k0 + kk;
-      if (k >= nrows) break;
+    for (int k = 0; k < nrows; ++k) {
       const int i = z0 + k;
       const bool row_in = i > sf.lo && i < sf.hi_z;
       const uint32_t sS = q0 + k + 2;
@@ -993,24 +992,21 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
         }
       }
       zN = zC; zC = zS; aN = aC; aC = aS;
-      // the buffer of row i - 1 is no longer needed
+      if ((k + 1) % FLUSH == 0 || k + 1 == nrows) {
+#pragma unroll
+        for (int qq = 0; qq < NSR_NPART; ++qq) {
+          if (half == 1 || qq < 2) accs[qq][tid] += (double)accf[qq];
+          accf[qq] = 0.0f;
+        }
+      }
+      // the buffer of row i (the centre) is no longer needed
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[eN]);
-      eN = eC;
+      if (lane == 0) mbar_arrive(&empty[eC]);
       eC = eS;
     }
-#pragma unroll
-    for (int qq = 0; qq < NSR_NPART; ++qq) {
-      if (half == 1 || qq < 2) accs[qq][tid] += (double)accf[qq];
-      accf[qq] = 0.0f;
-    }
-    }
-    // rows z1 - 1 and z1
+    // row z1 (south neighbour of the last row)
     __syncwarp();
-    if (lane == 0) {
-      mbar_arrive(&empty[eN]);
-      mbar_arrive(&empty[eC]);
-    }
+    if (lane == 0) mbar_arrive(&empty[eC]);
     q = q0 + nrows + 2;
 
     // Block sum of the partials (consumer threads only), then the arrival.
