@@ -726,13 +726,15 @@ __global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
 // copies themselves touches HBM on the read side, so the loads overlap the
 // stencil and FP64 dot products completely.
 // ---------------------------------------------------------------------------
-template <int W>
+// One row of the ring.  The first half (H = 0) needs no r and v, so its rows
+// are two fifths smaller and the same ring bytes hold more of them.
+template <int W, int H>
 struct StnLayout {
   static constexpr int OZ = 0;                    // float2 z[W + 4], column c0 - 2 + e
   static constexpr int ORH = OZ + (W + 4) * 8;    // float2 rhat[W]
-  static constexpr int OR = ORH + W * 8;          // float2 r[W]
-  static constexpr int OV = OR + W * 8;           // float2 v[W]
-  static constexpr int OA = OV + W * 8;           // float a[W + 8], column c0 - 4 + e
+  static constexpr int OR = ORH + W * 8;          // float2 r[W] (second half)
+  static constexpr int OV = OR + (H ? W * 8 : 0);   // float2 v[W] (second half)
+  static constexpr int OA = OV + (H ? W * 8 : 0);   // float a[W + 8], column c0 - 4 + e
   static constexpr int OB = OA + (W + 8) * 4;     // float b[W]
   static constexpr int OT = OB + W * 4;           // float t[W]
   static constexpr int SLOT = OT + W * 4;
@@ -763,18 +765,30 @@ __host__ __device__ inline StnItems stn_items(int nz, int nx, int tz, int ns) {
 
 // Resident CTAs per SM that the shared-memory ring of a k_stn shape allows
 // (at most 4): its register budget follows from it.
-template <int W, int D, int CPT>
+// Inner products of a half: <rhat, v> (first); <t, s>, <t, t>, <s, s>,
+// <rhat, t>, <rhat, s> (second), as (re, im) pairs where complex.
+__host__ __device__ constexpr int stn_parts(int H) { return H ? NSR_NPART : 2; }
+
+// Ring depth of the first half for a second-half depth D: the same ring bytes.
+template <int W>
+__host__ __device__ constexpr int stn_depth0(int D) {
+  return (D * StnLayout<W, 1>::SLOT) / StnLayout<W, 0>::SLOT;
+}
+
+template <int W, int D, int CPT, int H>
 __host__ __device__ constexpr int stn_min_blocks() {
   // ring, barriers and block sums (2 KB), FP64 accumulators of the consumers
-  constexpr int by_smem = (227 * 1024) / (D * StnLayout<W>::SLOT + 2048 + 8 * NSR_NPART * (W / CPT));
+  constexpr int by_smem = (227 * 1024) / (D * StnLayout<W, H>::SLOT + 2048 + 8 * stn_parts(H) * (W / CPT));
   constexpr int cap = (W / CPT + 32) > 256 ? 2 : 4;
   return by_smem < 1 ? 1 : (by_smem > cap ? cap : by_smem);
 }
 
-template <int W, int D, int CPT, bool ADJ>
-__global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
-    k_stn(SolveArgs A, int half, StnItems it, int ns) {
-  typedef StnLayout<W> Ly;
+template <int W, int D, int CPT, bool ADJ, int H>
+__global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>()))
+    k_stn(SolveArgs A, int /*half: H*/, StnItems it, int ns) {
+  typedef StnLayout<W, H> Ly;
+  constexpr int half = H;
+  constexpr int NP = stn_parts(H);
   constexpr int NC = W / CPT;   // consumer threads, CPT adjacent columns each
   constexpr int FLUSH = NSR_STN_FLUSH * 2 / CPT;   // rows per float partial sum
   extern __shared__ __align__(128) unsigned char ring[];
@@ -786,7 +800,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
   // Each consumer's FP64 accumulators live in shared memory (column tid): in
   // registers they pushed the 96-register budget of four CTAs per SM into
   // spills inside the row loop.
-  __shared__ double accs[NSR_NPART][NC];
+  __shared__ double accs[NP][NC];
   __shared__ int am_last;
   const Geo& g = A.g;
   const int nz = g.nz, nx = g.nx;
@@ -890,7 +904,10 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
     // products per thread), accumulated in FP64.
     float accf[NSR_NPART];
 #pragma unroll
-    for (int k = 0; k < NSR_NPART; ++k) { accs[k][tid] = 0.0; accf[k] = 0.0f; }
+    for (int k = 0; k < NSR_NPART; ++k) {
+      if (k < NP) accs[k][tid] = 0.0;
+      accf[k] = 0.0f;
+    }
     const uint32_t q0 = q;   // step of row z0 - 1
     bool ok = !abort_flag;
     // rows z0 - 1 and z0
@@ -995,7 +1012,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
       if ((k + 1) % FLUSH == 0 || k + 1 == nrows) {
 #pragma unroll
         for (int qq = 0; qq < NSR_NPART; ++qq) {
-          if (half == 1 || qq < 2) accs[qq][tid] += (double)accf[qq];
+          if (qq < NP) accs[qq][tid] += (double)accf[qq];
           accf[qq] = 0.0f;
         }
       }
@@ -1012,7 +1029,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT>()))
     // Block sum of the partials (consumer threads only), then the arrival.
 #pragma unroll
     for (int k = 0; k < NSR_NPART; ++k) {
-      const double s = warp_sum(accs[k][tid]);
+      const double s = k < NP ? warp_sum(accs[k][tid]) : 0.0;
       if (lane == 0) wsum[wid][k] = s;
     }
     named_sync(1, NC);
@@ -1267,17 +1284,23 @@ static int stn_items_max(const NsrGrid* g) {
 
 typedef void (*StnKernel)(SolveArgs, int, StnItems, int);
 
-static StnKernel stn_kernel(int w, int d, int cpt, bool adj) {
-#define NSR_STN_CASE(W_, D_, C_) \
-  if (w == W_ && d == D_ && cpt == C_) return adj ? k_stn<W_, D_, C_, true> : k_stn<W_, D_, C_, false>;
-  NSR_STN_CASE(256, 4, 2) NSR_STN_CASE(256, 5, 2) NSR_STN_CASE(256, 6, 2) NSR_STN_CASE(256, 8, 2)
-  NSR_STN_CASE(512, 4, 2) NSR_STN_CASE(512, 5, 2) NSR_STN_CASE(256, 4, 1) NSR_STN_CASE(256, 6, 1)
+// Stencil kernel of one half for the shape (w, d, cpt): d is the second
+// half's ring depth; the first half runs stn_depth0(d) of its smaller rows.
+static StnKernel stn_kernel(int w, int d, int cpt, bool adj, int half) {
+#define NSR_STN_CASE(W_, D_, C_)                                                                          \
+  if (w == W_ && d == D_ && cpt == C_) {                                                                  \
+    if (half) return adj ? k_stn<W_, D_, C_, true, 1> : k_stn<W_, D_, C_, false, 1>;                      \
+    return adj ? k_stn<W_, stn_depth0<W_>(D_), C_, true, 0> : k_stn<W_, stn_depth0<W_>(D_), C_, false, 0>; \
+  }
+  NSR_STN_CASE(256, 4, 2) NSR_STN_CASE(256, 5, 2) NSR_STN_CASE(256, 6, 2) NSR_STN_CASE(512, 4, 2)
+  NSR_STN_CASE(256, 4, 1)
 #undef NSR_STN_CASE
   return nullptr;
 }
 
-static size_t stn_smem(int w, int d) {
-  return (size_t)d * (w == 512 ? StnLayout<512>::SLOT : StnLayout<256>::SLOT);
+static size_t stn_smem(int w, int d, int half) {
+  if (w == 512) return half ? (size_t)d * StnLayout<512, 1>::SLOT : (size_t)stn_depth0<512>(d) * StnLayout<512, 0>::SLOT;
+  return half ? (size_t)d * StnLayout<256, 1>::SLOT : (size_t)stn_depth0<256>(d) * StnLayout<256, 0>::SLOT;
 }
 
 // Launch shapes of one call: NsrTiles with zero fields replaced by defaults.
@@ -1302,7 +1325,7 @@ static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileC
     c->cols_staged = t->cols_staged != 0;
     c->rows_staged = t->rows_staged != 0;
   }
-  if (!stn_kernel(c->sw, c->sd, c->scpt, false)) return NSR_ERR_ARGUMENT;
+  if (!stn_kernel(c->sw, c->sd, c->scpt, false, 1)) return NSR_ERR_ARGUMENT;
   if (c->sr < NSR_STN_MIN_ROWS || c->sr > 64 || c->sctas < 0 || c->sctas > 8) return NSR_ERR_ARGUMENT;
   if (!(c->tc == 8 || c->tc == 16) || (size_t)g->nz * c->tc * sizeof(float2) > 200 * 1024) return NSR_ERR_ARGUMENT;
   if (c->rows < 1 || c->rows > 8 || sizeof(float2) * (size_t)c->rows * nsr_row_stride(g->nx) > 200 * 1024)
@@ -1473,10 +1496,11 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
     const int nb_st = stencil_ctas(grid);
     const bool pairs = grid->nx % 2 == 0;
     const bool use_stn = stn_ok(grid);
-    const StnKernel stn_fn = stn_kernel(T.sw, T.sd, T.scpt, A.adjoint != 0);
+    const StnKernel stn_fn[2] = {stn_kernel(T.sw, T.sd, T.scpt, A.adjoint != 0, 0),
+                                 stn_kernel(T.sw, T.sd, T.scpt, A.adjoint != 0, 1)};
     const int stn_threads = T.sw / T.scpt + 32;
-    const size_t stn_sm = stn_smem(T.sw, T.sd);
-    int stn_per_sm = T.sctas;
+    const size_t stn_sm[2] = {stn_smem(T.sw, T.sd, 0), stn_smem(T.sw, T.sd, 1)};
+    int stn_per_sm[2] = {T.sctas, T.sctas};
     int n_sms = 1;
     {
       int dev = 0;
@@ -1484,11 +1508,14 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
       NSR_TRY(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev));
     }
     if (use_stn) {
-      NSR_TRY(cudaFuncSetAttribute((const void*)stn_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stn_sm));
-      if (stn_per_sm <= 0) {
-        NSR_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&stn_per_sm, (const void*)stn_fn, stn_threads,
-                                                              stn_sm));
-        if (stn_per_sm < 1) { err = NSR_ERR_ARGUMENT; goto cleanup; }
+      for (int h = 0; h < 2; ++h) {
+        NSR_TRY(cudaFuncSetAttribute((const void*)stn_fn[h], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)stn_sm[h]));
+        if (stn_per_sm[h] <= 0) {
+          NSR_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&stn_per_sm[h], (const void*)stn_fn[h], stn_threads,
+                                                                stn_sm[h]));
+          if (stn_per_sm[h] < 1) { err = NSR_ERR_ARGUMENT; goto cleanup; }
+        }
       }
     }
     // row kernels: direct (specialised widths) or staged through shared memory
@@ -1559,9 +1586,9 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
         si.per_slot = si.nbands * si.nstrips;
         si.n_items = ns * si.per_slot;
         int hv = half, nsv = ns;
-        const int gx = si.n_items < stn_per_sm * n_sms ? si.n_items : stn_per_sm * n_sms;
+        const int gx = si.n_items < stn_per_sm[half] * n_sms ? si.n_items : stn_per_sm[half] * n_sms;
         void* args[] = {&Ag, &hv, &si, &nsv};
-        cudaLaunchKernel((const void*)stn_fn, dim3(gx), dim3(stn_threads), args, stn_sm, sq);
+        cudaLaunchKernel((const void*)stn_fn[half], dim3(gx), dim3(stn_threads), args, stn_sm[half], sq);
       } else if (which == 3) {
         if (pairs) {
           if (A.adjoint) k_inv<true><<<g_inv, 256, 0, sq>>>(Ag, half);

@@ -35,9 +35,9 @@ import numpy as np
 # Parameter groups searched in this order; each candidate is a partial NsrTiles
 # dict (plus graph_iterations) merged into the current best.
 STENCIL_SHAPES = ([dict(stencil_width=w, stencil_depth=d, stencil_cols=2, stencil_rows=r)
-                   for (w, d) in ((256, 4), (256, 5), (256, 6), (256, 8), (512, 4), (512, 5))
+                   for (w, d) in ((256, 4), (256, 5), (256, 6), (512, 4))
                    for r in (16, 32, 64)] +
-                  [dict(stencil_width=256, stencil_depth=d, stencil_cols=1, stencil_rows=32) for d in (4, 6)])
+                  [dict(stencil_width=256, stencil_depth=4, stencil_cols=1, stencil_rows=32)])
 GROUPS = [
     ("stencil", STENCIL_SHAPES),
     ("stencil_ctas", [dict(stencil_ctas=0), dict(stencil_ctas=1), dict(stencil_ctas=2)]),

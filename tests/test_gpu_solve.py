@@ -277,9 +277,9 @@ def test_time_limit_reports_timeout(cuda):
     dict(rows_staged=1),
     dict(cols_staged=1, rows_staged=1, row_tile=8),
     dict(stencil_width=512, stencil_depth=4, stencil_rows=8),
-    dict(stencil_width=512, stencil_depth=5, stencil_cols=2, stencil_rows=32, stencil_ctas=1),
-    dict(stencil_width=256, stencil_depth=8, stencil_cols=2, stencil_rows=4, slot_groups=1),
-    dict(stencil_width=256, stencil_depth=6, stencil_cols=1, stencil_rows=64),
+    dict(stencil_width=512, stencil_depth=4, stencil_cols=2, stencil_rows=32, stencil_ctas=1),
+    dict(stencil_width=256, stencil_depth=6, stencil_cols=2, stencil_rows=4, slot_groups=1),
+    dict(stencil_width=256, stencil_depth=4, stencil_cols=1, stencil_rows=64),
 ])
 def test_launch_shapes_agree(cuda, tiles):
     """Every launch shape the autotuner may pick solves the same systems.  Shapes
