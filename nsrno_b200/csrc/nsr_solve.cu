@@ -928,11 +928,6 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
       if (z0 > 0) { zN = zload(eN); aN = aload(eN); }
       zC = zload(eC); aC = aload(eC);
     }
-    // A row's buffer is read while the row is the south neighbour (its z and
-    // a, into registers) and while it is the centre; after that it goes back
-    // to the producer.  Row z0 - 1 is only ever a north neighbour.
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[eN]);
     // Interior test (no PML stretch) per column, once per item; per row below.
     const bool col_in0 = j > sf.lo && j < sf.hi_x, col_in1 = j + CPT - 1 > sf.lo && j + CPT - 1 < sf.hi_x;
     for (int k = 0; k < nrows; ++k) {
@@ -1016,14 +1011,23 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
           accf[qq] = 0.0f;
         }
       }
-      // the buffer of row i (the centre) is no longer needed
+      // The buffer of row i - 1 goes back to the producer one row after its
+      // last use as centre.  Its values were loaded into registers during row
+      // i - 1, but a release right after those loads can overtake them: the
+      // arrival does not wait for shared-memory loads still in flight, and
+      // the producer's next bulk copy into the buffer then races them (seen
+      // as nondeterministic inner products with two slot groups).
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[eC]);
+      if (lane == 0) mbar_arrive(&empty[eN]);
+      eN = eC;
       eC = eS;
     }
-    // row z1 (south neighbour of the last row)
+    // rows z1 - 1 and z1
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[eC]);
+    if (lane == 0) {
+      mbar_arrive(&empty[eN]);
+      mbar_arrive(&empty[eC]);
+    }
     q = q0 + nrows + 2;
 
     // Block sum of the partials (consumer threads only), then the arrival.

@@ -298,6 +298,25 @@ def test_launch_shapes_agree(cuda, tiles):
         assert rel(got.iq.cpu().numpy(), base.iq.cpu().numpy()) < 1e-5
 
 
+@pytest.mark.parametrize("tiles", [None, dict(stencil_width=512, stencil_depth=4), dict(stencil_rows=16),
+                                   dict(stencil_rows=32, stencil_depth=5)])
+def test_two_slot_groups_are_deterministic(cuda, tiles):
+    """Twenty-two systems of the 1024 x 768 breast record, two slot groups on
+    concurrent graph branches, exactly ten iterations: two runs of one launch
+    shape give bitwise equal FP64 residuals.  A stencil ring that handed a row
+    buffer back before its shared-memory loads had landed made these shapes
+    differ from run to run."""
+    from nsrno_b200 import Geometry, Medium, solve_batched
+    from nsrno_b200.media import breast_record
+    rec = breast_record()
+    med = Medium(Geometry.from_record(rec), rec.c, rec.rho, rec.alpha, device=cuda)
+    f, a = rec.systems()
+    pick = np.linspace(0, len(f) - 1, 22).round().astype(int)
+    runs = [solve_batched(med, f[pick], a[pick], tolerance=1e-30, max_iterations=10, n_slots=22, tiles=tiles,
+                          blocking=True).residual.cpu() for _ in range(3)]
+    assert torch.equal(runs[0], runs[1]) and torch.equal(runs[0], runs[2])
+
+
 def test_grid_with_prime_factors_matches_lu(cuda):
     """110 x 140 = (2 5 11) x (4 5 7): transforms with direct-DFT prime stages
     in both directions, fixed and learned preconditioners, against SuperLU."""
