@@ -725,10 +725,7 @@ __device__ __forceinline__ bool fft_cols_direct(float2* s, const FftPlan& P, flo
 template <int R>
 struct RadixTag { static constexpr int value = R; };
 
-// UB: stage-0 butterflies whose inputs a thread gathers before transforming
-// any of them (their loads in flight together); 1 when `in` already issues
-// many loads per butterfly.
-template <int N, int UB, typename IN>
+template <int N, typename IN>
 __device__ __forceinline__ void ct_rows_forward_direct(float2* s, int nl, const float2* __restrict__ tws,
                                                        float2* __restrict__ g, IN in) {
   constexpr RadixList RL = nsr_radix_list(N);
@@ -736,34 +733,19 @@ __device__ __forceinline__ void ct_rows_forward_direct(float2* s, int nl, const 
   static_assert(LAST >= 1 && RL.r[LAST] == 16, "specialised sizes end with a radix-16 stage");
   constexpr int LS = N + N / 16;
   constexpr int R0 = RL.r[0], M0 = N / R0;
-  constexpr int U = R0 <= 4 ? UB : 1;
   const float2* __restrict__ tw0 = tws + nsr_twiddle_offset(N, N);
-  const int nb = nl * M0;
-  for (int b0 = threadIdx.x; b0 < nb; b0 += U * blockDim.x) {
-    float2 v[U][R0];
+  for (int b = threadIdx.x; b < nl * M0; b += blockDim.x) {
+    const int l = b / M0, j = b - l * M0;
+    float2 v[R0];
+    in(RadixTag<R0>{}, l * N + j, M0, v);
+    small_dft<R0, false>(v);
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int b = b0 + u * blockDim.x;
-      if (u == 0 || b < nb) {
-        const int l = b / M0, j = b - l * M0;
-        in(RadixTag<R0>{}, l * N + j, M0, v[u]);
-      }
-    }
+    for (int k = 1; k < R0; ++k) v[k] = v[k] * __ldg(tw0 + (k - 1) * M0 + j);
+    float2* d = s + l * LS;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int b = b0 + u * blockDim.x;
-      if (u == 0 || b < nb) {
-        const int l = b / M0, j = b - l * M0;
-        small_dft<R0, false>(v[u]);
-#pragma unroll
-        for (int k = 1; k < R0; ++k) v[u][k] = v[u][k] * __ldg(tw0 + (k - 1) * M0 + j);
-        float2* d = s + l * LS;
-#pragma unroll
-        for (int q = 0; q < R0; ++q) {
-          const int e = j + q * M0;
-          d[e + (e >> 4)] = v[u][q];
-        }
-      }
+    for (int q = 0; q < R0; ++q) {
+      const int e = j + q * M0;
+      d[e + (e >> 4)] = v[q];
     }
   }
   __syncthreads();
@@ -808,54 +790,37 @@ __device__ __forceinline__ void ct_rows_inverse_direct(float2* s, int nl, const 
   __syncthreads();
   if constexpr (LAST > 1) ct_inverse_downto<N, LAST - 1, 1, false, LS, 1, true>(s, nl, tws);
   constexpr int R0 = RL.r[0], M0 = N / R0;
-  // two butterflies per pass for the small first radices, so that the loads
-  // `out` makes (a gain plane) for both are in flight together
-  constexpr int U = R0 <= 4 ? 2 : 1;
   const float2* __restrict__ tw0 = tws + nsr_twiddle_offset(N, N);
-  const int nb = nl * M0;
-  for (int b0 = threadIdx.x; b0 < nb; b0 += U * blockDim.x) {
-    float2 v[U][R0];
+  for (int b = threadIdx.x; b < nl * M0; b += blockDim.x) {
+    const int l = b / M0, j = b - l * M0;
+    const float2* src = s + l * LS;
+    float2 v[R0];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int b = b0 + u * blockDim.x;
-      if (u == 0 || b < nb) {
-        const int l = b / M0, j = b - l * M0;
-        const float2* src = s + l * LS;
-#pragma unroll
-        for (int q = 0; q < R0; ++q) {
-          const int e = j + q * M0;
-          v[u][q] = src[e + (e >> 4)];
-        }
-#pragma unroll
-        for (int k = 1; k < R0; ++k) v[u][k] = v[u][k] * conjc(__ldg(tw0 + (k - 1) * M0 + j));
-        small_dft<R0, true>(v[u]);
-      }
+    for (int q = 0; q < R0; ++q) {
+      const int e = j + q * M0;
+      v[q] = src[e + (e >> 4)];
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int b = b0 + u * blockDim.x;
-      if (u == 0 || b < nb) {
-        const int l = b / M0, j = b - l * M0;
+    for (int k = 1; k < R0; ++k) v[k] = v[k] * conjc(__ldg(tw0 + (k - 1) * M0 + j));
+    small_dft<R0, true>(v);
 #pragma unroll
-        for (int q = 0; q < R0; ++q) out(l * N + j + q * M0, v[u][q]);
-      }
-    }
+    for (int q = 0; q < R0; ++q) out(l * N + j + q * M0, v[q]);
   }
 }
 
 // Dispatch of the direct row transforms over the specialised sizes; false for
 // any other size (the caller then stages the tile itself).
-template <int UB = 1, typename IN>
+template <typename IN>
 __device__ __forceinline__ bool fft_rows_forward_direct(float2* s, int nl, const FftPlan& P, float2* __restrict__ g,
                                                         IN in) {
   switch (P.n) {
-    case 256: ct_rows_forward_direct<256, UB>(s, nl, P.tws, g, in); return true;
-    case 384: ct_rows_forward_direct<384, UB>(s, nl, P.tws, g, in); return true;
-    case 512: ct_rows_forward_direct<512, UB>(s, nl, P.tws, g, in); return true;
-    case 768: ct_rows_forward_direct<768, UB>(s, nl, P.tws, g, in); return true;
-    case 1024: ct_rows_forward_direct<1024, UB>(s, nl, P.tws, g, in); return true;
-    case 1536: ct_rows_forward_direct<1536, UB>(s, nl, P.tws, g, in); return true;
-    case 2048: ct_rows_forward_direct<2048, UB>(s, nl, P.tws, g, in); return true;
+    case 256: ct_rows_forward_direct<256>(s, nl, P.tws, g, in); return true;
+    case 384: ct_rows_forward_direct<384>(s, nl, P.tws, g, in); return true;
+    case 512: ct_rows_forward_direct<512>(s, nl, P.tws, g, in); return true;
+    case 768: ct_rows_forward_direct<768>(s, nl, P.tws, g, in); return true;
+    case 1024: ct_rows_forward_direct<1024>(s, nl, P.tws, g, in); return true;
+    case 1536: ct_rows_forward_direct<1536>(s, nl, P.tws, g, in); return true;
+    case 2048: ct_rows_forward_direct<2048>(s, nl, P.tws, g, in); return true;
     default: return false;
   }
 }

@@ -283,10 +283,7 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
         for (int q = 0; q < R; ++q) out[q] = gain_mul(G.pre, goff + k0 + q * step, G.conj, out[q]);
       }
     };
-    // The first half's update loads five vectors per element; the others two
-    // or three, so they gather two butterflies' worth at a time.
-    if (mode == MODE_ITER_A) fft_rows_forward_direct<1>(sm, nr, A.tab.px, A.B.w + off, in);
-    else fft_rows_forward_direct<2>(sm, nr, A.tab.px, A.B.w + off, in);
+    fft_rows_forward_direct(sm, nr, A.tab.px, A.B.w + off, in);
   } else {
     fwd_staged(A, S, G, sm, mode, nr, off, goff, cnt, sv, rt, yp, ys, pp, pv);
   }
