@@ -62,11 +62,9 @@ FALLBACK_HBM_GBS = 6650.0
 KERNEL_BYTES = {"fwd_h0": 72, "cols_h0": 16, "rinv_h0": 16, "inv_h0": 24, "fwd_h1": 24, "cols_h1": 16,
                 "rinv_h1": 16, "res_h1": 0, "inv_h1": 40}
 # The learned preconditioner adds one complex64 read per node to every fwd
-# launch (inner gain) and every rinv launch (outer gain), and a half-precision
-# complex read (4 bytes) to every cols launch (the multiplier plane of the
-# slot's system).
-LEARNED_BYTES = {k: v + (8 if k.startswith(("fwd", "rinv")) else 4 if k.startswith("cols") else 0)
-                 for k, v in KERNEL_BYTES.items()}
+# launch (inner gain), every cols launch (the multiplier plane of the slot's
+# system) and every rinv launch (outer gain).
+LEARNED_BYTES = {k: v + (8 if k.startswith(("fwd", "cols", "rinv")) else 0) for k, v in KERNEL_BYTES.items()}
 COEF_BYTES = {"inv_h0": 12, "inv_h1": 12}
 LEARNED_SETUP_LAUNCHES = 5     # pool, three convolutions, gains
 

@@ -2,8 +2,6 @@
 // 5-point stencil at an explicit neighbourhood.
 #pragma once
 
-#include <cuda_fp16.h>
-
 #include "nsr_common.cuh"
 #include "nsr_internal.cuh"
 
@@ -270,19 +268,6 @@ __device__ __forceinline__ float2 learned_plane_value(const LearnedSpec& L, cons
   const float h2 = (float)(g.h * g.h);
   const float inv_n = 1.0f / (float)((long long)g.nz * g.nx);
   return inv_n * learned_symbol(L, tab.s2z[z], tab.s2x[x], kh2, h2);
-}
-
-// The batched solver's per-system multiplier plane holds the learned symbol
-// without the 1/n factor in half precision (the symbol's magnitude lies
-// between about 1e-1 and 1e3, well inside fp16's range; its 11-bit mantissa
-// perturbs the preconditioner by 5e-4 relative, which the Krylov iteration
-// and its FP64 true residual do not see): half the bytes of the column pass's
-// read, and its loads fit in registers next to the radix-16 butterfly.
-__device__ __forceinline__ __half2 learned_plane_half(const LearnedSpec& L, const Geo& g, const PrecTables& tab,
-                                                      float kh2, int z, int x) {
-  const float h2 = (float)(g.h * g.h);
-  const float2 m = learned_symbol(L, tab.s2z[z], tab.s2x[x], kh2, h2);
-  return __floats2half2_rn(m.x, m.y);
 }
 
 // Column pass of either preconditioner, chosen at run time: the learned

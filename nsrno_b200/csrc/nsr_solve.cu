@@ -63,7 +63,7 @@ struct SolveBufs {
   int* error;         // set by a kernel that gave up waiting on its copy ring
   double* partials;   // [n_slots][nb_inv][NSR_NPART]
   float2 *r, *rh, *p, *v, *t, *y, *w;   // [n_slots][n]
-  float2* sym;        // [n_slots][n] learned multiplier of the slot's system (learned solves only), read as half2
+  float2* sym;        // [n_slots][n] learned multiplier of the slot's system (learned solves only)
   double2* x;         // [n_slots][2][n]
 };
 
@@ -201,10 +201,10 @@ __global__ void __launch_bounds__(256, 4) k_fwd(SolveArgs A, int half) {
       // transformed field, for k_cols to read.
       const LearnedSpec L = load_learned_spec(A.lp);
       const float kh2 = (float)sys_scalars(g, S.freq).kh2;
-      __half2* __restrict__ sym = reinterpret_cast<__half2*>(A.B.sym) + off;
+      float2* __restrict__ sym = A.B.sym + off;
       for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
         const int l = k / g.nx;
-        sym[k] = learned_plane_half(L, g, A.tab, kh2, z0 + l, k - l * g.nx);
+        sym[k] = learned_plane_value(L, g, A.tab, kh2, z0 + l, k - l * g.nx);
       }
     }
     return;
@@ -303,10 +303,9 @@ __global__ void __launch_bounds__(512, 2) k_cols(SolveArgs A, int half) {
   const Geo& g = A.g;
   const int adjoint = A.adjoint;
   if (LEARNED) {
-    const __half2* __restrict__ symp = reinterpret_cast<const __half2*>(A.B.sym) + slot * n;
-    const float inv_n = 1.0f / (float)n;
+    const float2* __restrict__ symp = A.B.sym + slot * n;
     cols_pass_direct<TC, STAGED>(sm, g, A.tab, A.B.w + slot * n, c0, [&](int c, int z) -> float2 {
-      const float2 mul = inv_n * __half22float2(symp[(long long)z * g.nx + c0 + c]);
+      const float2 mul = symp[(long long)z * g.nx + c0 + c];
       return adjoint ? conjc(mul) : mul;
     });
   } else {

@@ -10,11 +10,11 @@ def test_iteration_bytes():
     assert list(bench.KERNEL_BYTES) == ["fwd_h0", "cols_h0", "rinv_h0", "inv_h0", "fwd_h1", "cols_h1", "rinv_h1",
                                         "res_h1", "inv_h1"]
     assert sum(bench.KERNEL_BYTES.values()) == 224
-    # learned: inner gain (fwd), half-precision multiplier plane (cols), outer gain (rinv)
+    # learned: inner gain (fwd), multiplier plane (cols), outer gain (rinv)
     extra = {k: bench.LEARNED_BYTES[k] - bench.KERNEL_BYTES[k] for k in bench.KERNEL_BYTES}
-    assert extra == {"fwd_h0": 8, "cols_h0": 4, "rinv_h0": 8, "inv_h0": 0, "fwd_h1": 8, "cols_h1": 4, "rinv_h1": 8,
+    assert extra == {"fwd_h0": 8, "cols_h0": 8, "rinv_h0": 8, "inv_h0": 0, "fwd_h1": 8, "cols_h1": 8, "rinv_h1": 8,
                      "res_h1": 0, "inv_h1": 0}
-    assert sum(bench.LEARNED_BYTES.values()) == 264
+    assert sum(bench.LEARNED_BYTES.values()) == 272
     assert set(bench.COEF_BYTES) == {"inv_h0", "inv_h1"}
 
 
