@@ -735,10 +735,8 @@ struct StnLayout {
   static constexpr int OR = ORH + W * 8;          // float2 r[W] (second half)
   static constexpr int OV = OR + (H ? W * 8 : 0);   // float2 v[W] (second half)
   static constexpr int OA = OV + (H ? W * 8 : 0);   // float a[W + 8], column c0 - 4 + e
-  static constexpr int OB = OA + (W + 8) * 4;     // float b[W]
-  static constexpr int OT = OB + W * 4;           // float t[W]
-  static constexpr int SLOT = OT + W * 4;
-  static_assert(ORH % 16 == 0 && OA % 16 == 0 && OB % 16 == 0 && OT % 16 == 0 && SLOT % 16 == 0, "alignment");
+  static constexpr int SLOT = OA + (W + 8) * 4;
+  static_assert(ORH % 16 == 0 && OA % 16 == 0 && SLOT % 16 == 0, "alignment");
 };
 
 #define NSR_STN_WAIT_NS 2000000000ull   // a ring wait longer than 2 s is an error
@@ -846,16 +844,14 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
         const bool own = row >= z0 && row < z1;
         uint32_t bytes = 0;
         if (in) bytes += (zhi - zlo) * 8 + (ahi - alo) * 4;
-        if (own) bytes += (phi - c0) * (8 + 4 + 4) + (half ? 2 * (phi - c0) * 8 : 0);
+        if (own) bytes += (phi - c0) * 8 + (half ? 2 * (phi - c0) * 8 : 0);
         mbar_arrive_expect_tx(&full[e], bytes);
         if (in) {
           const long long ro = (long long)row * nx;
           bulk_load(buf + Ly::OZ + (zlo - (c0 - 2)) * 8, zsrc + ro + zlo, (zhi - zlo) * 8, &full[e]);
           bulk_load(buf + Ly::OA + (alo - (c0 - 4)) * 4, A.mat.a32 + ro + alo, (ahi - alo) * 4, &full[e]);
           if (own) {
-            const uint32_t fb = (phi - c0) * 4, cb = (phi - c0) * 8;
-            bulk_load(buf + Ly::OB, A.mat.b32 + ro + c0, fb, &full[e]);
-            bulk_load(buf + Ly::OT, A.mat.t32 + ro + c0, fb, &full[e]);
+            const uint32_t cb = (phi - c0) * 8;
             bulk_load(buf + Ly::ORH, rhsrc + ro + c0, cb, &full[e]);
             if (half) {
               bulk_load(buf + Ly::OR, rsrc + ro + c0, cb, &full[e]);
@@ -928,11 +924,22 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
       if (z0 > 0) { zN = zload(eN); aN = aload(eN); }
       zC = zload(eC); aC = aload(eC);
     }
+    // The centre-only coefficients b and t are shared by every slot of the
+    // launch and come from L2 (the CTAs in flight work on the same rows):
+    // read directly, one row ahead, instead of through the ring.
+    const float* __restrict__ bpl = A.mat.b32;
+    const float* __restrict__ tpl = A.mat.t32;
+    auto bt = [&](const float* __restrict__ pl, int row) -> AT {
+      return own ? __ldg(reinterpret_cast<const AT*>(pl + (long long)row * nx + j)) : AT{};
+    };
+    AT bNext = bt(bpl, z0), tNext = bt(tpl, z0);
     // Interior test (no PML stretch) per column, once per item; per row below.
     const bool col_in0 = j > sf.lo && j < sf.hi_x, col_in1 = j + CPT - 1 > sf.lo && j + CPT - 1 < sf.hi_x;
     for (int k = 0; k < nrows; ++k) {
       const int i = z0 + k;
       const bool row_in = i > sf.lo && i < sf.hi_z;
+      const AT bRow = bNext, tRow = tNext;
+      if (k + 1 < nrows) { bNext = bt(bpl, i + 1); tNext = bt(tpl, i + 1); }
       const uint32_t sS = q0 + k + 2;
       const int eS = (eC + 1 == D) ? 0 : eC + 1;
       if (ok) ok = mbar_wait(&full[eS], (sS / D) & 1, &abort_word, NSR_STN_WAIT_NS);
@@ -951,8 +958,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
           const float2 ac = aC, an = aN, as = aS;
           const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
           const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 8) : 1.0f;
-          const float2 bb = *reinterpret_cast<const float2*>(bC + Ly::OB + 8 * tid);
-          const float2 tt = *reinterpret_cast<const float2*>(bC + Ly::OT + 8 * tid);
+          const float2 bb = bRow, tt = tRow;
           const float4 rk = *reinterpret_cast<const float4*>(bC + Ly::ORH + 16 * tid);
           const float2 c0v = lo2(zc), c1v = hi2(zc);
           const float2 av0 = stencil_pts_f<ADJ>(g, sf, row_in && col_in0, i, j, ac.x, ac.y, aw, as.x, an.x, bb.x,
@@ -983,8 +989,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
           const float ac = aC, an = aN, as = aS;
           const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
           const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 4) : 1.0f;
-          const float bb = *reinterpret_cast<const float*>(bC + Ly::OB + 4 * tid);
-          const float tt = *reinterpret_cast<const float*>(bC + Ly::OT + 4 * tid);
+          const float bb = bRow, tt = tRow;
           const float2 rk = *reinterpret_cast<const float2*>(bC + Ly::ORH + 8 * tid);
           const float2 av = stencil_pts_f<ADJ>(g, sf, row_in && col_in0, i, j, ac, ae, aw, as, an, bb, tt, zc, ze, zw,
                                                zs, zn);
@@ -1313,7 +1318,7 @@ struct TileChoice {
 };
 
 static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileChoice* c) {
-  c->sw = 256; c->sd = 4; c->sr = 64; c->sctas = 0; c->scpt = 2; c->cols_staged = 0; c->rows_staged = 0;
+  c->sw = 256; c->sd = 5; c->sr = 64; c->sctas = 0; c->scpt = 2; c->cols_staged = 0; c->rows_staged = 0;
   c->tc = nsr_cols_tc(g);
   c->rows = nsr_rows_per_cta(g);
   c->groups = n_slots >= 8 ? 2 : 1;

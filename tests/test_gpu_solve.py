@@ -280,6 +280,7 @@ def test_time_limit_reports_timeout(cuda):
     dict(stencil_width=512, stencil_depth=4, stencil_cols=2, stencil_rows=32, stencil_ctas=1),
     dict(stencil_width=256, stencil_depth=6, stencil_cols=2, stencil_rows=4, slot_groups=1),
     dict(stencil_width=256, stencil_depth=4, stencil_cols=1, stencil_rows=64),
+    dict(stencil_depth=4, stencil_rows=32),
 ])
 def test_launch_shapes_agree(cuda, tiles):
     """Every launch shape the autotuner may pick solves the same systems.  Shapes
