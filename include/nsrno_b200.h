@@ -73,7 +73,7 @@ typedef struct NsrGrid {
 typedef struct NsrTiles {
   int32_t stencil_width;     /* columns per stencil work item: 256 or 512      */
   int32_t stencil_depth;     /* row buffers of the second half's stencil ring:
-                                4, 5 (default), 6 (width 512: 4; one column per
+                                4 (default), 5, 6 (width 512: 4; one column per
                                 thread: 4); the first half's smaller rows fill
                                 the same bytes (7, 8 or 10 of them)            */
   int32_t stencil_rows;      /* rows per stencil work item (band): 4..64       */

@@ -1318,7 +1318,7 @@ struct TileChoice {
 };
 
 static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileChoice* c) {
-  c->sw = 256; c->sd = 5; c->sr = 64; c->sctas = 0; c->scpt = 2; c->cols_staged = 0; c->rows_staged = 0;
+  c->sw = 256; c->sd = 4; c->sr = 64; c->sctas = 0; c->scpt = 2; c->cols_staged = 0; c->rows_staged = 0;
   c->tc = nsr_cols_tc(g);
   c->rows = nsr_rows_per_cta(g);
   c->groups = n_slots >= 8 ? 2 : 1;

@@ -48,7 +48,7 @@ GROUPS = [
     ("slot_groups", [dict(slot_groups=1), dict(slot_groups=2)]),
     ("graph_iterations", [dict(graph_iterations=k) for k in (8, 16, 32)]),
 ]
-DEFAULT = dict(stencil_width=256, stencil_depth=5, stencil_cols=2, stencil_rows=64, stencil_ctas=0, cols_width=0,
+DEFAULT = dict(stencil_width=256, stencil_depth=4, stencil_cols=2, stencil_rows=64, stencil_ctas=0, cols_width=0,
                cols_staged=0, rows_staged=0, row_tile=0, slot_groups=0, graph_iterations=16)
 TILE_KEYS = ("stencil_width", "stencil_depth", "stencil_cols", "stencil_rows", "stencil_ctas", "cols_width",
              "cols_staged", "rows_staged", "row_tile", "slot_groups")

@@ -44,7 +44,7 @@ def test_rejected_default_is_an_error():
 
 def test_split_drops_zero_fields():
     tiles, k = tune.split({**tune.DEFAULT, "cols_width": 8, "graph_iterations": 32})
-    assert tiles == {"stencil_width": 256, "stencil_depth": 5, "stencil_cols": 2, "stencil_rows": 64,
+    assert tiles == {"stencil_width": 256, "stencil_depth": 4, "stencil_cols": 2, "stencil_rows": 64,
                      "cols_width": 8}
     assert k == 32
 
