@@ -80,7 +80,7 @@ typedef struct NsrTiles {
   int32_t stencil_ctas;      /* resident stencil CTAs per SM (0: occupancy)    */
   int32_t cols_width;        /* columns per column-FFT CTA: 8 or 16            */
   int32_t row_tile;          /* rows per row-FFT CTA: 1..8                     */
-  int32_t slot_groups;       /* independent slot groups on graph branches: 1, 2 */
+  int32_t slot_groups;       /* independent slot groups on graph branches: 1..4 */
   int32_t stencil_cols;      /* adjacent columns per stencil thread: 1 or 2    */
   int32_t cols_staged;       /* 1: column transform staged wholly through shared
                                 memory; 0: first and last stages fused into the

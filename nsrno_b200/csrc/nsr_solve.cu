@@ -34,6 +34,7 @@
 enum { MODE_EMPTY = 0, MODE_INIT = 1, MODE_ITER_A = 2, MODE_ITER_B = 3, MODE_RES = 4, MODE_EMIT = 5 };
 
 #define NSR_LAUNCHES_PER_IT 9
+#define NSR_MAX_GROUPS 4        // slot groups on parallel graph branches
 #define NSR_ST_TZ 32      // rows of one stencil CTA
 #define NSR_ST_TX 512     // columns of one stencil CTA (two per thread; even nx)
 #define NSR_ST_TX1 256    // columns of one stencil CTA of k_inv1 (one per thread; odd nx)
@@ -1339,8 +1340,8 @@ static int resolve_tiles(const NsrGrid* g, const NsrTiles* t, int n_slots, TileC
   if (!(c->tc == 8 || c->tc == 16) || (size_t)g->nz * c->tc * sizeof(float2) > 200 * 1024) return NSR_ERR_ARGUMENT;
   if (c->rows < 1 || c->rows > 8 || sizeof(float2) * (size_t)c->rows * nsr_row_stride(g->nx) > 200 * 1024)
     return NSR_ERR_ARGUMENT;
-  if (c->groups < 1 || c->groups > 2) return NSR_ERR_ARGUMENT;
-  if (n_slots < 2) c->groups = 1;
+  if (c->groups < 1 || c->groups > NSR_MAX_GROUPS) return NSR_ERR_ARGUMENT;
+  if (c->groups > n_slots) c->groups = n_slots;
   return 0;
 }
 
@@ -1419,8 +1420,9 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
   const size_t n = (size_t)grid->nz * grid->nx;
   cudaStream_t caller = (cudaStream_t)stream;
 
-  cudaStream_t st = nullptr, st2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // st runs slot group 0; sg[g] the other groups, forked from st and joined back
+  cudaStream_t st = nullptr, sg[NSR_MAX_GROUPS] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[NSR_MAX_GROUPS] = {};
   cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_poll[2] = {nullptr, nullptr};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1438,9 +1440,11 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
 #define NSR_TRY(x) do { ce = (x); if (ce != cudaSuccess) { err = (int)ce; goto cleanup; } } while (0)
   {
     NSR_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    NSR_TRY(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    for (int g = 1; g < NSR_MAX_GROUPS; ++g) {
+      NSR_TRY(cudaStreamCreateWithFlags(&sg[g], cudaStreamNonBlocking));
+      NSR_TRY(cudaEventCreateWithFlags(&ev_join[g], cudaEventDisableTiming));
+    }
     NSR_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    NSR_TRY(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     NSR_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
     NSR_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
     NSR_TRY(cudaEventCreateWithFlags(&ev_poll[0], cudaEventDisableTiming));
@@ -1550,14 +1554,14 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
     NSR_TRY(cudaGetLastError());
     launches = 3;  // two table kernels and the slot initialisation
 
-    // The slots run as two independent groups on two branches of the captured
-    // graph, so that one group's kernels fill the tail waves of the other's.
+    // The slots run as independent groups on branches of the captured graph,
+    // so that one group's kernels fill the tail waves of the others'.
     const int n_groups = T.groups;
-    int g_first[2] = {0, 0}, g_count[2] = {n_slots, 0};
-    if (n_groups == 2) {
-      g_count[0] = (n_slots + 1) / 2;
-      g_first[1] = g_count[0];
-      g_count[1] = n_slots - g_count[0];
+    int g_first[NSR_MAX_GROUPS] = {}, g_count[NSR_MAX_GROUPS] = {};
+    for (int g = 0, first = 0; g < n_groups; ++g) {
+      g_first[g] = first;
+      g_count[g] = n_slots / n_groups + (g < n_slots % n_groups ? 1 : 0);
+      first += g_count[g];
     }
     const int K = params->graph_iterations > 0 ? params->graph_iterations : 16;
     // One iteration = 9 launches: fwd, cols, rinv, inv of the first half, then
@@ -1631,12 +1635,12 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
       for (int it = 0; it < P; ++it)
         for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) {
           const int e = it * NSR_LAUNCHES_PER_IT + q;
-          if (n_groups == 2) NSR_TRY(cudaStreamWaitEvent(st2, ev_prof[e], 0));
+          for (int g = 1; g < n_groups; ++g) NSR_TRY(cudaStreamWaitEvent(sg[g], ev_prof[e], 0));
           launch(q, 0, st);
-          if (n_groups == 2) {
-            launch(q, 1, st2);
-            NSR_TRY(cudaEventRecord(ev_join, st2));
-            NSR_TRY(cudaStreamWaitEvent(st, ev_join, 0));
+          for (int g = 1; g < n_groups; ++g) {
+            launch(q, g, sg[g]);
+            NSR_TRY(cudaEventRecord(ev_join[g], sg[g]));
+            NSR_TRY(cudaStreamWaitEvent(st, ev_join[g], 0));
           }
           NSR_TRY(cudaGetLastError());
           NSR_TRY(cudaEventRecord(ev_prof[e + 1], st));
@@ -1652,18 +1656,15 @@ static int solve_impl(const NsrGrid* grid, const void* coef, const double* freq_
     // The K iterations of one round, captured from both slot-group streams.
     auto capture_round = [&]() -> cudaError_t {
       cudaError_t e = cudaSuccess;
-      if (n_groups == 2) {
-        if ((e = cudaEventRecord(ev_fork, st)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(st2, ev_fork, 0)) != cudaSuccess) return e;
-      }
+      if (n_groups > 1 && (e = cudaEventRecord(ev_fork, st)) != cudaSuccess) return e;
+      for (int g = 1; g < n_groups; ++g)
+        if ((e = cudaStreamWaitEvent(sg[g], ev_fork, 0)) != cudaSuccess) return e;
       for (int it = 0; it < K; ++it)
-        for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q) {
-          launch(q, 0, st);
-          if (n_groups == 2) launch(q, 1, st2);
-        }
-      if (n_groups == 2) {
-        if ((e = cudaEventRecord(ev_join, st2)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(st, ev_join, 0)) != cudaSuccess) return e;
+        for (int q = 0; q < NSR_LAUNCHES_PER_IT; ++q)
+          for (int g = 0; g < n_groups; ++g) launch(q, g, g ? sg[g] : st);
+      for (int g = 1; g < n_groups; ++g) {
+        if ((e = cudaEventRecord(ev_join[g], sg[g])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(st, ev_join[g], 0)) != cudaSuccess) return e;
       }
       return cudaGetLastError();
     };
@@ -1772,7 +1773,8 @@ cleanup:
   // graph, streams and events are then released by CUDA once it completes.
   if (blocking || err) {
     if (st) cudaStreamSynchronize(st);
-    if (st2) cudaStreamSynchronize(st2);
+    for (int g = 1; g < NSR_MAX_GROUPS; ++g)
+      if (sg[g]) cudaStreamSynchronize(sg[g]);
   }
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
@@ -1789,9 +1791,11 @@ cleanup:
     free(ev_prof);
   }
   if (st) cudaStreamDestroy(st);
-  if (st2) cudaStreamDestroy(st2);
+  for (int g = 1; g < NSR_MAX_GROUPS; ++g) {
+    if (sg[g]) cudaStreamDestroy(sg[g]);
+    if (ev_join[g]) cudaEventDestroy(ev_join[g]);
+  }
   if (ev_fork) cudaEventDestroy(ev_fork);
-  if (ev_join) cudaEventDestroy(ev_join);
 #undef NSR_TRY
   return err;
 }

@@ -241,7 +241,7 @@ def solve_batched(medium: Medium, freqs, angles=None, *, rhs=None, x0=None, tole
         words = torch.empty(8, dtype=torch.int32, pin_memory=True)
         words.copy_(ws[off:off + 32].view(torch.int32), non_blocking=True)
         groups = int((tiles or {}).get("slot_groups", 0)) or (2 if n_slots >= 8 else 1)
-        per_round = 9 * int(graph_iterations) * (groups if n_slots >= 2 else 1) + 1
+        per_round = 9 * int(graph_iterations) * min(groups, n_slots) + 1
         out.extra["progress_words"] = words
         out.extra["launches_per_round"] = per_round
     return out

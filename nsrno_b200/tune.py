@@ -45,7 +45,7 @@ GROUPS = [
     ("cols_staged", [dict(cols_staged=1), dict(cols_staged=0)]),
     ("rows_staged", [dict(rows_staged=1), dict(rows_staged=0)]),
     ("row_tile", [dict(row_tile=r) for r in (2, 4, 8)]),
-    ("slot_groups", [dict(slot_groups=1), dict(slot_groups=2)]),
+    ("slot_groups", [dict(slot_groups=g) for g in (1, 2, 3, 4)]),
     ("graph_iterations", [dict(graph_iterations=k) for k in (8, 16, 32)]),
 ]
 DEFAULT = dict(stencil_width=256, stencil_depth=4, stencil_cols=2, stencil_rows=64, stencil_ctas=0, cols_width=0,

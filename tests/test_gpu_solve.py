@@ -273,6 +273,8 @@ def test_time_limit_reports_timeout(cuda):
 
 @pytest.mark.parametrize("tiles", [
     dict(cols_width=8, row_tile=2, slot_groups=1),
+    dict(slot_groups=3),
+    dict(slot_groups=4, row_tile=8),
     dict(cols_staged=1),
     dict(rows_staged=1),
     dict(cols_staged=1, rows_staged=1, row_tile=8),
@@ -300,7 +302,7 @@ def test_launch_shapes_agree(cuda, tiles):
 
 
 @pytest.mark.parametrize("tiles", [None, dict(stencil_width=512, stencil_depth=4), dict(stencil_rows=16),
-                                   dict(stencil_rows=32, stencil_depth=5)])
+                                   dict(stencil_rows=32, stencil_depth=5), dict(slot_groups=4)])
 def test_two_slot_groups_are_deterministic(cuda, tiles):
     """Twenty-two systems of the 1024 x 768 breast record, two slot groups on
     concurrent graph branches, exactly ten iterations: two runs of one launch

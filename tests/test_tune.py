@@ -19,7 +19,7 @@ def fake_cost(cfg):
     c += {0: 0.0, 1: 0.01}[cfg["cols_staged"]]
     c += {0: 0.0, 1: 0.02}[cfg["rows_staged"]]
     c += {0: 0.03, 2: 0.05, 4: 0.0, 8: 0.02}[cfg["row_tile"]]
-    c += {0: 0.0, 1: 0.07, 2: 0.0}[cfg["slot_groups"]]
+    c += {0: 0.0, 1: 0.07, 2: 0.0, 3: 0.01, 4: 0.02}[cfg["slot_groups"]]
     c += {8: 0.02, 16: 0.01, 32: 0.0}[cfg["graph_iterations"]]
     return c
 
