@@ -715,28 +715,29 @@ __global__ void __launch_bounds__(256, 4) k_inv(SolveArgs A, int half) {
 // stn: the stencil of k_inv on rows staged through shared memory by bulk
 // (TMA) copies, for widths that are a multiple of 4.
 //
-// A persistent CTA walks work items (band of tz rows, strip of W columns,
-// slot).  One producer thread streams the rows of its items into a ring of D
-// row buffers with cp.async.bulk, completing on a `full` mbarrier per ring
-// entry; W/CPT consumer threads (CPT columns each) compute row i from the
-// buffers of rows i, i+1 (row i-1's values are carried in registers) and
-// release the buffer of row i-1 on an `empty` mbarrier.  A row buffer holds
-// the slot's vectors: z with two halo columns each side and, for the band's
-// own rows, rhat and, in the second half, r and v; D-3 row steps are in
-// flight per CTA while the consumers compute.  The medium's coefficients a,
-// b, t are the same for every slot of the launch, so they are read directly
-// and come from L2.
+// A persistent CTA walks work items (slot, band of tz rows, strip of W
+// columns).  One producer thread streams the rows of its items into a ring of
+// D row buffers with cp.async.bulk, completing on a `full` mbarrier per ring
+// entry; W/2 consumer threads (two columns each) compute row i from the
+// buffers of rows i-1, i, i+1 and release the buffer of row i-1 on an `empty`
+// mbarrier.  Every row buffer holds z (with two halo columns each side) and
+// a (four each side), and for the band's own rows b, t, rhat and, in the
+// second half, r and v: a row step moves about 22 B per column, and D-3 row
+// steps are in flight per CTA while the consumers compute.  Nothing but the
+// copies themselves touches HBM on the read side, so the loads overlap the
+// stencil and FP64 dot products completely.
 // ---------------------------------------------------------------------------
 // One row of the ring.  The first half (H = 0) needs no r and v, so its rows
-// are half the size and the same ring bytes hold about twice as many.
+// are two fifths smaller and the same ring bytes hold more of them.
 template <int W, int H>
 struct StnLayout {
   static constexpr int OZ = 0;                    // float2 z[W + 4], column c0 - 2 + e
   static constexpr int ORH = OZ + (W + 4) * 8;    // float2 rhat[W]
   static constexpr int OR = ORH + W * 8;          // float2 r[W] (second half)
   static constexpr int OV = OR + (H ? W * 8 : 0);   // float2 v[W] (second half)
-  static constexpr int SLOT = OV + (H ? W * 8 : 0);
-  static_assert(ORH % 16 == 0 && SLOT % 16 == 0, "alignment");
+  static constexpr int OA = OV + (H ? W * 8 : 0);   // float a[W + 8], column c0 - 4 + e
+  static constexpr int SLOT = OA + (W + 8) * 4;
+  static_assert(ORH % 16 == 0 && OA % 16 == 0 && SLOT % 16 == 0, "alignment");
 };
 
 #define NSR_STN_WAIT_NS 2000000000ull   // a ring wait longer than 2 s is an error
@@ -831,6 +832,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
       const float2* rsrc = A.B.r + soff;
       const float2* vsrc = A.B.v + soff;
       const int zlo = max(c0 - 2, 0), zhi = min(c0 + W + 2, nx);
+      const int alo = max(c0 - 4, 0), ahi = min(c0 + W + 4, nx);
       const int phi = min(c0 + W, nx);
       for (int row = z0 - 1; row <= z1; ++row, ++q) {
         const int e = q % D;
@@ -842,12 +844,13 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
         const bool in = row >= 0 && row < nz;
         const bool own = row >= z0 && row < z1;
         uint32_t bytes = 0;
-        if (in) bytes += (zhi - zlo) * 8;
+        if (in) bytes += (zhi - zlo) * 8 + (ahi - alo) * 4;
         if (own) bytes += (phi - c0) * 8 + (half ? 2 * (phi - c0) * 8 : 0);
         mbar_arrive_expect_tx(&full[e], bytes);
         if (in) {
           const long long ro = (long long)row * nx;
           bulk_load(buf + Ly::OZ + (zlo - (c0 - 2)) * 8, zsrc + ro + zlo, (zhi - zlo) * 8, &full[e]);
+          bulk_load(buf + Ly::OA + (alo - (c0 - 4)) * 4, A.mat.a32 + ro + alo, (ahi - alo) * 4, &full[e]);
           if (own) {
             const uint32_t cb = (phi - c0) * 8;
             bulk_load(buf + Ly::ORH, rhsrc + ro + c0, cb, &full[e]);
@@ -910,22 +913,17 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
     // column's z and a of rows i - 1 and i, carried from row to row so that
     // each row reads only its south neighbours from the ring.
     int eN = q0 % D, eC = (eN + 1 == D) ? 0 : eN + 1;
-    const int ez = (CPT * tid + 2) * 8;
+    const int ez = (CPT * tid + 2) * 8, ea = (CPT * tid + 4) * 4;
     typedef typename std::conditional<CPT == 2, float4, float2>::type ZT;
     typedef typename std::conditional<CPT == 2, float2, float>::type AT;
     auto zload = [&](int e) -> ZT { return *reinterpret_cast<const ZT*>(ring + (size_t)e * Ly::SLOT + Ly::OZ + ez); };
-    // The medium's coefficients are shared by every slot of the launch and
-    // come from L2 (the CTAs in flight work on the same rows): read directly.
-    const float* __restrict__ apl = A.mat.a32;
-    auto aload = [&](int row) -> AT {
-      return own ? __ldg(reinterpret_cast<const AT*>(apl + (long long)row * nx + j)) : AT{};
-    };
+    auto aload = [&](int e) -> AT { return *reinterpret_cast<const AT*>(ring + (size_t)e * Ly::SLOT + Ly::OA + ea); };
     ZT zN = ZT{}, zC = ZT{};
     AT aN, aC = AT{};
     if constexpr (CPT == 2) aN = make_float2(1.f, 1.f); else aN = 1.0f;   // no density contrast outside
     if (ok) {
-      if (z0 > 0) { zN = zload(eN); aN = aload(z0 - 1); }
-      zC = zload(eC); aC = aload(z0);
+      if (z0 > 0) { zN = zload(eN); aN = aload(eN); }
+      zC = zload(eC); aC = aload(eC);
     }
     // The centre-only coefficients b and t are shared by every slot of the
     // launch and come from L2 (the CTAs in flight work on the same rows):
@@ -950,7 +948,7 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
       ZT zS = ZT{};
       AT aS;
       if constexpr (CPT == 2) aS = make_float2(1.f, 1.f); else aS = 1.0f;
-      if (ok && i + 1 < nz) { zS = zload(eS); aS = aload(i + 1); }
+      if (ok && i + 1 < nz) { zS = zload(eS); aS = aload(eS); }
       if (ok && own) {
         const unsigned char* bC = ring + (size_t)eC * Ly::SLOT;
         const float2 zero = make_float2(0.f, 0.f);
@@ -959,8 +957,8 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
           const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
           const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 16) : zero;
           const float2 ac = aC, an = aN, as = aS;
-          const float aw = has_w ? __ldg(apl + (long long)i * nx + j - 1) : 1.0f;
-          const float ae = has_e ? __ldg(apl + (long long)i * nx + j + 2) : 1.0f;
+          const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
+          const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 8) : 1.0f;
           const float2 bb = bRow, tt = tRow;
           const float4 rk = *reinterpret_cast<const float4*>(bC + Ly::ORH + 16 * tid);
           const float2 c0v = lo2(zc), c1v = hi2(zc);
@@ -990,8 +988,8 @@ __global__ void __launch_bounds__(W / CPT + 32, (stn_min_blocks<W, D, CPT, H>())
           const float2 zw = has_w ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez - 8) : zero;
           const float2 ze = has_e ? *reinterpret_cast<const float2*>(bC + Ly::OZ + ez + 8) : zero;
           const float ac = aC, an = aN, as = aS;
-          const float aw = has_w ? __ldg(apl + (long long)i * nx + j - 1) : 1.0f;
-          const float ae = has_e ? __ldg(apl + (long long)i * nx + j + 1) : 1.0f;
+          const float aw = has_w ? *reinterpret_cast<const float*>(bC + Ly::OA + ea - 4) : 1.0f;
+          const float ae = has_e ? *reinterpret_cast<const float*>(bC + Ly::OA + ea + 4) : 1.0f;
           const float bb = bRow, tt = tRow;
           const float2 rk = *reinterpret_cast<const float2*>(bC + Ly::ORH + 8 * tid);
           const float2 av = stencil_pts_f<ADJ>(g, sf, row_in && col_in0, i, j, ac, ae, aw, as, an, bb, tt, zc, ze, zw,
