@@ -249,20 +249,9 @@ __device__ __forceinline__ void cols_pass_fixed(float2* sm, const Geo& g, const 
   });
 }
 
-// Learned multiplier read from a plane evaluated beforehand for this system:
-// symp[z * nx + x] at digit-reversed (z, x), 1/n included.
-template <int TC>
-__device__ __forceinline__ void cols_pass_plane(float2* sm, const Geo& g, const PrecTables& tab,
-                                                float2* __restrict__ ws, const float2* __restrict__ symp,
-                                                int adjoint, int c0) {
-  cols_pass_with<TC>(sm, g, tab, ws, c0, [&](int c, int z) -> float2 {
-    const float2 mul = symp[(long long)z * g.nx + c0 + c];
-    return adjoint ? conjc(mul) : mul;
-  });
-}
-
 // Learned multiplier times 1/n at digit-reversed position (z, x) of frequency
-// `freq`: the value cols_pass_plane expects in its plane.
+// `freq`: the value the batched solver's column pass reads from a system's
+// multiplier plane.
 __device__ __forceinline__ float2 learned_plane_value(const LearnedSpec& L, const Geo& g, const PrecTables& tab,
                                                       float kh2, int z, int x) {
   const float h2 = (float)(g.h * g.h);
