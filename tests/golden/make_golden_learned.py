@@ -1,6 +1,6 @@
 """Generate golden vectors of the learned preconditioner from the reference
-implementation (run in a container that has the reference checked out; the GPU
-box does not need this script).
+implementation (run on a machine that has the reference checked out; the
+tests only read the vectors it writes).
 
     python tests/golden/make_golden_learned.py REFERENCE_CHECKOUT
 

@@ -56,7 +56,7 @@ def test_surrogate_rejects_bins_outside_band():
     assert abs(bin_frequency(360) - 360 * 40e6 / 2401) < 1e-6
 
 
-def test_medium_requires_cuda_tensors_on_cpu_only_box():
+def test_medium_requires_cuda_tensors_without_a_gpu():
     from nsrno_b200 import Geometry, Medium
     geo = Geometry(nz=16, nx=16, h=1e-4, n_pml=2, face=3, rx_cols=np.arange(4), aperture_half_width=1e-3)
     if torch.cuda.is_available():
