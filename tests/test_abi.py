@@ -103,7 +103,8 @@ def test_ctypes_structs_match_the_header(tmp_path):
         pytest.skip("no C compiler")
     structs = {"NsrGrid": _lib.NsrGrid, "NsrLearned": _lib.NsrLearned, "NsrTiles": _lib.NsrTiles,
                "NsrSolveParams": _lib.NsrSolveParams, "NsrGmresParams": _lib.NsrGmresParams,
-               "NsrSolveStats": _lib.NsrSolveStats, "NsrDenseGrid": _lib.NsrDenseGrid}
+               "NsrSolveStats": _lib.NsrSolveStats, "NsrDenseGrid": _lib.NsrDenseGrid,
+               "NsrDenseSolveParams": _lib.NsrDenseSolveParams, "NsrDenseSolveInfo": _lib.NsrDenseSolveInfo}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "nsrno_b200.h"', 'int main(void) {']
     for name, cls in structs.items():
         lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
