@@ -58,11 +58,19 @@ def tangent_rhs(medium: Medium, freqs, u: torch.Tensor, dlogc, dlogrho):
     return out
 
 
-def _require_converged(res, what):
-    bad = [i for i, s in enumerate(res.status.cpu()) if int(s) != _lib.CONVERGED]
+def _require_converged(res, what, tolerance=None, accept_factor=1.0):
+    """Raise unless every system converged.  With ``accept_factor`` > 1, a
+    system that used its whole iteration budget but whose FP64 true residual
+    is within ``accept_factor * tolerance`` is accepted; returns how many."""
+    status = res.status.cpu()
+    resid = res.residual.cpu()
+    near = [i for i, s in enumerate(status) if int(s) == _lib.ITERATION_BUDGET and tolerance is not None
+            and float(resid[i]) <= accept_factor * tolerance]
+    bad = [i for i, s in enumerate(status) if int(s) != _lib.CONVERGED and i not in set(near)]
     if bad:
         raise RuntimeError(f"{what} failed to converge for {len(bad)} systems: "
                            f"{sorted(set(res.reasons()))}, max residual {float(res.residual.max()):.3g}")
+    return len(near)
 
 
 @dataclass
@@ -76,7 +84,13 @@ class GaussNewton:
     preconditioner: object = None     # LearnedPreconditioner or None (fixed shifted Laplace)
     tolerance: float = 1e-6
     n_slots: int = 22
-    max_iterations: int = 6000
+    max_iterations: int = 2000
+    # Adjoint solves with receiver-row sources can stall just above the
+    # tolerance at the accuracy the FP32 operator allows (a few of the
+    # band's highest frequencies at 0.04 mm): such a system is accepted when
+    # its FP64 true residual is within this factor of the tolerance, and
+    # counted in `near_tolerance`.
+    accept_factor: float = 2.0
     distributed: bool = False         # sum misfit, gradient and H v over the ranks of `group`
     group: object = None              # torch.distributed process group (None: the default group)
     timings: dict = field(default_factory=dict)
@@ -90,6 +104,7 @@ class GaussNewton:
         if self.preconditioner is not None:
             self.setup = self.preconditioner.setup(self.medium, torch.unique(self.f_dev))
         self.u = None
+        self.near_tolerance = {}
 
     def _solve(self, what, fields=True, **kw):
         t0 = time.perf_counter()
@@ -97,7 +112,7 @@ class GaussNewton:
                             n_slots=self.n_slots, learned=self.setup, return_fields=fields, **kw)
         torch.cuda.synchronize()
         self.timings[what] = self.timings.get(what, 0.0) + time.perf_counter() - t0
-        _require_converged(res, what)
+        self.near_tolerance[what] = _require_converged(res, what, self.tolerance, self.accept_factor)
         return res
 
     def _receiver_rhs(self, values):
@@ -176,7 +191,8 @@ class GaussNewton:
         total = time.perf_counter() - t0
         return dict(misfit=misfit, gradient_norm=gnorm, vHv=vhv, jv_norm2=jv2,
                     alpha=alpha, predicted_decrease=0.5 * gv * gv / vhv, seconds=total,
-                    phase_seconds=dict(self.timings), update=(alpha * vc, alpha * vr))
+                    phase_seconds=dict(self.timings), near_tolerance=dict(self.near_tolerance),
+                    update=(alpha * vc, alpha * vr))
 
 
 def main():
