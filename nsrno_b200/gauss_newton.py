@@ -94,6 +94,7 @@ class GaussNewton:
     distributed: bool = False         # sum misfit, gradient and H v over the ranks of `group`
     group: object = None              # torch.distributed process group (None: the default group)
     timings: dict = field(default_factory=dict)
+    near_tolerance: dict = field(default_factory=dict)   # per solve kind: systems accepted within accept_factor
 
     def __post_init__(self):
         dev = self.medium.device
@@ -104,7 +105,6 @@ class GaussNewton:
         if self.preconditioner is not None:
             self.setup = self.preconditioner.setup(self.medium, torch.unique(self.f_dev))
         self.u = None
-        self.near_tolerance = {}
 
     def _solve(self, what, fields=True, **kw):
         t0 = time.perf_counter()
