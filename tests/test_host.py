@@ -71,3 +71,29 @@ def test_receiver_response_is_band_limited():
     assert 0.5 < mid <= 1.01
     assert receiver_response(1.0e6) < 1e-3
     assert receiver_response(15e6) < 1e-3
+
+
+def test_gauss_newton_accepts_only_near_tolerance_stalls():
+    """The step's convergence check: converged systems pass; a system that
+    used its iteration budget passes only within accept_factor x tolerance
+    (and is counted); anything else, or a non-finite residual, raises."""
+    from types import SimpleNamespace
+    from nsrno_b200 import _lib
+    from nsrno_b200.gauss_newton import _require_converged
+
+    def res(status, resid):
+        st = torch.as_tensor(status, dtype=torch.int32)
+        return SimpleNamespace(status=st, residual=torch.as_tensor(resid, dtype=torch.float64),
+                               reasons=lambda: [_lib.REASONS[int(s)] for s in st])
+
+    C, B, D = _lib.CONVERGED, _lib.ITERATION_BUDGET, _lib.DIVERGED
+    assert _require_converged(res([C, C], [1e-7, 9e-7]), "forward", 1e-6, 2.0) == 0
+    assert _require_converged(res([C, B, B], [1e-7, 1.1e-6, 2e-6]), "adjoint", 1e-6, 2.0) == 2
+    with pytest.raises(RuntimeError):
+        _require_converged(res([C, B], [1e-7, 2.5e-6]), "adjoint", 1e-6, 2.0)
+    with pytest.raises(RuntimeError):
+        _require_converged(res([B], [float("nan")]), "adjoint", 1e-6, 2.0)
+    with pytest.raises(RuntimeError):
+        _require_converged(res([D], [1e-7]), "adjoint", 1e-6, 2.0)
+    with pytest.raises(RuntimeError):   # strict without a tolerance
+        _require_converged(res([B], [1e-7]), "observed data")
